@@ -1,0 +1,117 @@
+/*
+ * west_b200 — B200-native Wstat dielectric-response operator, C ABI.
+ *
+ * Drop-in boundary: WEST's
+ *     SUBROUTINE apply_operator(m, dvg, dng, tr2, iq)      Wstat/apply_operator.f90:14
+ * which applies dng = sqvc * chi0(sqvc * dvg) to m perturbations by solving
+ * Gamma-point Sternheimer equations (DFPT_kernel/dfpt_module.f90:22).
+ *
+ * All entry points are extern "C", take plain pointers and sizes, never abort
+ * and report errors as negative status codes with a message available from
+ * wb_last_error().  Complex arrays are interleaved (re, im) doubles, i.e.
+ * Fortran COMPLEX(DP) / C double _Complex, column-major with an explicit
+ * leading dimension.  A Fortran caller binds them with iso_c_binding.
+ */
+#ifndef WEST_B200_H
+#define WEST_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WB_OK 0
+#define WB_ERR_ARG (-1)         /* invalid argument or inconsistent system data */
+#define WB_ERR_CUDA (-2)        /* a CUDA call failed */
+#define WB_ERR_UNSUPPORTED (-3) /* valid in WEST but not provided here (k-points, non-cubic box...) */
+#define WB_ERR_NOMEM (-4)       /* device allocation failed */
+
+#define WB_PRECISION_FP64 0
+#define WB_PRECISION_MIXED 1
+
+typedef struct wb_ctx wb_ctx;
+
+/*
+ * Ground-state data that dfpt reads from QE/WEST modules.  Every pointer is a
+ * host pointer and is only read during wb_ctx_create (the context keeps
+ * device copies).  Field-by-field origin in WEST/QE:
+ */
+typedef struct wb_system {
+  int npw;             /* pwcom npw = ngk(1) = westcom npwq at Gamma              */
+  int npwx;            /* leading dimension of evc and vkb (pwcom npwx)           */
+  int nr1, nr2, nr3;   /* dffts%nr1..nr3 (a cubic box: all three equal)           */
+  int nbnd_occ;        /* westcom nbnd_occ(1)                                     */
+  int nkb;             /* uspp nkb                                                */
+  int n_dfpt_maxiter;  /* westcom n_dfpt_maxiter                                  */
+  int l_kinetic_only;  /* westcom l_kinetic_only (k_psi instead of h_psi)         */
+  int gstart;          /* gvect gstart: must be 2 (this process holds G=0)        */
+  const int* nl;       /* [npw] dffts%nl, 1-based box index of +G                 */
+  const int* nlm;      /* [npw] dffts%nlm, 1-based box index of -G                */
+  const double* g2kin; /* [npw] wvfct g2kin (Ry)                                  */
+  const double* vrs;   /* [nr1*nr2*nr3] scf vrs(:,1) on the smooth grid (Ry)      */
+  const double* evc;   /* [npwx, nbnd_occ] complex: wavefunctions evc             */
+  const double* et;    /* [nbnd_occ] wvfct et(:,1) (Ry)                           */
+  const double* occupation; /* [nbnd_occ] westcom occupation(:,1)                 */
+  const double* vkb;   /* [npwx, nkb] complex: uspp vkb after init_us_2           */
+  const double* deeq;  /* [nkb, nkb] KB coupling D, dense (block-diagonal per atom) */
+  const double* sqvc;  /* [npw] pot3D%sqvc (Coulomb_kernel/class_coulomb.f90:173) */
+  double alpha_pv;     /* westcom alphapv_dfpt (Tools/get_alpha_pv.f90)           */
+  double omega;        /* cell_base omega (bohr^3)                                */
+  double wk;           /* k_grid%weight(1) (QE wk; 2 for a spin-unpolarised Gamma) */
+} wb_system;
+
+/* Counters of the last wb_apply_operator call. */
+typedef struct wb_stats {
+  int m;                   /* perturbations processed                         */
+  int cg_iterations;       /* PCG iterations of the longest chunk             */
+  long long cg_active_sum; /* sum over iterations of active (pert, band) systems */
+  long long fft_boxes;     /* complex 3D box transforms performed             */
+  double ms_total;         /* device time of the call (ms, CUDA events)       */
+} wb_stats;
+
+/*
+ * Create a context on CUDA device `device` and upload the ground state.
+ * Replaces the setup part of dfpt (dfpt_module.f90:93-225: allocations,
+ * set_eprec, et/eprec gathering) and QE's FFT/projector setup.
+ */
+int wb_ctx_create(wb_ctx** ctx, const wb_system* sys, int device);
+
+/* Release all device memory of the context. */
+int wb_ctx_destroy(wb_ctx* ctx);
+
+/*
+ * The drop-in for apply_operator (Wstat/apply_operator.f90:14-69).
+ *   m            number of perturbations (columns)
+ *   dvg          [ld_dvg, m] complex, host memory, IN
+ *   dng          [ld_dng, m] complex, host memory, OUT (rows >= npw set to 0)
+ *   tr2          PCG threshold on <r|M^-1 r>; tr2 < 0 = lite solver (no PCG),
+ *                dfpt_module.f90:130,350
+ *   iq           q-point index; only 1 (Gamma) is provided
+ *   unconverged  [m] OUT (may be NULL): bands left unconverged per
+ *                perturbation (dfpt's ierr, dfpt_module.f90:356-359)
+ * Synchronous: returns when dng is written.
+ */
+int wb_apply_operator(wb_ctx* ctx, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng, double tr2,
+                      int iq, int* unconverged);
+
+/* Same contract with dvg and dng in device memory of the context's device. */
+int wb_apply_operator_device(wb_ctx* ctx, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng,
+                             double tr2, int iq, int* unconverged);
+
+/* WB_PRECISION_FP64 (default) or WB_PRECISION_MIXED. */
+int wb_set_precision(wb_ctx* ctx, int mode);
+
+/* Upper bound on perturbations processed per device batch (0 = automatic). */
+int wb_set_batch(wb_ctx* ctx, int max_perturbations);
+
+int wb_get_stats(const wb_ctx* ctx, wb_stats* out);
+
+/* Message of the last failed call in this thread ("" if none). */
+const char* wb_last_error(void);
+
+/* Library version: major * 10000 + minor * 100 + patch. */
+int wb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WEST_B200_H */

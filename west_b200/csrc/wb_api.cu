@@ -1,0 +1,575 @@
+// C ABI and host orchestration of the B200 response operator.
+//
+// The per-call pipeline replaces dfpt (DFPT_kernel/dfpt_module.f90:22-533) for
+// a whole batch of perturbations at once instead of one perturbation at a
+// time: all (perturbation, occupied band) Sternheimer systems run the masked
+// PCG of linsolve_sternheimer_m_wfcts together, each with its own
+// convergence mask, so every system follows exactly the reference's per-band
+// iteration while the FFTs and GEMMs see thousands of columns per launch.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/west_b200.h"
+#include "wb_internal.h"
+
+using namespace wb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define WB_CU(call)                                                                            \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail(WB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Grow-only device buffer.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t b) {
+    if (b <= bytes) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMalloc(&p, b) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    bytes = b;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct wb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int npw = 0, nr = 0, nnr = 0, nocc = 0, nkb = 0, nproj = 0, npv = 0;
+  int maxiter = 0, kinetic_only = 0, precision = WB_PRECISION_FP64, batch_cap = 0;
+  double omega = 0, wk = 0, alpha = 0;
+  StickTab st{};
+  FftArgs fa{};
+  // constant device data
+  DBuf perm, gqz, spg, stpos, tw, g2kin, sqvc, vs, evc, W, D, eprec, et, occ, evcr;
+  // per-call workspace
+  DBuf dvg_in, dng_out, aux, dvbox, B, X, G, T, sticks, sticks2, acc, part, C, rho, conv, act, items, nact,
+      ecol, epcol, unconv, items_pp, items_pk, iota_items;
+  int* nact_host = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  wb_stats stats{};
+};
+
+namespace {
+
+int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
+  const int N = s->nr1, npw = s->npw;
+  struct GInfo { int mx, my, mz, ref; };
+  std::vector<GInfo> gi(npw);
+  auto mill = [N](int v) { return v < (N + 1) / 2 ? v : v - N; };
+  std::map<long, long> seen;
+  for (int i = 0; i < npw; ++i) {
+    const long b = (long)s->nl[i] - 1;
+    if (b < 0 || b >= (long)N * N * N) return fail(WB_ERR_ARG, "nl out of range at G " + std::to_string(i + 1));
+    const int x = (int)(b % N), y = (int)((b / N) % N), z = (int)(b / ((long)N * N));
+    gi[i] = {mill(x), mill(y), mill(z), i};
+    if (2 * std::abs(gi[i].mx) >= N || 2 * std::abs(gi[i].my) >= N || 2 * std::abs(gi[i].mz) >= N)
+      return fail(WB_ERR_ARG, "G sphere reaches the box edge (aliasing) at G " + std::to_string(i + 1));
+    const long bm = (long)s->nlm[i] - 1;
+    const long want = ((-gi[i].mx + N) % N) + (long)N * (((-gi[i].my + N) % N) + (long)N * ((-gi[i].mz + N) % N));
+    if (bm != want) return fail(WB_ERR_ARG, "nlm is not the box index of -G at G " + std::to_string(i + 1));
+    if (seen.count(b) || (i > 0 && seen.count(bm)))
+      return fail(WB_ERR_ARG, "G and -G both stored (not a Gamma half sphere) at G " + std::to_string(i + 1));
+    seen[b] = i;
+  }
+  if (gi[0].mx != 0 || gi[0].my != 0 || gi[0].mz != 0) return fail(WB_ERR_ARG, "first G vector must be G=0");
+  // stick pairs: canonical stick (x > 0) or (x == 0, y > 0); (0,0) is pair 0
+  auto canon = [](int x, int y, int& cx, int& cy, int& side) {
+    if (x > 0 || (x == 0 && y > 0) || (x == 0 && y == 0)) { cx = x; cy = y; side = 0; }
+    else { cx = -x; cy = -y; side = 1; }
+  };
+  std::map<std::pair<int, int>, int> pairs;
+  pairs[{0, 0}] = 0;
+  std::vector<std::pair<int, int>> keys;
+  for (auto& g : gi) {
+    int cx, cy, sd;
+    canon(g.mx, g.my, cx, cy, sd);
+    if (cx == 0 && cy == 0) continue;
+    pairs.emplace(std::make_pair(cx, cy), 0);
+  }
+  int q = 1;
+  std::vector<std::pair<int, int>> pair_xy(pairs.size());
+  pair_xy[0] = {0, 0};
+  for (auto& kv : pairs) {
+    if (kv.first.first == 0 && kv.first.second == 0) continue;
+    kv.second = q;
+    pair_xy[q] = kv.first;
+    ++q;
+  }
+  const int nsp = (int)pairs.size();
+  std::vector<int> gq(npw), gside(npw);
+  int xmax = 0;
+  for (int i = 0; i < npw; ++i) {
+    int cx, cy, sd;
+    canon(gi[i].mx, gi[i].my, cx, cy, sd);
+    gq[i] = pairs[{cx, cy}];
+    gside[i] = (gq[i] == 0) ? 0 : sd;
+    xmax = std::max(xmax, std::abs(gi[i].mx));
+  }
+  std::vector<int> order(npw);
+  for (int i = 0; i < npw; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    if (gq[a] != gq[b]) return gq[a] < gq[b];
+    const int za = gq[a] == 0 ? std::abs(gi[a].mz) : gi[a].mz;
+    const int zb = gq[b] == 0 ? std::abs(gi[b].mz) : gi[b].mz;
+    return za < zb;
+  });
+  perm.assign(order.begin(), order.end());  // internal -> reference
+  std::vector<int> spg(nsp + 1, 0);
+  std::vector<int2> gqz(npw);
+  for (int i = 0; i < npw; ++i) {
+    const int r = order[i];
+    spg[gq[r] + 1]++;
+    gqz[i] = make_int2(2 * gq[r] + gside[r], gi[r].mz);
+  }
+  for (int p = 0; p < nsp; ++p) spg[p + 1] += spg[p];
+  const int nst = 2 * nsp;
+  std::vector<int> stpos(nst, -1);
+  for (int p = 0; p < nsp; ++p) {
+    const int x = pair_xy[p].first, y = pair_xy[p].second;
+    stpos[2 * p] = ((y + N) % N) * N + ((x + N) % N);
+    if (p > 0) stpos[2 * p + 1] = ((-y + N) % N) * N + ((-x + N) % N);
+  }
+  // device copies
+  if (c->gqz.ensure(sizeof(int2) * npw) || c->spg.ensure(sizeof(int) * (nsp + 1)) ||
+      c->stpos.ensure(sizeof(int) * nst) || c->perm.ensure(sizeof(int) * npw))
+    return fail(WB_ERR_NOMEM, "device allocation of stick tables failed");
+  WB_CU(cudaMemcpy(c->gqz.p, gqz.data(), sizeof(int2) * npw, cudaMemcpyHostToDevice));
+  WB_CU(cudaMemcpy(c->spg.p, spg.data(), sizeof(int) * (nsp + 1), cudaMemcpyHostToDevice));
+  WB_CU(cudaMemcpy(c->stpos.p, stpos.data(), sizeof(int) * nst, cudaMemcpyHostToDevice));
+  WB_CU(cudaMemcpy(c->perm.p, perm.data(), sizeof(int) * npw, cudaMemcpyHostToDevice));
+  c->st.nsp = nsp;
+  c->st.nst = nst;
+  c->st.sp_gstart = c->spg.as<int>();
+  c->st.g_qz = c->gqz.as<int2>();
+  c->st.st_pos = c->stpos.as<int>();
+  c->st.xhi = xmax;
+  c->st.ncols = 2 * xmax + 1;
+  return WB_OK;
+}
+
+// Upload a [ld, ncol] complex host array into internal order [ncol][npw].
+int upload_cols(const double* h, int ld, int ncol, const std::vector<int>& perm, DBuf& d) {
+  const int npw = (int)perm.size();
+  std::vector<double2> tmp((size_t)npw * ncol);
+  for (int j = 0; j < ncol; ++j)
+    for (int i = 0; i < npw; ++i) {
+      const double* src = h + 2 * ((size_t)j * ld + perm[i]);
+      tmp[(size_t)j * npw + i] = make_double2(src[0], src[1]);
+    }
+  if (d.ensure(sizeof(double2) * tmp.size() + 16)) return fail(WB_ERR_NOMEM, "device allocation failed");
+  WB_CU(cudaMemcpy(d.p, tmp.data(), sizeof(double2) * tmp.size(), cudaMemcpyHostToDevice));
+  return WB_OK;
+}
+
+template <class T>
+int upload(const T* h, size_t n, DBuf& d) {
+  if (d.ensure(sizeof(T) * n + 16)) return fail(WB_ERR_NOMEM, "device allocation failed");
+  WB_CU(cudaMemcpy(d.p, h, sizeof(T) * n, cudaMemcpyHostToDevice));
+  return WB_OK;
+}
+
+void pair_items(std::vector<int2>& it, int base, int n) {
+  for (int k = 0; k < (n + 1) / 2; ++k) it.push_back(make_int2(base + 2 * k, (2 * k + 1 < n) ? base + 2 * k + 1 : -1));
+}
+
+size_t per_pert_bytes(const wb_ctx* c) {
+  const size_t vec = sizeof(double2) * (size_t)c->npw * c->nocc;
+  const size_t stk = sizeof(double2) * (size_t)c->nr * c->st.nst;
+  return 4 * vec                                   // B, X, G, T
+         + stk * (size_t)c->npv                    // sticks (RHS / CG pairs / drho items)
+         + sizeof(double2) * (size_t)c->nnr * 1    // dvbox + acc (one box per two perturbations each)
+         + stk                                     // sticks2 (half per perturbation, rounded up)
+         + sizeof(double) * (size_t)c->nocc * c->nproj * 9  // GEMM partials and coefficients
+         + 2 * sizeof(double2) * (size_t)c->npw;   // aux, input/output staging
+}
+
+int choose_batch(wb_ctx* c, int m) {
+  size_t freeb = 0, totb = 0;
+  cudaMemGetInfo(&freeb, &totb);
+  const size_t budget = (size_t)(0.6 * (double)freeb);
+  int mb = (int)std::max<size_t>(2, budget / std::max<size_t>(1, per_pert_bytes(c)));
+  mb = std::min(mb, m);
+  if (c->batch_cap > 0) mb = std::min(mb, c->batch_cap);
+  return std::max(mb, 1);
+}
+
+int ensure_workspace(wb_ctx* c, int mb, long ld_in, long ld_out) {
+  const size_t nsys = (size_t)mb * c->nocc;
+  const size_t vec = sizeof(double2) * (size_t)c->npw * nsys;
+  const size_t stk1 = sizeof(double2) * (size_t)c->nr * c->st.nst;
+  const size_t mp = (mb + 1) / 2;
+  const size_t nitems = std::max<size_t>({(nsys + 1) / 2, (size_t)mb * c->npv, mp, (size_t)c->npv});
+  const int nsplit = gemm_tn_splits(c->nproj, (int)nsys, 2 * c->npw);
+  bool bad = false;
+  bad |= c->dvg_in.ensure(sizeof(double2) * ld_in * mb + 16) != 0;
+  bad |= c->dng_out.ensure(sizeof(double2) * ld_out * mb + 16) != 0;
+  bad |= c->aux.ensure(sizeof(double2) * (size_t)c->npw * mb) != 0;
+  bad |= c->dvbox.ensure(sizeof(double2) * (size_t)c->nnr * mp) != 0;
+  bad |= c->B.ensure(vec) || c->X.ensure(vec) || c->G.ensure(vec) || c->T.ensure(vec);
+  bad |= c->sticks.ensure(stk1 * nitems) != 0;
+  bad |= c->sticks2.ensure(stk1 * mp) != 0;
+  bad |= c->acc.ensure(sizeof(double2) * (size_t)c->nnr * mp) != 0;
+  bad |= c->part.ensure(sizeof(double) * (size_t)nsplit * nsys * c->nproj) != 0;
+  bad |= c->C.ensure(sizeof(double) * nsys * c->nproj) != 0;
+  bad |= c->rho.ensure(sizeof(double) * nsys) != 0;
+  bad |= c->conv.ensure(nsys + 16) != 0;
+  bad |= c->act.ensure(sizeof(int) * nsys) != 0;
+  bad |= c->items.ensure(sizeof(int2) * (nsys / 2 + 1)) != 0;
+  bad |= c->nact.ensure(sizeof(int) * 4) != 0;
+  bad |= c->ecol.ensure(sizeof(double) * nsys) != 0;
+  bad |= c->epcol.ensure(sizeof(double) * nsys) != 0;
+  bad |= c->unconv.ensure(sizeof(int) * mb) != 0;
+  bad |= c->items_pp.ensure(sizeof(int2) * mp) != 0;
+  bad |= c->items_pk.ensure(sizeof(int2) * (size_t)mb * c->npv) != 0;
+  if (bad) return fail(WB_ERR_NOMEM, "device workspace allocation failed for a batch of " + std::to_string(mb));
+  return WB_OK;
+}
+
+// T = (H - e + alpha Pv) X on columns cols[0..n) (pairs in items), K = 2 npw.
+void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const int2* items, int n, int nsys,
+             int nsplit) {
+  const long ld = c->npw;
+  const int K = 2 * c->npw;
+  cudaStream_t s = c->stream;
+  const double* W = c->W.as<double>();
+  int M = c->nproj, nkb = c->nkb;
+  const double* Wsub = W;
+  if (c->kinetic_only) {
+    kinetic_hpsi(Xv, Tv, c->g2kin.as<double>(), c->ecol.as<double>(), cols, n, c->npw, ld, s);
+    Wsub = W + (size_t)c->nkb * K;  // alpha Pv only
+    M = c->nocc;
+    nkb = 0;
+  } else {
+    const int nit = (n + 1) / 2;
+    fft_zinv(c->fa, Xv, ld, items, nit, c->sticks.as<double2>());
+    fft_plane_vloc(c->fa, c->sticks.as<double2>(), nit, c->vs.as<double>());
+    fft_zfwd_hpsi(c->fa, c->sticks.as<double2>(), items, nit, Xv, Tv, ld, c->g2kin.as<double>(),
+                  c->ecol.as<double>());
+    c->stats.fft_boxes += 2 * nit;
+  }
+  gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s);
+  gamma_reduce(c->part.as<double>(), nsplit, M, n, Wsub, K, (const double*)Xv, 2 * ld, cols, c->D.as<double>(), nkb,
+               c->alpha, c->C.as<double>(), s);
+  gemm_nn(Wsub, K, M, c->C.as<double>(), (double*)Tv, 2 * ld, cols, n, K, 1.0, s);
+  (void)nsys;
+}
+
+int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, long ld_out, double tr2,
+              int* unconv_host) {
+  cudaStream_t s = c->stream;
+  const int npw = c->npw, nocc = c->nocc, npv = c->npv, N = c->nr;
+  const int nsys = mb * nocc;
+  const long ld = npw;
+  const int K = 2 * npw;
+  const int mp = (mb + 1) / 2;
+  // item tables: perturbation pairs and (perturbation, band pair)
+  std::vector<int2> ipp, ipk;
+  pair_items(ipp, 0, mb);
+  for (int p = 0; p < mb; ++p) pair_items(ipk, p * nocc, nocc);
+  WB_CU(cudaMemcpyAsync(c->items_pp.p, ipp.data(), sizeof(int2) * ipp.size(), cudaMemcpyHostToDevice, s));
+  WB_CU(cudaMemcpyAsync(c->items_pk.p, ipk.data(), sizeof(int2) * ipk.size(), cudaMemcpyHostToDevice, s));
+  double2* aux = c->aux.as<double2>();
+  double2* B = c->B.as<double2>();
+  double2* X = c->X.as<double2>();
+  double2* G = c->G.as<double2>();
+  double2* T = c->T.as<double2>();
+  double2* stk = c->sticks.as<double2>();
+  fill_columns(c->et.as<double>(), nocc, nsys, c->ecol.as<double>(), s);
+  fill_columns(c->eprec.as<double>(), nocc, nsys, c->epcol.as<double>(), s);
+  // 1. aux = sqvc * dvg in internal order            (apply_operator.f90:49-53)
+  permute_scale(dvg, ld_in, c->perm.as<int>(), c->sqvc.as<double>(), npw, mb, aux, ld, s);
+  // 2. dv(r) of perturbation pairs                   (dfpt_module.f90:235)
+  fft_zinv(c->fa, aux, ld, c->items_pp.as<int2>(), mp, stk);
+  fft_plane_inv_box(c->fa, stk, mp, c->dvbox.as<double2>());
+  // 3. dvpsi = P_G[psi_v(r) dv(r)]                    (dfpt_module.f90:245-278)
+  fft_plane_rhs(c->fa, c->evcr.as<double2>(), c->dvbox.as<double2>(), npv, mb, stk);
+  fft_zfwd_store(c->fa, stk, c->items_pk.as<int2>(), mb * npv, B, ld);
+  c->stats.fft_boxes += mp + (long long)mb * npv;
+  // 4. dvpsi <- -Pc dvpsi = -dvpsi + evc (evc^T dvpsi)  (dfpt_module.f90:346)
+  const double* Wevc = c->W.as<double>() + (size_t)c->nkb * K;
+  const int nsplit = gemm_tn_splits(c->nproj, nsys, K);
+  gemm_tn(Wevc, K, nocc, (const double*)B, 2 * ld, nullptr, nsys, K, nsplit, c->part.as<double>(), s);
+  gamma_reduce(c->part.as<double>(), nsplit, nocc, nsys, Wevc, K, (const double*)B, 2 * ld, nullptr, nullptr, 0, 1.0,
+               c->C.as<double>(), s);
+  gemm_nn(Wevc, K, nocc, c->C.as<double>(), (double*)B, 2 * ld, nullptr, nsys, K, -1.0, s);
+  // 5. dpsi = precondition(dvpsi)                    (dfpt_module.f90:348)
+  precondition(B, X, c->g2kin.as<double>(), c->epcol.as<double>(), npw, nsys, ld, s);
+  // 6. PCG                                           (dfpt_module.f90:350-361)
+  int iters = 0;
+  if (tr2 >= 0.0) {
+    unsigned char* conv = c->conv.as<unsigned char>();
+    int* act = c->act.as<int>();
+    int2* items = c->items.as<int2>();
+    cg_reset(conv, nsys, s);
+    cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+    apply_A(c, X, T, act, items, nsys, nsys, nsplit);            // :127
+    sub_into(T, B, G, npw, nsys, ld, s);                         // :130-138
+    int nact = nsys;
+    for (int it = 1; it <= c->maxiter; ++it) {                   // :146
+      cg_prec_rho(act, nact, G, B, c->g2kin.as<double>(), c->epcol.as<double>(), c->rho.as<double>(), conv, it, tr2,
+                  npw, ld, s);
+      cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+      WB_CU(cudaStreamSynchronize(s));
+      nact = *c->nact_host;
+      iters = it;
+      if (nact == 0) break;                                      // :222
+      c->stats.cg_active_sum += nact;
+      apply_A(c, B, T, act, items, nact, nsys, nsplit);          // :251
+      cg_update(act, nact, X, G, B, T, npw, ld, s);              // :253-329
+    }
+    count_unconverged(conv, nocc, mb, c->unconv.as<int>(), s);
+  } else {
+    WB_CU(cudaMemsetAsync(c->unconv.p, 0, sizeof(int) * mb, s));
+  }
+  c->stats.cg_iterations = std::max(c->stats.cg_iterations, iters);
+  // 7. drho and dng                                   (dfpt_module.f90:403-487)
+  fft_zinv(c->fa, X, ld, c->items_pk.as<int2>(), mb * npv, stk);
+  const double scale = 2.0 * c->wk / c->omega / ((double)N * N * N);
+  fft_plane_drho(c->fa, stk, c->evcr.as<double2>(), c->occ.as<double>(), nocc, mb, c->acc.as<double2>(), scale,
+                 c->sticks2.as<double2>());
+  fft_zfwd_dng(c->fa, c->sticks2.as<double2>(), c->items_pp.as<int2>(), mp, dng, ld_out, c->perm.as<int>(),
+               c->sqvc.as<double>());
+  c->stats.fft_boxes += (long long)mb * npv + mp;
+  if (unconv_host) WB_CU(cudaMemcpyAsync(unconv_host, c->unconv.p, sizeof(int) * mb, cudaMemcpyDeviceToHost, s));
+  return WB_OK;
+}
+
+int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng, double tr2, int iq,
+               int* unconverged, bool on_device) {
+  g_err.clear();
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  if (m < 0) return fail(WB_ERR_ARG, "m < 0");
+  if (iq != 1) return fail(WB_ERR_UNSUPPORTED, "only iq = 1 (Gamma) is provided");
+  if (m > 0 && (!dvg || !dng)) return fail(WB_ERR_ARG, "null dvg or dng");
+  if (ld_dvg < c->npw || ld_dng < c->npw) return fail(WB_ERR_ARG, "leading dimension smaller than npw");
+  if (std::isnan(tr2)) return fail(WB_ERR_ARG, "tr2 is NaN");
+  if (c->precision != WB_PRECISION_FP64) return fail(WB_ERR_UNSUPPORTED, "mixed precision is not built yet");
+  WB_CU(cudaSetDevice(c->device));
+  c->stats = wb_stats{};
+  c->stats.m = m;
+  if (m == 0) return WB_OK;
+  cudaStream_t s = c->stream;
+  WB_CU(cudaEventRecord(c->ev0, s));
+  const int mb = choose_batch(c, m);
+  int rc = ensure_workspace(c, mb, on_device ? 1 : ld_dvg, on_device ? 1 : ld_dng);
+  if (rc) return rc;
+  std::vector<int> unc(m, 0);
+  std::vector<int> tmp(mb);
+  for (int p0 = 0; p0 < m; p0 += mb) {
+    const int nb = std::min(mb, m - p0);
+    const double2* din;
+    double2* dout;
+    if (on_device) {
+      din = reinterpret_cast<const double2*>(dvg) + (size_t)p0 * ld_dvg;
+      dout = reinterpret_cast<double2*>(dng) + (size_t)p0 * ld_dng;
+    } else {
+      WB_CU(cudaMemcpyAsync(c->dvg_in.p, dvg + 2 * (size_t)p0 * ld_dvg, sizeof(double2) * (size_t)ld_dvg * nb,
+                            cudaMemcpyHostToDevice, s));
+      din = c->dvg_in.as<double2>();
+      dout = c->dng_out.as<double2>();
+    }
+    // rows >= npw of dng are zero (apply_operator.f90:44, dng = 0)
+    if (ld_dng > c->npw)
+      WB_CU(cudaMemset2DAsync(dout + c->npw, sizeof(double2) * ld_dng, 0, sizeof(double2) * (ld_dng - c->npw), nb, s));
+    rc = run_batch(c, nb, din, ld_dvg, dout, ld_dng, tr2, tmp.data());
+    if (rc) return rc;
+    if (!on_device)
+      WB_CU(cudaMemcpyAsync(dng + 2 * (size_t)p0 * ld_dng, c->dng_out.p, sizeof(double2) * (size_t)ld_dng * nb,
+                            cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaStreamSynchronize(s));
+    for (int p = 0; p < nb; ++p) unc[p0 + p] = tmp[p];
+  }
+  WB_CU(cudaEventRecord(c->ev1, s));
+  WB_CU(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->stats.ms_total = ms;
+  WB_CU(cudaGetLastError());
+  if (unconverged) std::memcpy(unconverged, unc.data(), sizeof(int) * m);
+  return WB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wb_version(void) { return 100; }
+
+const char* wb_last_error(void) { return g_err.c_str(); }
+
+int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
+  g_err.clear();
+  if (!out || !s) return fail(WB_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (s->npw <= 0 || s->npwx < s->npw) return fail(WB_ERR_ARG, "need 0 < npw <= npwx");
+  if (s->nr1 != s->nr2 || s->nr1 != s->nr3) return fail(WB_ERR_UNSUPPORTED, "only cubic FFT boxes are provided");
+  if (!fft_supported(s->nr1)) return fail(WB_ERR_UNSUPPORTED, "FFT edge " + std::to_string(s->nr1) + " not provided");
+  if (s->nbnd_occ <= 0 || s->nkb < 0) return fail(WB_ERR_ARG, "bad nbnd_occ or nkb");
+  if (s->gstart != 2) return fail(WB_ERR_UNSUPPORTED, "gstart must be 2 (G=0 on this process)");
+  if (s->n_dfpt_maxiter < 0) return fail(WB_ERR_ARG, "n_dfpt_maxiter < 0");
+  if (!s->nl || !s->nlm || !s->g2kin || !s->vrs || !s->evc || !s->et || !s->occupation || !s->sqvc ||
+      (s->nkb > 0 && (!s->vkb || !s->deeq)))
+    return fail(WB_ERR_ARG, "null system array");
+  if (!(s->omega > 0.0)) return fail(WB_ERR_ARG, "omega must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return fail(WB_ERR_CUDA, "no CUDA device " + std::to_string(device));
+  }
+  wb_ctx* c = new wb_ctx();
+  c->device = device;
+  auto bail = [&](int code) {
+    wb_ctx_destroy(c);
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return bail(fail(WB_ERR_CUDA, "cudaSetDevice failed"));
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaMallocHost(&c->nact_host, sizeof(int) * 4) != cudaSuccess)
+    return bail(fail(WB_ERR_CUDA, "stream/event creation failed"));
+  c->npw = s->npw;
+  c->nr = s->nr1;
+  c->nnr = s->nr1 * s->nr2 * s->nr3;
+  c->nocc = s->nbnd_occ;
+  c->nkb = s->nkb;
+  c->nproj = s->nkb + s->nbnd_occ;
+  c->npv = (s->nbnd_occ + 1) / 2;
+  c->maxiter = s->n_dfpt_maxiter;
+  c->kinetic_only = s->l_kinetic_only;
+  c->omega = s->omega;
+  c->wk = s->wk;
+  c->alpha = s->alpha_pv;
+  std::vector<int> perm;
+  int rc = build_tables(c, s, perm);
+  if (rc) return bail(rc);
+  const int N = c->nr, npw = c->npw;
+  // twiddles exp(+2 pi i j / N), accurate host values
+  std::vector<double2> tw(N);
+  for (int j = 0; j < N; ++j) {
+    const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)j / (long double)N;
+    tw[j] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  std::vector<double> g2(npw), sq(npw);
+  for (int i = 0; i < npw; ++i) { g2[i] = s->g2kin[perm[i]]; sq[i] = s->sqvc[perm[i]]; }
+  std::vector<double> vsc(c->nnr);
+  for (int i = 0; i < c->nnr; ++i) vsc[i] = s->vrs[i] / (double)c->nnr;
+  if ((rc = upload(tw.data(), N, c->tw)) || (rc = upload(g2.data(), npw, c->g2kin)) ||
+      (rc = upload(sq.data(), npw, c->sqvc)) || (rc = upload(vsc.data(), c->nnr, c->vs)) ||
+      (rc = upload(s->et, c->nocc, c->et)) || (rc = upload(s->occupation, c->nocc, c->occ)))
+    return bail(rc);
+  if ((rc = upload_cols(s->evc, s->npwx, c->nocc, perm, c->evc))) return bail(rc);
+  // W = [vkb | evc] as real columns of length 2 npw
+  {
+    std::vector<double2> w((size_t)npw * c->nproj);
+    for (int j = 0; j < c->nproj; ++j) {
+      const double* src = j < c->nkb ? s->vkb + 2 * (size_t)j * s->npwx : s->evc + 2 * (size_t)(j - c->nkb) * s->npwx;
+      for (int i = 0; i < npw; ++i) w[(size_t)j * npw + i] = make_double2(src[2 * perm[i]], src[2 * perm[i] + 1]);
+    }
+    if ((rc = upload(w.data(), w.size(), c->W))) return bail(rc);
+    std::vector<double> dd(std::max(1, c->nkb * c->nkb), 0.0);
+    if (c->nkb) std::memcpy(dd.data(), s->deeq, sizeof(double) * c->nkb * c->nkb);
+    if ((rc = upload(dd.data(), dd.size(), c->D))) return bail(rc);
+  }
+  fft_setup(N);
+  c->fa.n = N;
+  c->fa.st = c->st;
+  c->fa.tw = c->tw.as<double2>();
+  c->fa.stream = c->stream;
+  // eprec (set_eprec.f90) and psi_v(r) for all occupied bands, in pairs
+  if (c->eprec.ensure(sizeof(double) * c->nocc) || c->evcr.ensure(sizeof(double2) * (size_t)c->nnr * c->npv) ||
+      c->iota_items.ensure(sizeof(int2) * c->npv) ||
+      c->sticks.ensure(sizeof(double2) * (size_t)N * c->st.nst * c->npv))
+    return bail(fail(WB_ERR_NOMEM, "device allocation failed"));
+  set_eprec(c->evc.as<double2>(), c->g2kin.as<double>(), npw, c->nocc, c->eprec.as<double>(), c->stream);
+  std::vector<int2> ib;
+  pair_items(ib, 0, c->nocc);
+  if (cudaMemcpy(c->iota_items.p, ib.data(), sizeof(int2) * ib.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(WB_ERR_CUDA, "upload failed"));
+  fft_zinv(c->fa, c->evc.as<double2>(), npw, c->iota_items.as<int2>(), c->npv, c->sticks.as<double2>());
+  fft_plane_inv_box(c->fa, c->sticks.as<double2>(), c->npv, c->evcr.as<double2>());
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return bail(fail(WB_ERR_CUDA, std::string("context setup: ") + cudaGetErrorString(e)));
+  *out = c;
+  return WB_OK;
+}
+
+int wb_ctx_destroy(wb_ctx* c) {
+  if (!c) return WB_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  DBuf* bufs[] = {&c->perm, &c->gqz, &c->spg, &c->stpos, &c->tw, &c->g2kin, &c->sqvc, &c->vs, &c->evc, &c->W,
+                  &c->D, &c->eprec, &c->et, &c->occ, &c->evcr, &c->dvg_in, &c->dng_out, &c->aux, &c->dvbox, &c->B,
+                  &c->X, &c->G, &c->T, &c->sticks, &c->sticks2, &c->acc, &c->part, &c->C, &c->rho, &c->conv,
+                  &c->act, &c->items, &c->nact, &c->ecol, &c->epcol, &c->unconv, &c->items_pp, &c->items_pk,
+                  &c->iota_items};
+  for (DBuf* b : bufs) b->release();
+  if (c->nact_host) cudaFreeHost(c->nact_host);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return WB_OK;
+}
+
+int wb_apply_operator(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng, double tr2, int iq,
+                      int* unconverged) {
+  return apply_impl(c, m, dvg, ld_dvg, dng, ld_dng, tr2, iq, unconverged, false);
+}
+
+int wb_apply_operator_device(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng, double tr2,
+                             int iq, int* unconverged) {
+  return apply_impl(c, m, dvg, ld_dvg, dng, ld_dng, tr2, iq, unconverged, true);
+}
+
+int wb_set_precision(wb_ctx* c, int mode) {
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  if (mode == WB_PRECISION_FP64) { c->precision = mode; return WB_OK; }
+  if (mode == WB_PRECISION_MIXED) return fail(WB_ERR_UNSUPPORTED, "mixed precision is not built yet");
+  return fail(WB_ERR_ARG, "unknown precision mode");
+}
+
+int wb_set_batch(wb_ctx* c, int maxp) {
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  if (maxp < 0) return fail(WB_ERR_ARG, "negative batch");
+  c->batch_cap = maxp;
+  return WB_OK;
+}
+
+int wb_get_stats(const wb_ctx* c, wb_stats* out) {
+  if (!c || !out) return fail(WB_ERR_ARG, "null argument");
+  *out = c->stats;
+  return WB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// Shared-memory / register FFT engine for the stick-and-plane 3D FFTs.
+//
+// A length-N line transform is split N = N1 * N2 (four-step):
+//   step 1: N2 threads per line, each does an N1-point DFT in registers over
+//           elements N2*n1 + n2, multiplies by W_N^(n2*k1) and writes back to
+//           the same positions (thread-private, no barrier needed);
+//   step 2: N1 threads per line, each reads N2 consecutive results, does an
+//           N2-point DFT in registers and writes element k1 + N1*k2 (natural
+//           order).  Reads and writes of one line overlap, so a barrier
+//           separates them.
+// The small DFTs (2, 3, 4, 5 and composites up to 16) are fully unrolled
+// register code.  Twiddles W_N^j = exp(+2 pi i j / N) come from a per-N table
+// in shared memory (computed on the host); DIR = +1 is QE's invfft sign,
+// DIR = -1 the fwfft sign.  No normalisation is applied here.
+#pragma once
+#include "wb_common.cuh"
+
+namespace wb {
+
+template <int N> struct FftSplit;
+template <> struct FftSplit<16> { static constexpr int N1 = 4, N2 = 4; };
+template <> struct FftSplit<20> { static constexpr int N1 = 5, N2 = 4; };
+template <> struct FftSplit<24> { static constexpr int N1 = 6, N2 = 4; };
+template <> struct FftSplit<32> { static constexpr int N1 = 8, N2 = 4; };
+template <> struct FftSplit<36> { static constexpr int N1 = 6, N2 = 6; };
+template <> struct FftSplit<40> { static constexpr int N1 = 8, N2 = 5; };
+template <> struct FftSplit<48> { static constexpr int N1 = 8, N2 = 6; };
+template <> struct FftSplit<60> { static constexpr int N1 = 10, N2 = 6; };
+template <> struct FftSplit<64> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct FftSplit<72> { static constexpr int N1 = 8, N2 = 9; };
+template <> struct FftSplit<80> { static constexpr int N1 = 8, N2 = 10; };
+template <> struct FftSplit<96> { static constexpr int N1 = 8, N2 = 12; };
+template <> struct FftSplit<100> { static constexpr int N1 = 10, N2 = 10; };
+template <> struct FftSplit<108> { static constexpr int N1 = 12, N2 = 9; };
+template <> struct FftSplit<120> { static constexpr int N1 = 12, N2 = 10; };
+
+// Literal constants of the radix-3 and radix-5 butterflies.
+constexpr double kS3 = 0.86602540378443864676;   // sin(2 pi / 3)
+constexpr double kC51 = 0.30901699437494742410;  // cos(2 pi / 5)
+constexpr double kC52 = -0.80901699437494742410; // cos(4 pi / 5)
+constexpr double kS51 = 0.95105651629515357212;  // sin(2 pi / 5)
+constexpr double kS52 = 0.58778525229247312917;  // sin(4 pi / 5)
+
+template <int R> struct Factor2;  // composite radices R = A * B
+template <> struct Factor2<6> { static constexpr int A = 3, B = 2; };
+template <> struct Factor2<8> { static constexpr int A = 4, B = 2; };
+template <> struct Factor2<9> { static constexpr int A = 3, B = 3; };
+template <> struct Factor2<10> { static constexpr int A = 5, B = 2; };
+template <> struct Factor2<12> { static constexpr int A = 4, B = 3; };
+template <> struct Factor2<16> { static constexpr int A = 4, B = 4; };
+
+// In-register DFT of size R: v[k] <- sum_n v[n] exp(DIR 2 pi i n k / R).
+// NT is the length of the shared twiddle table twN (R divides NT).
+template <int R, int DIR, int NT>
+WB_DEV void rdft(double2* v, const double2* twN) {
+  if constexpr (R == 1) {
+    return;
+  } else if constexpr (R == 2) {
+    double2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 3) {
+    double2 t1 = cadd(v[1], v[2]);
+    double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
+    double2 d = csub(v[1], v[2]);
+    double2 t3 = cmul_i<DIR>(make_double2(kS3 * d.x, kS3 * d.y));
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+  } else if constexpr (R == 4) {
+    double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+    double2 c = cadd(v[1], v[3]), d = cmul_i<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(a, c);
+    v[2] = csub(a, c);
+    v[1] = cadd(b, d);
+    v[3] = csub(b, d);
+  } else if constexpr (R == 5) {
+    double2 x0 = v[0];
+    double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    double2 a1 = make_double2(x0.x + kC51 * t1.x + kC52 * t2.x, x0.y + kC51 * t1.y + kC52 * t2.y);
+    double2 a2 = make_double2(x0.x + kC52 * t1.x + kC51 * t2.x, x0.y + kC52 * t1.y + kC51 * t2.y);
+    double2 b1 = cmul_i<DIR>(make_double2(kS51 * t3.x + kS52 * t4.x, kS51 * t3.y + kS52 * t4.y));
+    double2 b2 = cmul_i<DIR>(make_double2(kS52 * t3.x - kS51 * t4.x, kS52 * t3.y - kS51 * t4.y));
+    v[0] = cadd(x0, cadd(t1, t2));
+    v[1] = cadd(a1, b1);
+    v[4] = csub(a1, b1);
+    v[2] = cadd(a2, b2);
+    v[3] = csub(a2, b2);
+  } else {
+    constexpr int A = Factor2<R>::A, B = Factor2<R>::B;
+    double2 z[B][A];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+#pragma unroll
+      for (int a = 0; a < A; ++a) z[b][a] = v[B * a + b];
+      rdft<A, DIR, NT>(z[b], twN);
+#pragma unroll
+      for (int k1 = 1; k1 < A; ++k1)
+        if (b > 0) z[b][k1] = ctw<DIR>(z[b][k1], twN[((b * k1) * (NT / R)) % NT]);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      double2 t[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) t[b] = z[b][k1];
+      rdft<B, DIR, NT>(t, twN);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = t[k2];
+    }
+  }
+}
+
+// Batched line FFTs in shared memory.  Line l starts at data + off(l) and has
+// element stride es.  LINE_FAST puts consecutive threads on consecutive lines
+// (use it when lines are adjacent in memory, e.g. columns of a row-major
+// plane); otherwise consecutive threads walk along one line.
+// Must be called by all NT threads of the block (contains barriers).
+template <int N, int DIR, int NT, bool LINE_FAST, class Off>
+WB_DEV void fft_lines(double2* data, Off off, int es, int nlines, const double2* twN) {
+  constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
+  const int tid = threadIdx.x;
+  // step 1: N1-point DFTs, thread-private
+  const int items1 = nlines * N2;
+  for (int it = tid; it < items1; it += NT) {
+    int line, n2;
+    if (LINE_FAST) { line = it % nlines; n2 = it / nlines; }
+    else { line = it / N2; n2 = it % N2; }
+    double2* p = data + off(line);
+    double2 v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = p[(N2 * n1 + n2) * es];
+    rdft<N1, DIR, N>(v, twN);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = ctw<DIR>(v[k1], twN[(n2 * k1) % N]);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) p[(N2 * k1 + n2) * es] = v[k1];
+  }
+  __syncthreads();
+  // step 2: N2-point DFTs, one line's N1 work items inside one chunk
+  constexpr int LPC = NT / N1;
+  const int nchunks = (nlines + LPC - 1) / LPC;
+  for (int c = 0; c < nchunks; ++c) {
+    int line, k1;
+    if (LINE_FAST) { line = c * LPC + tid % LPC; k1 = tid / LPC; }
+    else { line = c * LPC + tid / N1; k1 = tid % N1; }
+    const bool act = (tid < LPC * N1) && (line < nlines);
+    double2 v[N2];
+    double2* p = data + (act ? off(line) : 0);
+    if (act) {
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) v[n2] = p[(N2 * k1 + n2) * es];
+      rdft<N2, DIR, N>(v, twN);
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) p[(k1 + N1 * k2) * es] = v[k2];
+    }
+  }
+  __syncthreads();
+}
+
+struct OffLinear {
+  int stride;
+  WB_DEV int operator()(int l) const { return l * stride; }
+};
+// Active columns of a plane: x in [0, xhi] and [N - xlo, N).
+struct OffCols {
+  int nlow, n;  // nlow = xhi + 1 columns from 0, the rest from n - (ncols - nlow)
+  int ncols;
+  WB_DEV int operator()(int l) const { return l < nlow ? l : n - ncols + l; }
+};
+
+}  // namespace wb

@@ -1,0 +1,453 @@
+// Stick-and-plane 3D FFTs of the Gamma-only response operator.
+//
+// The G sphere is cut into sticks along z.  A "stick pair" is the stick at
+// (x, y) of the stored half sphere together with its mirror at (-x, -y), which
+// holds the -G partners; the (0,0) stick is its own mirror.  Inside the
+// library G vectors are ordered stick pair by stick pair, z ascending, so
+// every stick pair reads one contiguous run of coefficients.
+//
+// One complex 3D FFT carries two real functions (FFT_kernel/fft_at_gamma.f90):
+//   inverse: box(+G) = a1 + i a2, box(-G) = conj(a1 - i a2)          (:55-64)
+//   forward: fp = (A(G) + A(-G))/2, fm = (A(G) - A(-G))/2,
+//            b1 = (Re fp, Im fm), b2 = (Im fp, -Re fm)                 (:98-111)
+// Both are fused into the z-pass kernels.  The x-y passes run one plane per
+// CTA in shared memory, with the pointwise work of the caller (local
+// potential, RHS product, density accumulation) fused between the inverse and
+// forward transforms.
+//
+// Stick buffer layout: [item][z][stick], stick = 2q and 2q+1 for the two
+// sticks of pair q; stick 1 (mirror slot of (0,0)) is a dummy that is never
+// scattered.  g_qz of a stored G is (2q + side, z), side = which of the two
+// sticks of the pair holds it.
+#include "wb_fft.cuh"
+#include "wb_internal.h"
+
+namespace wb {
+
+constexpr int ZSG = 16;     // stick pairs per CTA in the z passes
+constexpr int ZNT = 256;
+constexpr int PNT = 256;
+
+template <int N>
+WB_DEV void load_tw(double2* tw, const double2* twg) {
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
+}
+
+// ---------------------------------------------------------------------------
+// z pass, inverse: sphere coefficients of a pair of columns -> sticks
+// ---------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, long ld,
+                                              const int2* __restrict__ items, StickTab st,
+                                              double2* __restrict__ out,
+                                              const double2* __restrict__ twg) {
+  constexpr int LS = N + 1;  // padded line stride (odd: conflict-free column reads)
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* zb = sm + N;
+  const int item = blockIdx.y;
+  const int q0 = blockIdx.x * ZSG;
+  const int nq = min(ZSG, st.nsp - q0);
+  load_tw<N>(tw, twg);
+  for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  const int2 it = items[item];
+  const double2* a = src + (long)it.x * ld;
+  const double2* b = src + (long)(it.y >= 0 ? it.y : it.x) * ld;
+  const bool two = it.y >= 0;
+  const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
+  for (int g = g0 + threadIdx.x; g < g1; g += ZNT) {
+    const int2 qz = st.g_qz[g];
+    const double2 a1 = a[g];
+    const double2 a2 = two ? b[g] : make_double2(0.0, 0.0);
+    // pos = a1 + i a2 ; neg = conj(a1 - i a2)
+    const double2 pos = make_double2(a1.x - a2.y, a1.y + a2.x);
+    const double2 neg = make_double2(a1.x + a2.y, a2.x - a1.y);
+    const int z = qz.y;
+    if (qz.x < 2) {  // the (0,0) stick is its own mirror
+      if (z != 0) { zb[(z + N) % N] = pos; zb[(N - z) % N] = neg; }
+      else zb[0] = neg;  // G = 0: the -G store wins, as in the reference loop
+    } else {
+      const int l = qz.x - 2 * q0;  // slot of the stick holding G; its mirror is l ^ 1
+      zb[l * LS + ((z + N) % N)] = pos;
+      zb[(l ^ 1) * LS + ((N - z) % N)] = neg;
+    }
+  }
+  __syncthreads();
+  fft_lines<N, +1, ZNT, false>(zb, OffLinear{LS}, 1, 2 * nq, tw);
+  const int ns = 2 * nq;
+  double2* o = out + (long)item * N * st.nst + 2 * q0;
+  for (int e = threadIdx.x; e < ns * N; e += ZNT) {
+    const int s = e % ns, z = e / ns;
+    o[(long)z * st.nst + s] = zb[s * LS + z];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass, forward: sticks -> sphere with the Gamma unpack, then an epilogue
+// ---------------------------------------------------------------------------
+template <int N, class Epi>
+__global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks,
+                                              const int2* __restrict__ items, StickTab st,
+                                              const double2* __restrict__ twg, Epi epi) {
+  constexpr int LS = N + 1;
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* zb = sm + N;
+  const int item = blockIdx.y;
+  const int q0 = blockIdx.x * ZSG;
+  const int nq = min(ZSG, st.nsp - q0);
+  const int ns = 2 * nq;
+  load_tw<N>(tw, twg);
+  const double2* s0 = sticks + (long)item * N * st.nst + 2 * q0;
+  for (int e = threadIdx.x; e < ns * N; e += ZNT) {
+    const int s = e % ns, z = e / ns;
+    zb[s * LS + z] = s0[(long)z * st.nst + s];
+  }
+  __syncthreads();
+  fft_lines<N, -1, ZNT, false>(zb, OffLinear{LS}, 1, ns, tw);
+  const int2 it = items[item];
+  const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
+  for (int g = g0 + threadIdx.x; g < g1; g += ZNT) {
+    const int2 qz = st.g_qz[g];
+    const int z = qz.y;
+    double2 ap, am;
+    if (qz.x < 2) {
+      ap = zb[(z + N) % N];
+      am = zb[(N - z) % N];
+    } else {
+      const int l = qz.x - 2 * q0;
+      ap = zb[l * LS + ((z + N) % N)];
+      am = zb[(l ^ 1) * LS + ((N - z) % N)];
+    }
+    const double2 fp = make_double2(0.5 * (ap.x + am.x), 0.5 * (ap.y + am.y));
+    const double2 fm = make_double2(0.5 * (ap.x - am.x), 0.5 * (ap.y - am.y));
+    epi(g, it, make_double2(fp.x, fm.y), make_double2(fp.y, -fm.x));
+  }
+}
+
+struct EpiStore {
+  double2* dst;
+  long ld;
+  WB_DEV void operator()(int g, int2 it, double2 b1, double2 b2) const {
+    dst[(long)it.x * ld + g] = b1;
+    if (it.y >= 0) dst[(long)it.y * ld + g] = b2;
+  }
+};
+
+// T = (V psi + g2kin psi with Im(G=0) = 0) - e psi   (h_psi then
+// apply_sternheimerop_to_m_wfcs.f90:65-74; KB and alpha Pv follow as GEMMs)
+struct EpiHpsi {
+  const double2* P;
+  double2* T;
+  long ld;
+  const double* g2kin;
+  const double* ecol;
+  WB_DEV void one(int g, int c, double2 vp) const {
+    const double2 p = P[(long)c * ld + g];
+    const double k = g2kin[g];
+    double2 h = make_double2(fma(k, p.x, vp.x), fma(k, p.y, vp.y));
+    if (g == 0) h.y = 0.0;
+    const double e = ecol[c];
+    T[(long)c * ld + g] = make_double2(fma(-e, p.x, h.x), fma(-e, p.y, h.y));
+  }
+  WB_DEV void operator()(int g, int2 it, double2 b1, double2 b2) const {
+    one(g, it.x, b1);
+    if (it.y >= 0) one(g, it.y, b2);
+  }
+};
+
+// dng(perm(g), p) = sqvc(g) * drho_G(g), G = 0 zeroed
+// (dfpt_module.f90:485-487,502-503 and apply_operator.f90:63-67)
+struct EpiDng {
+  double2* dng;
+  long ld;
+  const int* perm;
+  const double* sqvc;
+  WB_DEV void operator()(int g, int2 it, double2 b1, double2 b2) const {
+    const double s = (g == 0) ? 0.0 : sqvc[g];
+    const long r = perm[g];
+    dng[(long)it.x * ld + r] = make_double2(s * b1.x, s * b1.y);
+    if (it.y >= 0) dng[(long)it.y * ld + r] = make_double2(s * b2.x, s * b2.y);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// x-y plane passes
+// ---------------------------------------------------------------------------
+template <int N>
+WB_DEV void plane_zero(double2* pl) {
+  for (int e = threadIdx.x; e < N * N; e += PNT) pl[e] = make_double2(0.0, 0.0);
+}
+WB_DEV void plane_scatter(double2* pl, const double2* __restrict__ sz, const int* __restrict__ pos, int nst) {
+  for (int s = threadIdx.x; s < nst; s += PNT) {
+    const int p = pos[s];
+    if (p >= 0) pl[p] = sz[s];
+  }
+}
+WB_DEV void plane_gather(const double2* pl, double2* __restrict__ sz, const int* __restrict__ pos, int nst) {
+  for (int s = threadIdx.x; s < nst; s += PNT) {
+    const int p = pos[s];
+    sz[s] = p >= 0 ? pl[p] : make_double2(0.0, 0.0);
+  }
+}
+template <int N, int DIR>
+WB_DEV void plane_fft_cols(double2* pl, const StickTab& st, const double2* tw) {
+  fft_lines<N, DIR, PNT, true>(pl, OffCols{st.xhi + 1, N, st.ncols}, N, st.ncols, tw);
+}
+template <int N, int DIR>
+WB_DEV void plane_fft_rows(double2* pl, const double2* tw) {
+  fft_lines<N, DIR, PNT, false>(pl, OffLinear{N}, 1, N, tw);
+}
+
+// psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma)
+template <int N>
+__global__ void __launch_bounds__(PNT) k_plane_vloc(double2* __restrict__ sticks, StickTab st,
+                                                    const double* __restrict__ vs,
+                                                    const double2* __restrict__ twg) {
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* pl = sm + N;
+  const int z = blockIdx.x, item = blockIdx.y;
+  double2* sz = sticks + ((long)item * N + z) * st.nst;
+  load_tw<N>(tw, twg);
+  plane_zero<N>(pl);
+  __syncthreads();
+  plane_scatter(pl, sz, st.st_pos, st.nst);
+  __syncthreads();
+  plane_fft_cols<N, +1>(pl, st, tw);
+  plane_fft_rows<N, +1>(pl, tw);
+  const double* v = vs + (long)z * N * N;
+  for (int e = threadIdx.x; e < N * N; e += PNT) pl[e] = cscale(pl[e], v[e]);
+  __syncthreads();
+  plane_fft_rows<N, -1>(pl, tw);
+  plane_fft_cols<N, -1>(pl, st, tw);
+  plane_gather(pl, sz, st.st_pos, st.nst);
+}
+
+// sticks -> full real-space box (complex: two real functions), no scaling
+template <int N>
+__global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict__ sticks, StickTab st,
+                                                       double2* __restrict__ box,
+                                                       const double2* __restrict__ twg) {
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* pl = sm + N;
+  const int z = blockIdx.x, item = blockIdx.y;
+  const double2* sz = sticks + ((long)item * N + z) * st.nst;
+  load_tw<N>(tw, twg);
+  plane_zero<N>(pl);
+  __syncthreads();
+  plane_scatter(pl, sz, st.st_pos, st.nst);
+  __syncthreads();
+  plane_fft_cols<N, +1>(pl, st, tw);
+  plane_fft_rows<N, +1>(pl, tw);
+  double2* o = box + ((long)item * N + z) * N * N;
+  for (int e = threadIdx.x; e < N * N; e += PNT) o[e] = pl[e];
+}
+
+// RHS of the Sternheimer equation, dfpt_module.f90:245-260:
+// (psi_v1(r) + i psi_v2(r)) * dv_p(r) / N^3 -> forward -> sticks
+template <int N>
+__global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ evcr,
+                                                   const double2* __restrict__ dvbox, int npv,
+                                                   StickTab st, double2* __restrict__ sticks,
+                                                   const double2* __restrict__ twg) {
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* pl = sm + N;
+  const int z = blockIdx.x, k = blockIdx.y, p = blockIdx.z;
+  load_tw<N>(tw, twg);
+  const double2* ps = evcr + ((long)k * N + z) * N * N;
+  const double2* dv = dvbox + ((long)(p >> 1) * N + z) * N * N;
+  const bool hi = p & 1;
+  constexpr double inv = 1.0 / ((double)N * N * N);
+  for (int e = threadIdx.x; e < N * N; e += PNT) {
+    const double2 d = dv[e];
+    const double w = (hi ? d.y : d.x) * inv;
+    pl[e] = cscale(ps[e], w);
+  }
+  __syncthreads();
+  plane_fft_rows<N, -1>(pl, tw);
+  plane_fft_cols<N, -1>(pl, st, tw);
+  const long item = (long)p * npv + k;
+  plane_gather(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+}
+
+// Density response, dfpt_module.f90:403-423 and :478:
+// drho_p(r) = sum_v occ_v psi_v(r) dpsi_v(r), two perturbations per CTA,
+// then (drho_p1 + i drho_p2) * scale -> forward -> sticks.
+// acc is per-CTA scratch in global memory ([pp][z][N*N] double2), owned
+// element-wise by the thread that writes it.
+template <int N>
+__global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ dsticks,
+                                                    const double2* __restrict__ evcr,
+                                                    const double* __restrict__ occ, int nocc,
+                                                    int mb, StickTab st, double2* __restrict__ acc,
+                                                    double scale, double2* __restrict__ osticks,
+                                                    const double2* __restrict__ twg) {
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* pl = sm + N;
+  const int z = blockIdx.x, pp = blockIdx.y;
+  const int npv = (nocc + 1) / 2;
+  load_tw<N>(tw, twg);
+  double2* ac = acc + ((long)pp * N + z) * N * N;
+  for (int pi = 0; pi < 2; ++pi) {
+    const int p = 2 * pp + pi;
+    if (p >= mb) {
+      for (int e = threadIdx.x; e < N * N; e += PNT) ac[e].y = 0.0;
+      break;
+    }
+    for (int k = 0; k < npv; ++k) {
+      const long item = (long)p * npv + k;
+      __syncthreads();
+      plane_zero<N>(pl);
+      __syncthreads();
+      plane_scatter(pl, dsticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+      __syncthreads();
+      plane_fft_cols<N, +1>(pl, st, tw);
+      plane_fft_rows<N, +1>(pl, tw);
+      const double o1 = occ[2 * k];
+      const double o2 = (2 * k + 1 < nocc) ? occ[2 * k + 1] : 0.0;
+      const double2* ps = evcr + ((long)k * N + z) * N * N;
+      for (int e = threadIdx.x; e < N * N; e += PNT) {
+        const double2 d = pl[e], s = ps[e];
+        const double c = fma(o1 * s.x, d.x, o2 * s.y * d.y);
+        if (pi == 0) {
+          if (k == 0) ac[e].x = c; else ac[e].x += c;
+        } else {
+          if (k == 0) ac[e].y = c; else ac[e].y += c;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < N * N; e += PNT) pl[e] = cscale(ac[e], scale);
+  __syncthreads();
+  plane_fft_rows<N, -1>(pl, tw);
+  plane_fft_cols<N, -1>(pl, st, tw);
+  plane_gather(pl, osticks + ((long)pp * N + z) * st.nst, st.st_pos, st.nst);
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+template <int N>
+static size_t zsmem() { return sizeof(double2) * (N + 2 * ZSG * (N + 1)); }
+template <int N>
+static size_t psmem() { return sizeof(double2) * (N + N * N); }
+
+template <int N>
+struct FftN {
+  static void setup() {
+    cudaFuncSetAttribute(k_zinv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, EpiHpsi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, EpiDng>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_plane_vloc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    cudaFuncSetAttribute(k_plane_inv_box<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    cudaFuncSetAttribute(k_plane_rhs<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    cudaFuncSetAttribute(k_plane_drho<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+  }
+  static dim3 zgrid(const StickTab& st, int nitems) { return dim3((st.nsp + ZSG - 1) / ZSG, nitems); }
+  static void zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks) {
+    if (nitems <= 0) return;
+    k_zinv<N><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+  }
+  template <class Epi>
+  static void zfwd(const FftArgs& f, const double2* sticks, const int2* items, int nitems, Epi epi) {
+    if (nitems <= 0) return;
+    k_zfwd<N, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
+  }
+  static void vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs) {
+    if (nitems <= 0) return;
+    k_plane_vloc<N><<<dim3(N, nitems), PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+  }
+  static void inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box) {
+    if (nitems <= 0) return;
+    k_plane_inv_box<N><<<dim3(N, nitems), PNT, psmem<N>(), f.stream>>>(sticks, f.st, box, f.tw);
+  }
+  static void rhs(const FftArgs& f, const double2* evcr, const double2* dvbox, int npv, int mb, double2* sticks) {
+    if (mb <= 0) return;
+    k_plane_rhs<N><<<dim3(N, npv, mb), PNT, psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
+  }
+  static void drho(const FftArgs& f, const double2* dsticks, const double2* evcr, const double* occ, int nocc,
+                   int mb, double2* acc, double scale, double2* osticks) {
+    if (mb <= 0) return;
+    k_plane_drho<N><<<dim3(N, (mb + 1) / 2), PNT, psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st,
+                                                                         acc, scale, osticks, f.tw);
+  }
+};
+
+#define WB_FOR_EACH_N(X) X(16) X(20) X(24) X(32) X(36) X(40) X(48) X(60) X(64) X(72) X(80) X(96) X(100) X(108)
+
+bool fft_supported(int n) {
+  switch (n) {
+#define X(n) case n: return true;
+    WB_FOR_EACH_N(X)
+#undef X
+    default: return false;
+  }
+}
+
+void fft_setup(int n) {
+  switch (n) {
+#define X(n) case n: FftN<n>::setup(); break;
+    WB_FOR_EACH_N(X)
+#undef X
+    default: break;
+  }
+}
+
+#define WB_DISPATCH(n, call) \
+  switch (n) {               \
+    WB_FOR_EACH_N(X)         \
+    default: break;          \
+  }
+
+void fft_zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks) {
+#define X(n) case n: FftN<n>::zinv(f, src, ld, items, nitems, sticks); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_zfwd_store(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dst, long ld) {
+#define X(n) case n: FftN<n>::zfwd(f, sticks, items, nitems, EpiStore{dst, ld}); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_zfwd_hpsi(const FftArgs& f, const double2* sticks, const int2* items, int nitems, const double2* P,
+                   double2* T, long ld, const double* g2kin, const double* ecol) {
+#define X(n) case n: FftN<n>::zfwd(f, sticks, items, nitems, EpiHpsi{P, T, ld, g2kin, ecol}); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_zfwd_dng(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dng, long ld,
+                  const int* perm, const double* sqvc) {
+#define X(n) case n: FftN<n>::zfwd(f, sticks, items, nitems, EpiDng{dng, ld, perm, sqvc}); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_plane_vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs) {
+#define X(n) case n: FftN<n>::vloc(f, sticks, nitems, vs); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_plane_inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box) {
+#define X(n) case n: FftN<n>::inv_box(f, sticks, nitems, box); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_plane_rhs(const FftArgs& f, const double2* evcr, const double2* dvbox, int npv, int mb, double2* sticks) {
+#define X(n) case n: FftN<n>::rhs(f, evcr, dvbox, npv, mb, sticks); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_plane_drho(const FftArgs& f, const double2* dsticks, const double2* evcr, const double* occ, int nocc,
+                    int mb, double2* acc, double scale, double2* osticks) {
+#define X(n) case n: FftN<n>::drho(f, dsticks, evcr, occ, nocc, mb, acc, scale, osticks); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+
+}  // namespace wb

@@ -1,0 +1,71 @@
+// Internal interfaces between the west_b200 host code and its kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace wb {
+
+// Stick decomposition of the Gamma half sphere (built on the host from nl).
+struct StickTab {
+  int nsp;               // stick pairs; pair 0 is the (0,0) stick
+  int nst;               // sticks in the buffer = 2 * nsp (stick 1 is a dummy)
+  const int* sp_gstart;  // [nsp + 1] first internal G index of each pair
+  const int2* g_qz;      // [npw] (2 * pair + side, signed z) of each internal G
+  const int* st_pos;     // [nst] plane offset y*N + x of each stick, -1 = dummy
+  int xhi;               // active plane columns: x in [0, xhi] and [N - (ncols - xhi - 1), N)
+  int ncols;
+};
+
+struct FftArgs {
+  int n;                 // box edge
+  StickTab st;
+  const double2* tw;     // [n] exp(+2 pi i j / n)
+  cudaStream_t stream;
+};
+
+bool fft_supported(int n);
+void fft_setup(int n);
+void fft_zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks);
+void fft_zfwd_store(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dst, long ld);
+void fft_zfwd_hpsi(const FftArgs& f, const double2* sticks, const int2* items, int nitems, const double2* P,
+                   double2* T, long ld, const double* g2kin, const double* ecol);
+void fft_zfwd_dng(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dng, long ld,
+                  const int* perm, const double* sqvc);
+void fft_plane_vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs);
+void fft_plane_inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box);
+void fft_plane_rhs(const FftArgs& f, const double2* evcr, const double2* dvbox, int npv, int mb, double2* sticks);
+void fft_plane_drho(const FftArgs& f, const double2* dsticks, const double2* evcr, const double* occ, int nocc,
+                    int mb, double2* acc, double scale, double2* osticks);
+
+// ---- dense kernels (wb_la.cu) ----
+// part[s][j][r] = sum_{k in split s} W[r*ldw + k] * X[col(j)*ldx + k]
+int gemm_tn_splits(int M, int ncol, int K);
+void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
+             int nsplit, double* part, cudaStream_t s);
+// S = 2 sum_s part - W0 X0 (Gamma bra-ket, glbrak.f90:39-40), then
+// C[j][r] = sum_{r'<nkb} D[r][r'] S[j][r'] for r < nkb, alpha S[j][r] otherwise
+void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double* W, long ldw, const double* X,
+                  long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s);
+// Y[col(j)] = beta Y[col(j)] + W C[j]  over K real rows
+void gemm_nn(const double* W, long ldw, int M, const double* C, double* Y, long ldy, const int* cols, int ncol,
+             int K, double beta, cudaStream_t s);
+
+void permute_scale(const double2* dvg, long ld_in, const int* perm, const double* sqvc, int npw, int m,
+                   double2* aux, long ld_out, cudaStream_t s);
+void precondition(const double2* f, double2* pf, const double* g2kin, const double* eprec_col, int npw, int ncol,
+                  long ld, cudaStream_t s);
+void sub_into(const double2* a, const double2* b, double2* out, int npw, int ncol, long ld, cudaStream_t s);
+void kinetic_hpsi(const double2* P, double2* T, const double* g2kin, const double* ecol, const int* cols, int ncol,
+                  int npw, long ld, cudaStream_t s);
+void set_eprec(const double2* evc, const double* g2kin, int npw, int nocc, double* eprec, cudaStream_t s);
+void fill_columns(const double* per_band, int nocc, int nsys, double* out, cudaStream_t s);
+void cg_reset(unsigned char* conv, int nsys, cudaStream_t s);
+void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* g2kin,
+                 const double* eprec_col, double* rho_prev, unsigned char* conv, int iter, double tr2, int npw,
+                 long ld, cudaStream_t s);
+void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int* nact_dev, int* nact_host,
+                cudaStream_t s);
+void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
+               long ld, cudaStream_t s);
+void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cudaStream_t s);
+
+}  // namespace wb

@@ -1,0 +1,438 @@
+// Dense and streaming kernels of the response operator: the Gamma bra-ket
+// GEMMs on FP64 tensor cores (DMMA), the masked preconditioned CG steps, and
+// small pointwise passes.
+//
+// Complex arrays of length npw are treated as real arrays of length 2*npw
+// (Re, Im interleaved), exactly as WEST passes them to DGEMM at Gamma
+// (glbrak.f90:37-40, apply_alpha_pc_to_m_wfcs.f90:65-72).
+#include "wb_common.cuh"
+#include "wb_internal.h"
+
+namespace wb {
+
+WB_DEV void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// ---------------------------------------------------------------------------
+// part[s][j][r] = sum_{k in split s} W[r][k] X[col j][k]        (A^T B, split K)
+// CTA tile 32 r x 32 j, four warps interleave k in steps of 4 and are summed
+// through shared memory at the end.
+// ---------------------------------------------------------------------------
+constexpr int TN_T = 32;
+constexpr int TN_W = 4;
+
+__global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict__ W, long ldw, int M,
+                                                       const double* __restrict__ X, long ldx,
+                                                       const int* __restrict__ cols, int ncol, int K, int kchunk,
+                                                       double* __restrict__ part) {
+  __shared__ double red[TN_W][TN_T * TN_T];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lr = lane >> 2, lk = lane & 3;
+  const int r0 = blockIdx.x * TN_T, j0 = blockIdx.y * TN_T, split = blockIdx.z;
+  const int kb = split * kchunk, ke = min(K, kb + kchunk);
+  const double* arow[4];
+  bool aok[4];
+  const double* bcol[4];
+  bool bok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = r0 + i * 8 + lr;
+    aok[i] = r < M;
+    arow[i] = W + (long)(aok[i] ? r : 0) * ldw;
+    const int j = j0 + i * 8 + lr;
+    bok[i] = j < ncol;
+    const int c = bok[i] ? (cols ? cols[j] : j) : 0;
+    bcol[i] = X + (long)c * ldx;
+  }
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll 2
+  for (int k = kb + warp * 4; k < ke; k += 4 * TN_W) {
+    const int kk = k + lk;
+    const bool kok = kk < ke;
+    double av[4], bv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      av[i] = (aok[i] && kok) ? __ldg(arow[i] + kk) : 0.0;
+      bv[i] = (bok[i] && kok) ? __ldg(bcol[i] + kk) : 0.0;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) red[warp][(a * 8 + lr) * TN_T + b * 8 + 2 * lk + h] = acc[a][b][h];
+  __syncthreads();
+  for (int e = threadIdx.x; e < TN_T * TN_T; e += 32 * TN_W) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < TN_W; ++w) s += red[w][e];
+    const int r = r0 + e / TN_T, j = j0 + e % TN_T;
+    if (r < M && j < ncol) part[((long)split * ncol + j) * M + r] = s;
+  }
+}
+
+int gemm_tn_splits(int M, int ncol, int K) {
+  const int tiles = ((M + TN_T - 1) / TN_T) * ((ncol + TN_T - 1) / TN_T);
+  int ns = (2 * 148 * 2 + tiles - 1) / tiles;
+  const int maxs = (K + 511) / 512;
+  if (ns > maxs) ns = maxs;
+  if (ns < 1) ns = 1;
+  return ns;
+}
+
+void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
+             int nsplit, double* part, cudaStream_t s) {
+  if (ncol <= 0 || M <= 0) return;
+  int kchunk = (K + nsplit - 1) / nsplit;
+  kchunk = (kchunk + 15) / 16 * 16;
+  dim3 grid((M + TN_T - 1) / TN_T, (ncol + TN_T - 1) / TN_T, nsplit);
+  k_gemm_tn<<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, K, kchunk, part);
+}
+
+__global__ void __launch_bounds__(256) k_gamma_reduce(const double* __restrict__ part, int nsplit, int M, int ncol,
+                                                      const double* __restrict__ W, long ldw,
+                                                      const double* __restrict__ X, long ldx,
+                                                      const int* __restrict__ cols, const double* __restrict__ D,
+                                                      int nkb, double alpha, double* __restrict__ C) {
+  extern __shared__ double S[];
+  const int j = blockIdx.x;
+  const int col = cols ? cols[j] : j;
+  const double x0 = X[(long)col * ldx];
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double s = 0.0;
+    for (int sp = 0; sp < nsplit; ++sp) s += part[((long)sp * ncol + j) * M + r];
+    S[r] = 2.0 * s - W[(long)r * ldw] * x0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double c;
+    if (r < nkb) {
+      c = 0.0;
+      for (int q = 0; q < nkb; ++q) c = fma(D[r + (long)q * nkb], S[q], c);
+    } else {
+      c = alpha * S[r];
+    }
+    C[(long)j * M + r] = c;
+  }
+}
+
+void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double* W, long ldw, const double* X,
+                  long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s) {
+  if (ncol <= 0 || M <= 0) return;
+  k_gamma_reduce<<<ncol, 256, sizeof(double) * M, s>>>(part, nsplit, M, ncol, W, ldw, X, ldx, cols, D, nkb, alpha,
+                                                        C);
+}
+
+// ---------------------------------------------------------------------------
+// Y[col j][k] = beta Y[col j][k] + sum_r W[r][k] C[j][r]
+// CTA: 4 warps x 32 rows of k, 32 columns j; inner loop over r in steps of 4.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_gemm_nn(const double* __restrict__ W, long ldw, int M,
+                                                 const double* __restrict__ C, double* __restrict__ Y, long ldy,
+                                                 const int* __restrict__ cols, int ncol, int K, double beta) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lr = lane >> 2, lk = lane & 3;
+  const int k0 = blockIdx.x * 128 + warp * 32, j0 = blockIdx.y * 32;
+  bool kok[4], jok[4];
+  const double* crow[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    kok[i] = (k0 + i * 8 + lr) < K;
+    const int j = j0 + i * 8 + lr;
+    jok[i] = j < ncol;
+    crow[i] = C + (long)(jok[i] ? j : 0) * M;
+  }
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll 2
+  for (int r = 0; r < M; r += 4) {
+    const int rr = r + lk;
+    const bool rok = rr < M;
+    const double* wr = W + (long)(rok ? rr : 0) * ldw + k0 + lr;
+    double av[4], bv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      av[i] = (rok && kok[i]) ? __ldg(wr + i * 8) : 0.0;
+      bv[i] = (rok && jok[i]) ? __ldg(crow[i] + rr) : 0.0;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = j0 + b * 8 + 2 * lk + h;
+      if (j >= ncol) continue;
+      const int col = cols ? cols[j] : j;
+      double* y = Y + (long)col * ldy;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int k = k0 + a * 8 + lr;
+        if (k < K) y[k] = (beta == 0.0 ? 0.0 : beta * y[k]) + acc[a][b][h];
+      }
+    }
+}
+
+void gemm_nn(const double* W, long ldw, int M, const double* C, double* Y, long ldy, const int* cols, int ncol,
+             int K, double beta, cudaStream_t s) {
+  if (ncol <= 0 || M <= 0) return;
+  dim3 grid((K + 127) / 128, (ncol + 31) / 32);
+  k_gemm_nn<<<grid, 128, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, K, beta);
+}
+
+// ---------------------------------------------------------------------------
+// pointwise passes
+// ---------------------------------------------------------------------------
+// aux(i, p) = dvg(perm(i), p) * sqvc(i)      (apply_operator.f90:49-53)
+__global__ void k_permute_scale(const double2* __restrict__ dvg, long ld_in, const int* __restrict__ perm,
+                                const double* __restrict__ sqvc, int npw, double2* __restrict__ aux, long ld_out) {
+  const int p = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x)
+    aux[(long)p * ld_out + i] = cscale(dvg[(long)p * ld_in + perm[i]], sqvc[i]);
+}
+void permute_scale(const double2* dvg, long ld_in, const int* perm, const double* sqvc, int npw, int m,
+                   double2* aux, long ld_out, cudaStream_t s) {
+  if (m <= 0) return;
+  k_permute_scale<<<dim3((npw + 255) / 256, m), 256, 0, s>>>(dvg, ld_in, perm, sqvc, npw, aux, ld_out);
+}
+
+// pf = f / max(1, g2kin / eprec)         (precondition_m_wfcts.f90:35-51)
+__global__ void k_precondition(const double2* __restrict__ f, double2* __restrict__ pf,
+                               const double* __restrict__ g2kin, const double* __restrict__ eprec_col, int npw,
+                               long ld) {
+  const int j = blockIdx.y;
+  const double ep = eprec_col[j];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
+    const double den = fmax(1.0, g2kin[i] / ep);
+    const double2 v = f[(long)j * ld + i];
+    pf[(long)j * ld + i] = make_double2(v.x / den, v.y / den);
+  }
+}
+void precondition(const double2* f, double2* pf, const double* g2kin, const double* eprec_col, int npw, int ncol,
+                  long ld, cudaStream_t s) {
+  if (ncol <= 0) return;
+  k_precondition<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(f, pf, g2kin, eprec_col, npw, ld);
+}
+
+__global__ void k_sub_into(const double2* __restrict__ a, const double2* __restrict__ b, double2* __restrict__ out,
+                           int npw, long ld) {
+  const int j = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x)
+    out[(long)j * ld + i] = csub(a[(long)j * ld + i], b[(long)j * ld + i]);
+}
+void sub_into(const double2* a, const double2* b, double2* out, int npw, int ncol, long ld, cudaStream_t s) {
+  if (ncol <= 0) return;
+  k_sub_into<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(a, b, out, npw, ld);
+}
+
+// T = g2kin P (Im at G=0 zeroed) - e P     (k_psi.f90:51-77 then :65-74 of
+// apply_sternheimerop_to_m_wfcs.f90)
+__global__ void k_kinetic_hpsi(const double2* __restrict__ P, double2* __restrict__ T,
+                               const double* __restrict__ g2kin, const double* __restrict__ ecol,
+                               const int* __restrict__ cols, int npw, long ld) {
+  const int c = cols ? cols[blockIdx.y] : blockIdx.y;
+  const double e = ecol[c];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
+    const double2 p = P[(long)c * ld + i];
+    double2 h = cscale(p, g2kin[i]);
+    if (i == 0) h.y = 0.0;
+    T[(long)c * ld + i] = make_double2(fma(-e, p.x, h.x), fma(-e, p.y, h.y));
+  }
+}
+void kinetic_hpsi(const double2* P, double2* T, const double* g2kin, const double* ecol, const int* cols, int ncol,
+                  int npw, long ld, cudaStream_t s) {
+  if (ncol <= 0) return;
+  k_kinetic_hpsi<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(P, T, g2kin, ecol, cols, npw, ld);
+}
+
+// eprec_v = 1.35 sum_G |psi_v(G)|^2 g2kin(G)       (set_eprec.f90:40-53)
+__global__ void __launch_bounds__(256) k_set_eprec(const double2* __restrict__ evc, const double* __restrict__ g2kin,
+                                                   int npw, double* __restrict__ eprec) {
+  __shared__ double red[8];
+  const int v = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double2 c = evc[(long)v * npw + i];
+    s += (c.x * c.x + c.y * c.y) * g2kin[i];
+  }
+  s = block_sum<256>(s, red);
+  if (threadIdx.x == 0) eprec[v] = 1.35 * s;
+}
+void set_eprec(const double2* evc, const double* g2kin, int npw, int nocc, double* eprec, cudaStream_t s) {
+  k_set_eprec<<<nocc, 256, 0, s>>>(evc, g2kin, npw, eprec);
+}
+
+__global__ void k_fill_columns(const double* __restrict__ pb, int nocc, int nsys, double* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nsys; j += gridDim.x * blockDim.x) out[j] = pb[j % nocc];
+}
+void fill_columns(const double* per_band, int nocc, int nsys, double* out, cudaStream_t s) {
+  k_fill_columns<<<(nsys + 255) / 256, 256, 0, s>>>(per_band, nocc, nsys, out);
+}
+
+// ---------------------------------------------------------------------------
+// masked PCG (linsolve_sternheimer_m_wfcts.f90:146-330), one CTA per system
+// ---------------------------------------------------------------------------
+__global__ void k_cg_reset(unsigned char* conv, int nsys) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nsys; j += gridDim.x * blockDim.x) conv[j] = 0;
+}
+void cg_reset(unsigned char* conv, int nsys, cudaStream_t s) {
+  k_cg_reset<<<(nsys + 255) / 256, 256, 0, s>>>(conv, nsys);
+}
+
+// h = g / max(1, g2kin/eprec); rho = <h|g>_Gamma; converged if rho < tr2;
+// otherwise P = -h + (rho / rho_prev) P  (P = -h at the first iteration).
+__global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act, const double2* __restrict__ g,
+                                                     double2* __restrict__ P, const double* __restrict__ g2kin,
+                                                     const double* __restrict__ eprec_col, double* rho_prev,
+                                                     unsigned char* conv, int iter, double tr2, int npw, long ld) {
+  __shared__ double red[16];
+  const int j = act[blockIdx.x];
+  const double2* gj = g + (long)j * ld;
+  double2* pj = P + (long)j * ld;
+  const double ep = eprec_col[j];
+  double t = 0.0, t0 = 0.0;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double den = fmax(1.0, g2kin[i] / ep);
+    const double2 gv = gj[i];
+    const double hx = gv.x / den, hy = gv.y / den;
+    t = fma(hx, gv.x, fma(hy, gv.y, t));
+    if (i == 0) t0 = hx * gv.x;
+  }
+  const double2 s = block_sum2<256>(t, t0, red);
+  const double rho = 2.0 * s.x - s.y;
+  const bool c = rho < tr2;
+  if (c) {
+    if (threadIdx.x == 0) conv[j] = 1;
+    return;
+  }
+  const double beta = (iter == 1) ? 0.0 : rho / rho_prev[j];
+  __syncthreads();
+  if (threadIdx.x == 0) rho_prev[j] = rho;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double den = fmax(1.0, g2kin[i] / ep);
+    const double2 gv = gj[i];
+    const double hx = gv.x / den, hy = gv.y / den;
+    if (iter == 1) {
+      pj[i] = make_double2(-hx, -hy);
+    } else {
+      const double2 pv = pj[i];
+      pj[i] = make_double2(fma(beta, pv.x, -hx), fma(beta, pv.y, -hy));
+    }
+  }
+}
+void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* g2kin,
+                 const double* eprec_col, double* rho_prev, unsigned char* conv, int iter, double tr2, int npw,
+                 long ld, cudaStream_t s) {
+  if (nact <= 0) return;
+  k_cg_prec_rho<<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, npw, ld);
+}
+
+// Active list in increasing system order (map_lbnd2ibnd, :356-382) and the
+// Gamma FFT pairs (act[2k], act[2k+1]).
+__global__ void __launch_bounds__(1024) k_cg_compact(const unsigned char* __restrict__ conv, int nsys,
+                                                     int* __restrict__ act, int2* __restrict__ items,
+                                                     int* __restrict__ nact_out) {
+  __shared__ int wsum[32];
+  __shared__ int base;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid == 0) base = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < nsys; c0 += 1024) {
+    const int i = c0 + tid;
+    const bool f = (i < nsys) && !conv[i];
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    const int pre = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 0) wsum[w] = __popc(bal);
+    __syncthreads();
+    if (w == 0) {
+      int v = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+      }
+      wsum[lane] = v;  // inclusive
+    }
+    __syncthreads();
+    const int off = base + (w > 0 ? wsum[w - 1] : 0) + pre;
+    if (f) act[off] = i;
+    __syncthreads();
+    if (tid == 0) base += wsum[31];
+    __syncthreads();
+  }
+  const int n = base;
+  for (int k = tid; k < (n + 1) / 2; k += 1024)
+    items[k] = make_int2(act[2 * k], (2 * k + 1 < n) ? act[2 * k + 1] : -1);
+  if (tid == 0) *nact_out = n;
+}
+void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int* nact_dev, int* nact_host,
+                cudaStream_t s) {
+  k_cg_compact<<<1, 1024, 0, s>>>(conv, nsys, act, items, nact_dev);
+  cudaMemcpyAsync(nact_host, nact_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+}
+
+// a = <P|g>, c = <P|T> (Gamma); x -= (a/c) P ; g -= (a/c) T     (:253-322)
+__global__ void __launch_bounds__(256) k_cg_update(const int* __restrict__ act, double2* __restrict__ x,
+                                                   double2* __restrict__ g, const double2* __restrict__ P,
+                                                   const double2* __restrict__ T, int npw, long ld) {
+  __shared__ double red[16];
+  const int j = act[blockIdx.x];
+  const double2* pj = P + (long)j * ld;
+  const double2* tj = T + (long)j * ld;
+  double2* gj = g + (long)j * ld;
+  double2* xj = x + (long)j * ld;
+  double a = 0.0, c = 0.0;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double2 p = pj[i], gv = gj[i], t = tj[i];
+    double da = fma(p.x, gv.x, p.y * gv.y);
+    double dc = fma(p.x, t.x, p.y * t.y);
+    if (i == 0) { da -= 0.5 * p.x * gv.x; dc -= 0.5 * p.x * t.x; }
+    a += da;
+    c += dc;
+  }
+  const double2 s = block_sum2<256>(a, c, red);
+  const double r = (2.0 * s.x) / (2.0 * s.y);
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double2 p = pj[i], t = tj[i];
+    double2 xv = xj[i], gv = gj[i];
+    xj[i] = make_double2(fma(-r, p.x, xv.x), fma(-r, p.y, xv.y));
+    gj[i] = make_double2(fma(-r, t.x, gv.x), fma(-r, t.y, gv.y));
+  }
+}
+void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
+               long ld, cudaStream_t s) {
+  if (nact <= 0) return;
+  k_cg_update<<<nact, 256, 0, s>>>(act, x, g, P, T, npw, ld);
+}
+
+__global__ void k_count_unconverged(const unsigned char* __restrict__ conv, int nocc, int mb, int* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= mb) return;
+  int n = 0;
+  for (int v = 0; v < nocc; ++v) n += conv[(long)p * nocc + v] ? 0 : 1;
+  out[p] = n;
+}
+void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cudaStream_t s) {
+  if (mb <= 0) return;
+  k_count_unconverged<<<(mb + 127) / 128, 128, 0, s>>>(conv, nocc, mb, out);
+}
+
+}  // namespace wb

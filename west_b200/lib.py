@@ -1,0 +1,86 @@
+"""ctypes binding of ``libwestb200.so`` (declarations in include/west_b200.h).
+
+The library is loaded from the package directory only; there is no fallback:
+if it is missing, ``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwestb200.so")
+
+WB_OK = 0
+WB_ERR_ARG = -1
+WB_ERR_CUDA = -2
+WB_ERR_UNSUPPORTED = -3
+WB_ERR_NOMEM = -4
+WB_PRECISION_FP64 = 0
+WB_PRECISION_MIXED = 1
+
+# Every symbol include/west_b200.h declares.
+EXPORTS = (
+    "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
+    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_last_error", "wb_version",
+)
+
+_p = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+
+class WbSystem(ctypes.Structure):
+    _fields_ = [
+        ("npw", _i), ("npwx", _i), ("nr1", _i), ("nr2", _i), ("nr3", _i),
+        ("nbnd_occ", _i), ("nkb", _i), ("n_dfpt_maxiter", _i), ("l_kinetic_only", _i), ("gstart", _i),
+        ("nl", _p), ("nlm", _p), ("g2kin", _p), ("vrs", _p), ("evc", _p), ("et", _p),
+        ("occupation", _p), ("vkb", _p), ("deeq", _p), ("sqvc", _p),
+        ("alpha_pv", _d), ("omega", _d), ("wk", _d),
+    ]
+
+
+class WbStats(ctypes.Structure):
+    _fields_ = [("m", _i), ("cg_iterations", _i), ("cg_active_sum", ctypes.c_longlong),
+                ("fft_boxes", ctypes.c_longlong), ("ms_total", _d)]
+
+
+class WestB200Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"west_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the library (once) and declare argument types."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: run `python -m west_b200.build` (nvcc, sm_100a)")
+    lib = ctypes.CDLL(path)
+    lib.wb_ctx_create.argtypes = [ctypes.POINTER(_p), ctypes.POINTER(WbSystem), _i]
+    lib.wb_ctx_destroy.argtypes = [_p]
+    for name in ("wb_apply_operator", "wb_apply_operator_device"):
+        getattr(lib, name).argtypes = [_p, _i, _p, _i, _p, _i, _d, _i, _p]
+    lib.wb_set_precision.argtypes = [_p, _i]
+    lib.wb_set_batch.argtypes = [_p, _i]
+    lib.wb_get_stats.argtypes = [_p, ctypes.POINTER(WbStats)]
+    lib.wb_last_error.restype = ctypes.c_char_p
+    lib.wb_last_error.argtypes = []
+    lib.wb_version.argtypes = []
+    for name in EXPORTS:
+        if name not in ("wb_last_error",):
+            getattr(lib, name).restype = _i
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> int:
+    if rc < 0:
+        msg = _lib.wb_last_error().decode() if _lib is not None else ""
+        raise WestB200Error(rc, msg)
+    return rc

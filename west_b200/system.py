@@ -1,0 +1,272 @@
+"""Synthetic Gamma-point plane-wave systems: the implicit inputs of Wstat's
+response operator.
+
+``apply_operator`` (Wstat/apply_operator.f90:14) reads its ground state from
+Quantum ESPRESSO module variables: ``evc``, ``et``, ``g2kin``, ``vrs``,
+``vkb``, ``deeq``, ``dffts%nl/nlm``, ``omega``, ``wk`` and the Coulomb factor
+``pot3D%sqvc``.  This module builds those arrays for a cubic cell filled with
+Gaussian pseudo-atoms, in QE's conventions:
+
+* Rydberg units; kinetic energy ``g2kin = |G|^2 tpiba2``; ``e2 = 2``.
+* Gamma-only storage: the half sphere ``x > 0 | (x = 0, y > 0) | (x = y = 0,
+  z >= 0)`` with ``psi(-G) = conj(psi(G))``, sorted by ``|G|^2`` so that G=0
+  comes first (``gstart = 2`` in Fortran numbering).
+* ``nl``/``nlm``: box positions of +G / -G in an ``nr^3`` box, x fastest.
+  They are returned 0-based here; the C ABI takes QE's 1-based values.
+* ``invfft`` is the unscaled sum over ``exp(+iGr)``; ``fwfft`` carries 1/N^3.
+
+The ground state comes from an exact diagonalisation of the same Hamiltonian
+the response operator applies (kinetic + local potential sampled on the FFT
+box + Kleinman-Bylander projectors), written as a real symmetric matrix on
+the Gamma half sphere.  With no aliasing in the box (2*Gmax < nr/2) the dense
+matrix equals the FFT-based ``h_psi`` exactly.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+E2 = 2.0          # e^2 in Rydberg units (QE constants: e2)
+FPI = 4.0 * math.pi
+
+
+@dataclasses.dataclass(frozen=True)
+class SystemSpec:
+    """Parameters of a synthetic cubic Gamma-only system."""
+    L: float                 # cubic cell edge (bohr)
+    ecutwfc: float           # wavefunction cutoff (Ry)
+    nr: int                  # FFT box edge
+    natoms: int              # Gaussian pseudo-atoms at seeded uniform positions
+    nbnd_occ: int            # occupied bands
+    proj: str = "s"          # "s" or "sp": KB projectors per atom
+    Z: float = 4.0           # local well depth (Ry): V(r) = -Z exp(-r^2 / 2 sigma^2)
+    sigma: float = 0.8       # local well width (bohr)
+    sigma_p: float = 0.6     # Gaussian radial width of the KB projectors (bohr)
+    dion: float = 1.0        # KB coupling D (Ry), diagonal
+    nbnd_extra: int = 4      # empty bands computed beside the occupied ones
+    seed: int = 0
+
+
+# Workloads.  c1..c5 follow the five named configurations; ``tiny``/``small``
+# are the sizes the CPU tests run in seconds.
+SPECS = {
+    "tiny": SystemSpec(L=8.0, ecutwfc=6.0, nr=16, natoms=2, nbnd_occ=3, proj="sp", seed=11),
+    "small": SystemSpec(L=10.0, ecutwfc=8.0, nr=24, natoms=3, nbnd_occ=7, proj="sp", seed=12),
+    "c1": SystemSpec(L=15.0, ecutwfc=20.0, nr=48, natoms=4, nbnd_occ=8, proj="s", seed=1),
+    "c2": SystemSpec(L=20.0, ecutwfc=25.0, nr=64, natoms=8, nbnd_occ=32, proj="sp", seed=2),
+    "c4a": SystemSpec(L=15.0, ecutwfc=20.0, nr=48, natoms=4, nbnd_occ=8, proj="sp", seed=41),
+    "c4b": SystemSpec(L=20.0, ecutwfc=25.0, nr=64, natoms=8, nbnd_occ=32, proj="sp", seed=42),
+    "c4c": SystemSpec(L=25.0, ecutwfc=25.0, nr=80, natoms=12, nbnd_occ=64, proj="sp", seed=43),
+    "c5": SystemSpec(L=30.0, ecutwfc=30.0, nr=108, natoms=20, nbnd_occ=128, proj="sp", seed=5),
+}
+
+
+@dataclasses.dataclass
+class GammaSystem:
+    """All arrays the response operator consumes (QE/WEST naming)."""
+    spec: SystemSpec
+    omega: float
+    tpiba2: float
+    nr: int
+    mill: np.ndarray        # int32 [npw, 3] Miller indices, |G| order, G=0 first
+    g2kin: np.ndarray       # f64 [npw]
+    nl: np.ndarray          # int64 [npw] 0-based box index of +G
+    nlm: np.ndarray         # int64 [npw] 0-based box index of -G
+    vrs: np.ndarray         # f64 [nr^3] local potential on the box (x fastest)
+    vkb: np.ndarray         # c128 [npw, nkb]
+    deeq: np.ndarray        # f64 [nkb, nkb]
+    evc: np.ndarray         # c128 [npw, nbnd_occ]
+    et: np.ndarray          # f64 [nbnd_occ + nbnd_extra]
+    occupation: np.ndarray  # f64 [nbnd_occ]
+    sqvc: np.ndarray        # f64 [npw]
+    alpha_pv: float
+    wk: float = 2.0         # QE k weight at Gamma, non-spin-polarised (sum = 2)
+    tau: Optional[np.ndarray] = None
+
+    @property
+    def npw(self) -> int:
+        return int(self.mill.shape[0])
+
+    @property
+    def nbnd_occ(self) -> int:
+        return int(self.evc.shape[1])
+
+    @property
+    def nkb(self) -> int:
+        return int(self.vkb.shape[1])
+
+    @property
+    def nnr(self) -> int:
+        return self.nr ** 3
+
+
+def gamma_half_sphere(L: float, ecutwfc: float, nr: int):
+    """Miller indices of the Gamma half sphere |G|^2 tpiba2 <= ecutwfc,
+    sorted by |G|^2 (ties by Miller index) so that G=0 is first."""
+    tpiba2 = (2.0 * math.pi / L) ** 2
+    nmax = int(math.sqrt(ecutwfc / tpiba2)) + 1
+    r = np.arange(-nmax, nmax + 1)
+    i, j, k = np.meshgrid(r, r, r, indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    n2 = i * i + j * j + k * k
+    keep = (n2 * tpiba2 <= ecutwfc) & ((i > 0) | ((i == 0) & (j > 0)) | ((i == 0) & (j == 0) & (k >= 0)))
+    mill = np.stack([i[keep], j[keep], k[keep]], axis=1).astype(np.int32)
+    n2 = n2[keep]
+    order = np.lexsort((mill[:, 2], mill[:, 1], mill[:, 0], n2))
+    mill = mill[order]
+    if np.abs(mill).max() * 2 >= nr:
+        raise ValueError(f"FFT box {nr} too small for cutoff {ecutwfc} Ry in cell {L}")
+    return mill, tpiba2
+
+
+def box_index(mill: np.ndarray, nr: int) -> np.ndarray:
+    """0-based linear index (x fastest) of Miller triples in an nr^3 box."""
+    m = np.mod(mill.astype(np.int64), nr)
+    return m[:, 0] + nr * (m[:, 1] + nr * m[:, 2])
+
+
+def _local_potential(L, nr, tau, Z, sigma):
+    x = np.arange(nr) * (L / nr)
+    v = np.zeros((nr, nr, nr))          # [k][j][i] = (z, y, x)
+    for t in tau:
+        dx = x - t[0]; dx -= L * np.round(dx / L)
+        dy = x - t[1]; dy -= L * np.round(dy / L)
+        dz = x - t[2]; dz -= L * np.round(dz / L)
+        d2 = dz[:, None, None] ** 2 + dy[None, :, None] ** 2 + dx[None, None, :] ** 2
+        v += -Z * np.exp(-d2 / (2.0 * sigma * sigma))
+    return v.ravel()
+
+
+def _kb_projectors(mill, L, tau, proj, sigma_p):
+    tpiba = 2.0 * math.pi / L
+    G = mill.astype(np.float64) * tpiba                    # [npw, 3] bohr^-1
+    g2 = (G * G).sum(1)
+    radial = np.exp(-0.5 * sigma_p * sigma_p * g2)
+    cols = []
+    for t in tau:
+        phase = np.exp(-1j * (G @ np.asarray(t)))
+        cols.append(radial * phase)                        # s
+        if proj == "sp":
+            for a in range(3):                             # p_x, p_y, p_z (real in r space)
+                cols.append(-1j * sigma_p * G[:, a] * radial * phase)
+    vkb = np.stack(cols, axis=1)
+    # unit norm under the Gamma dot product 2 sum_half |b|^2 - |b(0)|^2
+    nrm = 2.0 * (np.abs(vkb) ** 2).sum(0) - np.abs(vkb[0]) ** 2
+    return vkb / np.sqrt(nrm)[None, :]
+
+
+def _dense_gamma_hamiltonian(sysd, device="cpu"):
+    """Real symmetric Hamiltonian on the orthonormal Gamma basis
+    {e_0, (e_G + e_-G)/sqrt2, i(e_G - e_-G)/sqrt2}."""
+    import torch
+    nr = sysd["nr"]
+    mill = torch.as_tensor(sysd["mill"].astype(np.int64), device=device)
+    vt = np.fft.fftn(sysd["vrs"].reshape(nr, nr, nr)) / nr ** 3     # V(G) on the box
+    vt = torch.as_tensor(vt.ravel(), device=device)
+    npw = mill.shape[0]
+
+    def vidx(sign):
+        d = (mill[:, None, :] + sign * mill[None, :, :]) % nr
+        return d[..., 0] + nr * (d[..., 1] + nr * d[..., 2])
+
+    B = torch.as_tensor(sysd["vkb"], device=device)
+    D = torch.as_tensor(sysd["deeq"], device=device).to(B.dtype)
+    hpp = vt[vidx(-1)]                       # H(G, G')
+    hpp += B @ D @ B.conj().T
+    hpp += torch.diag(torch.as_tensor(sysd["g2kin"], device=device)).to(hpp.dtype)
+    hpq = vt[vidx(+1)]                       # H(G, -G')
+    hpq += B @ D @ B.T
+    H = torch.empty((2 * npw, 2 * npw), dtype=torch.float64, device=device)
+    H[:npw, :npw] = hpp.real + hpq.real
+    H[npw:, npw:] = hpp.real - hpq.real
+    H[:npw, npw:] = -hpp.imag + hpq.imag
+    H[npw:, :npw] = H[:npw, npw:].T
+    del hpp, hpq
+    # G = 0 has no sine partner; its cosine vector is sqrt2 * e_0
+    s = 1.0 / math.sqrt(2.0)
+    H[0, :] *= s
+    H[:, 0] *= s
+    keep = torch.ones(2 * npw, dtype=torch.bool, device=device)
+    keep[npw] = False
+    return H[keep][:, keep]
+
+
+def _ground_state(sysd, nbnd, device="cpu"):
+    import torch
+    H = _dense_gamma_hamiltonian(sysd, device=device)
+    H = 0.5 * (H + H.T)
+    w, v = torch.linalg.eigh(H)
+    w = w[:nbnd].cpu().numpy()
+    x = v[:, :nbnd].cpu().numpy()
+    npw = sysd["mill"].shape[0]
+    evc = np.empty((npw, nbnd), dtype=np.complex128)
+    evc[0] = x[0]
+    s = 1.0 / math.sqrt(2.0)
+    evc[1:] = (x[1:npw] + 1j * x[npw:]) * s
+    # only a sign is free (psi(r) stays real): make the largest real part positive
+    for b in range(nbnd):
+        k = np.argmax(np.abs(evc[:, b].real))
+        if evc[k, b].real < 0:
+            evc[:, b] *= -1.0
+    return w, evc
+
+
+def build_system(spec: SystemSpec | str, device: Optional[str] = None) -> GammaSystem:
+    """Build a synthetic Gamma system from a spec (or the name of one)."""
+    if isinstance(spec, str):
+        spec = SPECS[spec]
+    if device is None:
+        device = "cpu"
+    rng = np.random.default_rng(spec.seed)
+    L, nr = spec.L, spec.nr
+    mill, tpiba2 = gamma_half_sphere(L, spec.ecutwfc, nr)
+    tau = rng.uniform(0.0, L, size=(spec.natoms, 3))
+    g2kin = (mill.astype(np.float64) ** 2).sum(1) * tpiba2
+    nl = box_index(mill, nr)
+    nlm = box_index(-mill, nr)
+    vrs = _local_potential(L, nr, tau, spec.Z, spec.sigma)
+    vkb = _kb_projectors(mill, L, tau, spec.proj, spec.sigma_p)
+    nkb = vkb.shape[1]
+    deeq = np.eye(nkb) * spec.dion
+    sysd = dict(nr=nr, mill=mill, vrs=vrs, vkb=vkb, deeq=deeq, g2kin=g2kin)
+    nbnd = spec.nbnd_occ + spec.nbnd_extra
+    et, evc = _ground_state(sysd, nbnd, device=device)
+    qg2 = g2kin.copy()
+    sqvc = np.zeros_like(qg2)
+    nz = qg2 > 1e-8
+    sqvc[nz] = np.sqrt(E2 * FPI / qg2[nz])           # Coulomb_kernel/class_coulomb.f90:173
+    emin = et.min()
+    emax = et[: spec.nbnd_occ].max()
+    alpha_pv = max(2.0 * (emax - emin), 0.01)          # Tools/get_alpha_pv.f90:59-63
+    return GammaSystem(
+        spec=spec, omega=L ** 3, tpiba2=tpiba2, nr=nr, mill=mill, g2kin=g2kin,
+        nl=nl, nlm=nlm, vrs=vrs, vkb=vkb, deeq=deeq,
+        evc=np.ascontiguousarray(evc[:, : spec.nbnd_occ]), et=et,
+        occupation=np.ones(spec.nbnd_occ), sqvc=sqvc, alpha_pv=alpha_pv, tau=tau)
+
+
+def perturbations(sysm: GammaSystem, m: int, seed: int = 1234) -> np.ndarray:
+    """dvg test batch: seeded complex-normal coefficients times 4 pi / |G|^2
+    (G = 0 zeroed), column-major [npw, m]."""
+    rng = np.random.default_rng(seed)
+    z = rng.standard_normal((sysm.npw, m)) + 1j * rng.standard_normal((sysm.npw, m))
+    scale = np.zeros(sysm.npw)
+    nz = sysm.g2kin > 1e-8
+    scale[nz] = FPI / sysm.g2kin[nz]
+    return np.asfortranarray(z * scale[:, None])
+
+
+def randomized_basis(sysm: GammaSystem, m: int, seed: int = 4321) -> np.ndarray:
+    """Starting PDEP guesses in the manner of do_randomize
+    (Wstat/davidson_diago.f90:1121-1182): amplitude rr uniform in [0,1), phase
+    2 pi uniform, divided by (|g|^2 + 1) with g in 2pi/alat units; G=0 left 0."""
+    rng = np.random.default_rng(seed)
+    rr = rng.random((sysm.npw, m))
+    arg = 2.0 * math.pi * rng.random((sysm.npw, m))
+    g2 = (sysm.mill.astype(np.float64) ** 2).sum(1)
+    a = rr * np.exp(1j * arg) / (g2 + 1.0)[:, None]
+    a[0] = 0.0
+    return np.asfortranarray(a)

@@ -1,0 +1,120 @@
+"""Python host interface mirroring WEST's Wstat response operator.
+
+``ResponseOperator.apply_operator(m, dvg, dng, tr2, iq)`` has the argument
+meaning of ``SUBROUTINE apply_operator(m, dvg, dng, tr2, iq)``
+(Wstat/apply_operator.f90:14): ``dvg`` and ``dng`` are ``[npwqx, m]``
+complex128 arrays (Fortran order), ``dng`` is overwritten, ``tr2 < 0``
+selects the lite solver, and ``iq`` must be 1 (Gamma).  Unconverged bands are
+reported the way dfpt does (a WARNING line per perturbation,
+DFPT_kernel/dfpt_module.f90:358-359) and returned as the ``ierr`` array;
+setup errors raise, where WEST calls ``errore``.
+
+Device arrays are accepted as torch CUDA tensors (complex128, Fortran column
+layout expressed as a ``[m, npwqx]`` row-major tensor), which skips the host
+copies.
+"""
+from __future__ import annotations
+
+import ctypes
+import sys
+
+import numpy as np
+
+from . import lib as _lib
+from .system import GammaSystem
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class ResponseOperator:
+    """B200 implementation of apply_operator for one Gamma-point ground state."""
+
+    def __init__(self, system: GammaSystem, n_dfpt_maxiter: int = 250, l_kinetic_only: bool = False,
+                 device: int = 0, verbose: bool = True):
+        self._lib = _lib.load()
+        self.system = system
+        self.verbose = verbose
+        s = system
+        self._keep = keep = dict(
+            nl=np.ascontiguousarray(s.nl + 1, dtype=np.int32),
+            nlm=np.ascontiguousarray(s.nlm + 1, dtype=np.int32),
+            g2kin=np.ascontiguousarray(s.g2kin, dtype=np.float64),
+            vrs=np.ascontiguousarray(s.vrs, dtype=np.float64),
+            evc=np.asfortranarray(s.evc, dtype=np.complex128),
+            et=np.ascontiguousarray(s.et[: s.nbnd_occ], dtype=np.float64),
+            occ=np.ascontiguousarray(s.occupation, dtype=np.float64),
+            vkb=np.asfortranarray(s.vkb, dtype=np.complex128),
+            deeq=np.asfortranarray(s.deeq, dtype=np.float64),
+            sqvc=np.ascontiguousarray(s.sqvc, dtype=np.float64),
+        )
+        ws = _lib.WbSystem()
+        ws.npw = ws.npwx = s.npw
+        ws.nr1 = ws.nr2 = ws.nr3 = s.nr
+        ws.nbnd_occ = s.nbnd_occ
+        ws.nkb = s.nkb
+        ws.n_dfpt_maxiter = n_dfpt_maxiter
+        ws.l_kinetic_only = int(bool(l_kinetic_only))
+        ws.gstart = 2
+        ws.nl = _ptr(keep["nl"]); ws.nlm = _ptr(keep["nlm"])
+        ws.g2kin = _ptr(keep["g2kin"]); ws.vrs = _ptr(keep["vrs"])
+        ws.evc = _ptr(keep["evc"]); ws.et = _ptr(keep["et"]); ws.occupation = _ptr(keep["occ"])
+        ws.vkb = _ptr(keep["vkb"]); ws.deeq = _ptr(keep["deeq"]); ws.sqvc = _ptr(keep["sqvc"])
+        ws.alpha_pv = s.alpha_pv
+        ws.omega = s.omega
+        ws.wk = s.wk
+        ctx = ctypes.c_void_p()
+        _lib.check(self._lib.wb_ctx_create(ctypes.byref(ctx), ctypes.byref(ws), device))
+        self._ctx = ctx
+        self.npwqx = s.npw
+
+    def close(self):
+        if getattr(self, "_ctx", None) is not None and self._ctx.value:
+            self._lib.wb_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, mode: str):
+        code = {"fp64": _lib.WB_PRECISION_FP64, "mixed": _lib.WB_PRECISION_MIXED}[mode]
+        _lib.check(self._lib.wb_set_precision(self._ctx, code))
+
+    def set_batch(self, max_perturbations: int):
+        _lib.check(self._lib.wb_set_batch(self._ctx, int(max_perturbations)))
+
+    def stats(self) -> dict:
+        st = _lib.WbStats()
+        _lib.check(self._lib.wb_get_stats(self._ctx, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def apply_operator(self, m, dvg, dng, tr2, iq=1):
+        """dng <- sqvc chi0 sqvc dvg for m columns; returns ierr[m]."""
+        ierr = np.zeros(max(m, 1), dtype=np.int32)
+        if _is_torch_cuda(dvg):
+            ld_in = int(dvg.shape[1]); ld_out = int(dng.shape[1])
+            rc = self._lib.wb_apply_operator_device(self._ctx, m, dvg.data_ptr(), ld_in, dng.data_ptr(), ld_out,
+                                                    float(tr2), int(iq), _ptr(ierr))
+        else:
+            if not (isinstance(dng, np.ndarray) and dng.dtype == np.complex128 and dng.flags.f_contiguous):
+                raise TypeError("dng must be a Fortran-ordered complex128 array")
+            dvg_f = np.asfortranarray(dvg, dtype=np.complex128)
+            if dvg_f.ndim != 2 or dvg_f.shape[1] < m or dng.shape[1] < m:
+                raise ValueError("dvg/dng must be [npwqx, >= m]")
+            rc = self._lib.wb_apply_operator(self._ctx, m, _ptr(dvg_f), dvg_f.shape[0], _ptr(dng), dng.shape[0],
+                                             float(tr2), int(iq), _ptr(ierr))
+        _lib.check(rc)
+        ierr = ierr[:m]
+        if self.verbose:
+            for ipert in np.flatnonzero(ierr):
+                sys.stdout.write(f"       ** WARNING : PERT {ipert + 1:8d} iks {1:8d} not converged, "
+                                 f"ierr = {ierr[ipert]:8d}\n")
+        return ierr
+
+
+def _is_torch_cuda(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
