@@ -1,0 +1,345 @@
+"""Benchmark of the Wstat response operator: dvg -> drho applications per second.
+
+Workload (one "step"): one apply_operator call on 64 perturbations of the
+L = 20 bohr, 25 Ry Gamma system (npw 8,440, 64^3 FFT box, 8 Gaussian
+pseudo-atoms with s+p Kleinman-Bylander projectors, 32 occupied bands),
+seeded complex-normal perturbations scaled by 4 pi / |G|^2, PCG threshold
+tr2 = 1e-10, FP64.  Synthetic inputs; the ground state comes from an exact
+diagonalisation of the same Hamiltonian.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One JSON line on stdout (rank 0).  Under torchrun every rank applies its own
+64 perturbations (weak scaling, no collective on the data path); the time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "c2"
+M_PERT = 64
+TR2 = 1e-10
+METRIC = "dvg->drho applications/s (apply_operator, FP64)"
+UNIT = "applications/s"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--m", type=int, default=M_PERT)
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--cpu-sample", type=int, default=1, help="perturbations in the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _config(args, extra=None):
+    from west_b200.system import SPECS
+    sp = SPECS[args.workload]
+    cfg = {"workload": f"apply_operator {args.workload}: L={sp.L:g} bohr, ecutwfc={sp.ecutwfc:g} Ry, "
+                       f"{sp.nr}^3 FFT, {sp.natoms} atoms ({sp.proj}), nbnd_occ={sp.nbnd_occ}, "
+                       f"m={args.m} perturbations, tr2={TR2:g}",
+           "m_per_rank": args.m, "tr2": TR2, "n_dfpt_maxiter": 250, "precision": "fp64",
+           "l2": "working set per step >> 126 MB L2 (PCG vectors and stick buffers, GBs)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def _fp64_gemm_peak(torch):
+    """FP64 DGEMM throughput of this GPU (cuBLAS, 8192^3), TFLOP/s, best of 3."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(); torch.matmul(a, b); e1.record(); torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def _cpu_baseline(system, m_sample, seed):
+    """The oracle (CPU restatement of WEST's algorithm) on a bounded sample."""
+    from oracle import west_oracle as O
+    from west_b200.system import perturbations
+    dvg = perturbations(system, m_sample, seed=seed)
+    t0 = time.perf_counter()
+    O.apply_operator(system, dvg, TR2)
+    dt = time.perf_counter() - t0
+    return {"value": m_sample / dt, "unit": UNIT, "cores": O._WORKERS, "kind": "port",
+            "sample": f"{m_sample} perturbation(s) of the same workload through the NumPy/SciPy FP64 oracle "
+                      f"(scipy.fft workers={O._WORKERS}, BLAS threads default), {dt:.1f} s"}
+
+
+def _build_system(name, device):
+    from west_b200.system import build_system
+    return build_system(name, device=device)
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU restatement of WEST's apply_operator, timed on the host cores."""
+    if rank != 0:
+        return None
+    import torch
+    from oracle import west_oracle as O
+    from west_b200.system import perturbations
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    s = _build_system(args.workload, dev)           # ground-state synthesis only
+    m = max(1, args.cpu_sample)
+    times = []
+    for it in range(args.warmup + args.steps):
+        dvg = perturbations(s, m, seed=1000 + it)
+        t0 = time.perf_counter()
+        O.apply_operator(s, dvg, TR2)
+        if it >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = m * args.steps / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": _config(args, {"reference_sample_m": m}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O._WORKERS, "kind": "port",
+                             "sample": f"{m} perturbation(s) per step through the NumPy/SciPy FP64 restatement "
+                                       f"of WEST's apply_operator (the Fortran reference cannot be built here)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from west_b200.system import perturbations
+    from west_b200.wstat import ResponseOperator
+
+    torch.cuda.set_device(local_rank)
+    t0 = time.time()
+    s = _build_system(args.workload, "cuda")
+    t_sys = time.time() - t0
+    m = args.m
+    op = ResponseOperator(s, device=local_rank, verbose=False)
+    npw = s.npw
+    dvg_h = perturbations(s, m, seed=1234 + rank)
+    dvg_d = torch.from_numpy(np.ascontiguousarray(dvg_h.T)).cuda()      # [m, npw] = Fortran [npw, m]
+    dng_d = torch.zeros_like(dvg_d)
+    dvg_p = torch.from_numpy(np.ascontiguousarray(dvg_h.T)).pin_memory()
+    dng_p = torch.zeros_like(dvg_p).pin_memory()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (also settles the device workspace)
+    for _ in range(args.warmup):
+        op.apply_operator(m, dvg_d, dng_d, TR2)
+    torch.cuda.synchronize()
+
+    # timed region: inputs resident in HBM, stage events on the library stream
+    op.set_profiling(1)
+    stage_tot = {}
+    launches = 0
+    iters, act_sum, boxes = [], 0, 0
+    barrier(); torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            ierr = op.apply_operator(m, dvg_d, dng_d, TR2)
+            st = op.stats()
+            launches += st["launches"]
+            iters.append(st["cg_iterations"]); act_sum += st["cg_active_sum"]; boxes += st["fft_boxes"]
+            for k, v in st["stages"].items():
+                a = stage_tot.setdefault(k, {"ms": 0.0, "launches": 0, "items": 0})
+                a["ms"] += v["ms"]; a["launches"] += v["launches"]; a["items"] += v["items"]
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    op.set_profiling(0)
+    value = world * m * args.steps / (ms * 1e-3)
+    dng_val = dng_d.cpu().numpy().T.copy()
+
+    # end-to-end through the host-pointer entry point, pinned host buffers
+    dvg_np = dvg_p.numpy().T      # Fortran-ordered view of pinned memory
+    dng_np = dng_p.numpy().T
+    barrier(); torch.cuda.synchronize()
+    t_e2e0 = time.perf_counter()
+    for _ in range(args.steps):
+        op.apply_operator(m, dvg_np, dng_np, TR2)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t_e2e0)
+    barrier()
+    e2e_val = world * m * args.steps / e2e_s
+    e2e_ok = bool(np.allclose(dng_np, dng_val, rtol=0, atol=1e-12 * np.abs(dng_val).max()))
+
+    line = None
+    if rank == 0:
+        peaks = _measured_peaks()
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        fp64_peak = _fp64_gemm_peak(torch)
+        N = s.nr
+        # dominant stage: the local-potential FFT (zinv + plane + zfwd = 2 box FFTs per item)
+        vz = [stage_tot[k] for k in ("vloc_zinv", "vloc_plane", "vloc_zfwd")]
+        items = vz[1]["items"]; nl = max(1, vz[1]["launches"])
+        t_ms = sum(v["ms"] for v in vz)
+        alg_bytes = 2.0 * items * 2.0 * N ** 3 * 16.0           # B_fft = 2 N^3 s per FFT, 2 FFTs per item
+        per_launch_bytes = alg_bytes / nl
+        per_launch_s = t_ms * 1e-3 / nl
+        achieved = per_launch_bytes / per_launch_s / 1e9
+        flops = 2.0 * items * 5.0 * N ** 3 * math.log2(N ** 3)  # nominal radix-2 count, full box
+        fp64_ach = flops / (t_ms * 1e-3) / 1e12
+        traffic = _profiled_traffic()
+        steps_ms = ms / args.steps
+        stage_share = {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in stage_tot.values())), 4)
+                       for k, v in stage_tot.items()}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = _cpu_baseline(s, args.cpu_sample, seed=77)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": steps_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian pseudo-atoms, exact ground state)",
+            "config": _config(args, {"parallelism": f"perturbation shards x{world}", "npw": npw,
+                                     "cg_iterations": iters, "system_build_s": round(t_sys, 1)}),
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(m * npw * 16),
+                    "d2h_bytes_per_step": int(m * npw * 16), "matches_device_path": e2e_ok},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "vloc FFT stage (k_zinv + k_plane_vloc + k_zfwd), per launch",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                         "algorithmic_bytes_per_launch": per_launch_bytes,
+                         "fp64": {"achieved_tflops_nominal": fp64_ach, "dgemm_peak_tflops": fp64_peak,
+                                  "frac": fp64_ach / fp64_peak}},
+            "stage_share": stage_share,
+            "work": {"cg_active_sum": act_sum, "fft_boxes": boxes},
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+    return line
+
+
+def main():
+    args = _args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, rank, world)
+        else:
+            line = run_b200(args, rank, world, local_rank)
+        if line is not None and rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+def _profiled_traffic():
+    """DRAM bytes per launch of the vloc FFT stage from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "vloc_fft_traffic.json")
+    try:
+        return json.load(open(p))["dram_bytes_per_launch"]
+    except Exception:
+        return None
+
+
+if __name__ == "__main__":
+    main()

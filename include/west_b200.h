@@ -59,13 +59,30 @@ typedef struct wb_system {
   double wk;           /* k_grid%weight(1) (QE wk; 2 for a spin-unpolarised Gamma) */
 } wb_system;
 
+/* Pipeline stages timed by wb_set_profiling (CUDA events on the library's stream). */
+#define WB_STAGE_VLOC_ZINV 0   /* local potential: sphere -> sticks, inverse z FFT   */
+#define WB_STAGE_VLOC_PLANE 1  /* local potential: x-y FFTs, V(r) product, back      */
+#define WB_STAGE_VLOC_ZFWD 2   /* local potential: forward z FFT, unpack, kinetic    */
+#define WB_STAGE_GEMM_TN 3     /* <W|X> bra-ket GEMM (calbec, Pv, Pc)                */
+#define WB_STAGE_GEMM_REDUCE 4 /* split-K reduction, Gamma G=0 term, D / alpha       */
+#define WB_STAGE_GEMM_NN 5     /* W C accumulation (add_vuspsi, Pv, Pc)              */
+#define WB_STAGE_CG 6          /* PCG vector steps and compaction                    */
+#define WB_STAGE_RHS 7         /* dv(r), psi_v dv products, forward FFTs             */
+#define WB_STAGE_DRHO 8        /* density response and its forward FFT               */
+#define WB_STAGE_OTHER 9       /* permutation, Pc, preconditioner, copies            */
+#define WB_NSTAGES 10
+
 /* Counters of the last wb_apply_operator call. */
 typedef struct wb_stats {
   int m;                   /* perturbations processed                         */
   int cg_iterations;       /* PCG iterations of the longest chunk             */
   long long cg_active_sum; /* sum over iterations of active (pert, band) systems */
   long long fft_boxes;     /* complex 3D box transforms performed             */
+  long long launches;      /* kernel launches issued by the library           */
   double ms_total;         /* device time of the call (ms, CUDA events)       */
+  double stage_ms[WB_NSTAGES];          /* per-stage device time (profiling on) */
+  long long stage_launches[WB_NSTAGES]; /* per-stage kernel launches            */
+  long long stage_items[WB_NSTAGES];    /* per-stage work items (FFT boxes, columns) */
 } wb_stats;
 
 /*
@@ -104,6 +121,9 @@ int wb_set_precision(wb_ctx* ctx, int mode);
 int wb_set_batch(wb_ctx* ctx, int max_perturbations);
 
 int wb_get_stats(const wb_ctx* ctx, wb_stats* out);
+
+/* 0 = off (default); 1 = time every pipeline stage with CUDA events. */
+int wb_set_profiling(wb_ctx* ctx, int level);
 
 /* Message of the last failed call in this thread ("" if none). */
 const char* wb_last_error(void);

@@ -77,6 +77,20 @@ struct wb_ctx {
   int* nact_host = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   wb_stats stats{};
+  // stage profiling: event pairs recorded on the stream, resolved after the call
+  int prof = 0;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+  struct Mark { int stage, e0, e1; };
+  std::vector<Mark> marks;
+  int ev_get() {
+    if (evused == evpool.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      evpool.push_back(e);
+    }
+    return (int)evused++;
+  }
 };
 
 namespace {
@@ -198,6 +212,38 @@ int upload(const T* h, size_t n, DBuf& d) {
   return WB_OK;
 }
 
+// Accounts one pipeline stage: launches and work items always, device time
+// when profiling is on.
+struct Stage {
+  wb_ctx* c;
+  int st, e0 = -1;
+  Stage(wb_ctx* c_, int st_, int launches, long long items) : c(c_), st(st_) {
+    c->stats.stage_launches[st] += launches;
+    c->stats.stage_items[st] += items;
+    c->stats.launches += launches;
+    if (c->prof) {
+      e0 = c->ev_get();
+      if (e0 >= 0) cudaEventRecord(c->evpool[e0], c->stream);
+    }
+  }
+  ~Stage() {
+    if (e0 < 0) return;
+    const int e1 = c->ev_get();
+    if (e1 < 0) return;
+    cudaEventRecord(c->evpool[e1], c->stream);
+    c->marks.push_back({st, e0, e1});
+  }
+};
+
+void resolve_marks(wb_ctx* c) {
+  for (auto& mk : c->marks) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->evpool[mk.e0], c->evpool[mk.e1]) == cudaSuccess) c->stats.stage_ms[mk.stage] += ms;
+  }
+  c->marks.clear();
+  c->evused = 0;
+}
+
 void pair_items(std::vector<int2>& it, int base, int n) {
   for (int k = 0; k < (n + 1) / 2; ++k) it.push_back(make_int2(base + 2 * k, (2 * k + 1 < n) ? base + 2 * k + 1 : -1));
 }
@@ -265,22 +311,41 @@ void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const i
   int M = c->nproj, nkb = c->nkb;
   const double* Wsub = W;
   if (c->kinetic_only) {
+    Stage g(c, WB_STAGE_VLOC_ZFWD, 1, n);
     kinetic_hpsi(Xv, Tv, c->g2kin.as<double>(), c->ecol.as<double>(), cols, n, c->npw, ld, s);
     Wsub = W + (size_t)c->nkb * K;  // alpha Pv only
     M = c->nocc;
     nkb = 0;
   } else {
     const int nit = (n + 1) / 2;
-    fft_zinv(c->fa, Xv, ld, items, nit, c->sticks.as<double2>());
-    fft_plane_vloc(c->fa, c->sticks.as<double2>(), nit, c->vs.as<double>());
-    fft_zfwd_hpsi(c->fa, c->sticks.as<double2>(), items, nit, Xv, Tv, ld, c->g2kin.as<double>(),
-                  c->ecol.as<double>());
+    {
+      Stage g(c, WB_STAGE_VLOC_ZINV, 1, nit);
+      fft_zinv(c->fa, Xv, ld, items, nit, c->sticks.as<double2>());
+    }
+    {
+      Stage g(c, WB_STAGE_VLOC_PLANE, 1, nit);
+      fft_plane_vloc(c->fa, c->sticks.as<double2>(), nit, c->vs.as<double>());
+    }
+    {
+      Stage g(c, WB_STAGE_VLOC_ZFWD, 1, nit);
+      fft_zfwd_hpsi(c->fa, c->sticks.as<double2>(), items, nit, Xv, Tv, ld, c->g2kin.as<double>(),
+                    c->ecol.as<double>());
+    }
     c->stats.fft_boxes += 2 * nit;
   }
-  gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s);
-  gamma_reduce(c->part.as<double>(), nsplit, M, n, Wsub, K, (const double*)Xv, 2 * ld, cols, c->D.as<double>(), nkb,
-               c->alpha, c->C.as<double>(), s);
-  gemm_nn(Wsub, K, M, c->C.as<double>(), (double*)Tv, 2 * ld, cols, n, K, 1.0, s);
+  {
+    Stage g(c, WB_STAGE_GEMM_TN, 1, n);
+    gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s);
+  }
+  {
+    Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
+    gamma_reduce(c->part.as<double>(), nsplit, M, n, Wsub, K, (const double*)Xv, 2 * ld, cols, c->D.as<double>(),
+                 nkb, c->alpha, c->C.as<double>(), s);
+  }
+  {
+    Stage g(c, WB_STAGE_GEMM_NN, 1, n);
+    gemm_nn(Wsub, K, M, c->C.as<double>(), (double*)Tv, 2 * ld, cols, n, K, 1.0, s);
+  }
   (void)nsys;
 }
 
@@ -304,61 +369,88 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
   double2* G = c->G.as<double2>();
   double2* T = c->T.as<double2>();
   double2* stk = c->sticks.as<double2>();
-  fill_columns(c->et.as<double>(), nocc, nsys, c->ecol.as<double>(), s);
-  fill_columns(c->eprec.as<double>(), nocc, nsys, c->epcol.as<double>(), s);
-  // 1. aux = sqvc * dvg in internal order            (apply_operator.f90:49-53)
-  permute_scale(dvg, ld_in, c->perm.as<int>(), c->sqvc.as<double>(), npw, mb, aux, ld, s);
-  // 2. dv(r) of perturbation pairs                   (dfpt_module.f90:235)
-  fft_zinv(c->fa, aux, ld, c->items_pp.as<int2>(), mp, stk);
-  fft_plane_inv_box(c->fa, stk, mp, c->dvbox.as<double2>());
-  // 3. dvpsi = P_G[psi_v(r) dv(r)]                    (dfpt_module.f90:245-278)
-  fft_plane_rhs(c->fa, c->evcr.as<double2>(), c->dvbox.as<double2>(), npv, mb, stk);
-  fft_zfwd_store(c->fa, stk, c->items_pk.as<int2>(), mb * npv, B, ld);
+  {
+    Stage g(c, WB_STAGE_OTHER, 3, mb);
+    fill_columns(c->et.as<double>(), nocc, nsys, c->ecol.as<double>(), s);
+    fill_columns(c->eprec.as<double>(), nocc, nsys, c->epcol.as<double>(), s);
+    // 1. aux = sqvc * dvg in internal order            (apply_operator.f90:49-53)
+    permute_scale(dvg, ld_in, c->perm.as<int>(), c->sqvc.as<double>(), npw, mb, aux, ld, s);
+  }
+  {
+    Stage g(c, WB_STAGE_RHS, 4, mp + (long long)mb * npv);
+    // 2. dv(r) of perturbation pairs                   (dfpt_module.f90:235)
+    fft_zinv(c->fa, aux, ld, c->items_pp.as<int2>(), mp, stk);
+    fft_plane_inv_box(c->fa, stk, mp, c->dvbox.as<double2>());
+    // 3. dvpsi = P_G[psi_v(r) dv(r)]                    (dfpt_module.f90:245-278)
+    fft_plane_rhs(c->fa, c->evcr.as<double2>(), c->dvbox.as<double2>(), npv, mb, stk);
+    fft_zfwd_store(c->fa, stk, c->items_pk.as<int2>(), mb * npv, B, ld);
+  }
   c->stats.fft_boxes += mp + (long long)mb * npv;
   // 4. dvpsi <- -Pc dvpsi = -dvpsi + evc (evc^T dvpsi)  (dfpt_module.f90:346)
   const double* Wevc = c->W.as<double>() + (size_t)c->nkb * K;
   const int nsplit = gemm_tn_splits(c->nproj, nsys, K);
-  gemm_tn(Wevc, K, nocc, (const double*)B, 2 * ld, nullptr, nsys, K, nsplit, c->part.as<double>(), s);
-  gamma_reduce(c->part.as<double>(), nsplit, nocc, nsys, Wevc, K, (const double*)B, 2 * ld, nullptr, nullptr, 0, 1.0,
-               c->C.as<double>(), s);
-  gemm_nn(Wevc, K, nocc, c->C.as<double>(), (double*)B, 2 * ld, nullptr, nsys, K, -1.0, s);
-  // 5. dpsi = precondition(dvpsi)                    (dfpt_module.f90:348)
-  precondition(B, X, c->g2kin.as<double>(), c->epcol.as<double>(), npw, nsys, ld, s);
+  {
+    Stage g(c, WB_STAGE_OTHER, 4, nsys);
+    gemm_tn(Wevc, K, nocc, (const double*)B, 2 * ld, nullptr, nsys, K, nsplit, c->part.as<double>(), s);
+    gamma_reduce(c->part.as<double>(), nsplit, nocc, nsys, Wevc, K, (const double*)B, 2 * ld, nullptr, nullptr, 0,
+                 1.0, c->C.as<double>(), s);
+    gemm_nn(Wevc, K, nocc, c->C.as<double>(), (double*)B, 2 * ld, nullptr, nsys, K, -1.0, s);
+    // 5. dpsi = precondition(dvpsi)                    (dfpt_module.f90:348)
+    precondition(B, X, c->g2kin.as<double>(), c->epcol.as<double>(), npw, nsys, ld, s);
+  }
   // 6. PCG                                           (dfpt_module.f90:350-361)
   int iters = 0;
   if (tr2 >= 0.0) {
     unsigned char* conv = c->conv.as<unsigned char>();
     int* act = c->act.as<int>();
     int2* items = c->items.as<int2>();
-    cg_reset(conv, nsys, s);
-    cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+    {
+      Stage g(c, WB_STAGE_CG, 2, nsys);
+      cg_reset(conv, nsys, s);
+      cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+    }
     apply_A(c, X, T, act, items, nsys, nsys, nsplit);            // :127
-    sub_into(T, B, G, npw, nsys, ld, s);                         // :130-138
+    {
+      Stage g(c, WB_STAGE_CG, 1, nsys);
+      sub_into(T, B, G, npw, nsys, ld, s);                       // :130-138
+    }
     int nact = nsys;
     for (int it = 1; it <= c->maxiter; ++it) {                   // :146
-      cg_prec_rho(act, nact, G, B, c->g2kin.as<double>(), c->epcol.as<double>(), c->rho.as<double>(), conv, it, tr2,
-                  npw, ld, s);
-      cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+      {
+        Stage g(c, WB_STAGE_CG, 2, nact);
+        cg_prec_rho(act, nact, G, B, c->g2kin.as<double>(), c->epcol.as<double>(), c->rho.as<double>(), conv, it,
+                    tr2, npw, ld, s);
+        cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+      }
       WB_CU(cudaStreamSynchronize(s));
       nact = *c->nact_host;
       iters = it;
       if (nact == 0) break;                                      // :222
       c->stats.cg_active_sum += nact;
       apply_A(c, B, T, act, items, nact, nsys, nsplit);          // :251
-      cg_update(act, nact, X, G, B, T, npw, ld, s);              // :253-329
+      {
+        Stage g(c, WB_STAGE_CG, 1, nact);
+        cg_update(act, nact, X, G, B, T, npw, ld, s);            // :253-329
+      }
     }
-    count_unconverged(conv, nocc, mb, c->unconv.as<int>(), s);
+    {
+      Stage g(c, WB_STAGE_CG, 1, mb);
+      count_unconverged(conv, nocc, mb, c->unconv.as<int>(), s);
+    }
   } else {
     WB_CU(cudaMemsetAsync(c->unconv.p, 0, sizeof(int) * mb, s));
   }
   c->stats.cg_iterations = std::max(c->stats.cg_iterations, iters);
   // 7. drho and dng                                   (dfpt_module.f90:403-487)
-  fft_zinv(c->fa, X, ld, c->items_pk.as<int2>(), mb * npv, stk);
-  const double scale = 2.0 * c->wk / c->omega / ((double)N * N * N);
-  fft_plane_drho(c->fa, stk, c->evcr.as<double2>(), c->occ.as<double>(), nocc, mb, c->acc.as<double2>(), scale,
-                 c->sticks2.as<double2>());
-  fft_zfwd_dng(c->fa, c->sticks2.as<double2>(), c->items_pp.as<int2>(), mp, dng, ld_out, c->perm.as<int>(),
-               c->sqvc.as<double>());
+  {
+    Stage g(c, WB_STAGE_DRHO, 3, (long long)mb * npv + mp);
+    fft_zinv(c->fa, X, ld, c->items_pk.as<int2>(), mb * npv, stk);
+    const double scale = 2.0 * c->wk / c->omega / ((double)N * N * N);
+    fft_plane_drho(c->fa, stk, c->evcr.as<double2>(), c->occ.as<double>(), nocc, mb, c->acc.as<double2>(), scale,
+                   c->sticks2.as<double2>());
+    fft_zfwd_dng(c->fa, c->sticks2.as<double2>(), c->items_pp.as<int2>(), mp, dng, ld_out, c->perm.as<int>(),
+                 c->sqvc.as<double>());
+  }
   c->stats.fft_boxes += (long long)mb * npv + mp;
   if (unconv_host) WB_CU(cudaMemcpyAsync(unconv_host, c->unconv.p, sizeof(int) * mb, cudaMemcpyDeviceToHost, s));
   return WB_OK;
@@ -376,6 +468,8 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
   if (c->precision != WB_PRECISION_FP64) return fail(WB_ERR_UNSUPPORTED, "mixed precision is not built yet");
   WB_CU(cudaSetDevice(c->device));
   c->stats = wb_stats{};
+  c->marks.clear();
+  c->evused = 0;
   c->stats.m = m;
   if (m == 0) return WB_OK;
   cudaStream_t s = c->stream;
@@ -414,6 +508,7 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->stats.ms_total = ms;
+  resolve_marks(c);
   WB_CU(cudaGetLastError());
   if (unconverged) std::memcpy(unconverged, unc.data(), sizeof(int) * m);
   return WB_OK;
@@ -535,6 +630,7 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->iota_items};
   for (DBuf* b : bufs) b->release();
   if (c->nact_host) cudaFreeHost(c->nact_host);
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -563,6 +659,13 @@ int wb_set_batch(wb_ctx* c, int maxp) {
   if (!c) return fail(WB_ERR_ARG, "null context");
   if (maxp < 0) return fail(WB_ERR_ARG, "negative batch");
   c->batch_cap = maxp;
+  return WB_OK;
+}
+
+int wb_set_profiling(wb_ctx* c, int level) {
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  if (level < 0 || level > 1) return fail(WB_ERR_ARG, "profiling level must be 0 or 1");
+  c->prof = level;
   return WB_OK;
 }
 

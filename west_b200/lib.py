@@ -22,8 +22,11 @@ WB_PRECISION_MIXED = 1
 # Every symbol include/west_b200.h declares.
 EXPORTS = (
     "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
-    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_last_error", "wb_version",
+    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling", "wb_last_error", "wb_version",
 )
+NSTAGES = 10
+STAGES = ("vloc_zinv", "vloc_plane", "vloc_zfwd", "gemm_tn", "gemm_reduce", "gemm_nn", "cg", "rhs", "drho",
+          "other")
 
 _p = ctypes.c_void_p
 _i = ctypes.c_int
@@ -42,7 +45,9 @@ class WbSystem(ctypes.Structure):
 
 class WbStats(ctypes.Structure):
     _fields_ = [("m", _i), ("cg_iterations", _i), ("cg_active_sum", ctypes.c_longlong),
-                ("fft_boxes", ctypes.c_longlong), ("ms_total", _d)]
+                ("fft_boxes", ctypes.c_longlong), ("launches", ctypes.c_longlong), ("ms_total", _d),
+                ("stage_ms", _d * 10), ("stage_launches", ctypes.c_longlong * 10),
+                ("stage_items", ctypes.c_longlong * 10)]
 
 
 class WestB200Error(RuntimeError):
@@ -68,6 +73,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         getattr(lib, name).argtypes = [_p, _i, _p, _i, _p, _i, _d, _i, _p]
     lib.wb_set_precision.argtypes = [_p, _i]
     lib.wb_set_batch.argtypes = [_p, _i]
+    lib.wb_set_profiling.argtypes = [_p, _i]
     lib.wb_get_stats.argtypes = [_p, ctypes.POINTER(WbStats)]
     lib.wb_last_error.restype = ctypes.c_char_p
     lib.wb_last_error.argtypes = []

@@ -87,10 +87,16 @@ class ResponseOperator:
     def set_batch(self, max_perturbations: int):
         _lib.check(self._lib.wb_set_batch(self._ctx, int(max_perturbations)))
 
+    def set_profiling(self, level: int):
+        _lib.check(self._lib.wb_set_profiling(self._ctx, int(level)))
+
     def stats(self) -> dict:
         st = _lib.WbStats()
         _lib.check(self._lib.wb_get_stats(self._ctx, ctypes.byref(st)))
-        return {k: getattr(st, k) for k, _ in st._fields_}
+        out = {k: getattr(st, k) for k, _ in st._fields_ if not k.startswith("stage_")}
+        out["stages"] = {name: {"ms": st.stage_ms[i], "launches": st.stage_launches[i],
+                                "items": st.stage_items[i]} for i, name in enumerate(_lib.STAGES)}
+        return out
 
     def apply_operator(self, m, dvg, dng, tr2, iq=1):
         """dng <- sqvc chi0 sqvc dvg for m columns; returns ierr[m]."""
