@@ -145,7 +145,7 @@ def test_oracle_regression_fixture():
     s = build_system("tiny")
     np.testing.assert_allclose(np.abs(s.evc), np.abs(g["evc"]), atol=1e-10)
     s.evc = g["evc"]; s.et = g["et"]
-    for tag, tr2, maxit in (("lite", -1.0, 250), ("tr2_1e-12", 1e-12, 250), ("fixed8", 0.0, 8)):
+    for tag, tr2, maxit in (("lite", -1.0, 250), ("tr2_1e-12", 1e-12, 250), ("fixed5", 0.0, 5)):
         dng, ierr = O.apply_operator(s, g["dvg"], tr2, maxiter=maxit)
         ref = g["dng_" + tag]
         assert np.abs(dng - ref).max() <= 1e-10 * np.abs(ref).max()

@@ -111,30 +111,44 @@ WB_DEV void rdft(double2* v, const double2* twN) {
   }
 }
 
-// Batched line FFTs in shared memory.  Line l starts at data + off(l) and has
-// element stride es.  LINE_FAST puts consecutive threads on consecutive lines
-// (use it when lines are adjacent in memory, e.g. columns of a row-major
-// plane); otherwise consecutive threads walk along one line.
-// Must be called by all NT threads of the block (contains barriers).
-template <int N, int DIR, int NT, bool LINE_FAST, class Off>
-WB_DEV void fft_lines(double2* data, Off off, int es, int nlines, const double2* twN) {
+// Element layout of one line in shared memory.  Element e = N2*a + b is stored
+// at (N2 + PAD)*a + b: with an odd block length, the N1 threads of step 2 (which
+// read elements N2*k1 + n2) hit distinct banks, as do the N2 threads of step 1.
+template <int N>
+struct LinePad {
+  static constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
+  static constexpr int PAD = (N2 % 2 == 0) ? 1 : 0;
+  static constexpr int LEN = N1 * (N2 + PAD);  // stored length of a line
+  WB_DEV static int off(int e) { return (e / N2) * (N2 + PAD) + (e % N2); }
+  WB_DEV static int off_blk(int a, int b) { return (N2 + PAD) * a + b; }
+};
+
+// Batched line FFTs in shared memory.  Line l starts at data + loff(l).
+// Elements of a line are either padded-contiguous (PADDED, LinePad layout,
+// element stride 1) or strided by es with no padding (columns of a plane,
+// where consecutive threads take consecutive lines).  LINE_FAST puts
+// consecutive threads on consecutive lines.  Must be called by all NT threads
+// of the block (contains barriers).
+template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, class Off>
+WB_DEV void fft_lines(double2* data, Off loff, int es, int nlines, const double2* twN) {
+  using LP = LinePad<N>;
   constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
   const int tid = threadIdx.x;
-  // step 1: N1-point DFTs, thread-private
+  // step 1: N1-point DFTs over elements N2*n1 + n2, thread-private
   const int items1 = nlines * N2;
   for (int it = tid; it < items1; it += NT) {
     int line, n2;
     if (LINE_FAST) { line = it % nlines; n2 = it / nlines; }
     else { line = it / N2; n2 = it % N2; }
-    double2* p = data + off(line);
+    double2* p = data + loff(line);
     double2 v[N1];
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[n1] = p[(N2 * n1 + n2) * es];
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = p[PADDED ? LP::off_blk(n1, n2) : (N2 * n1 + n2) * es];
     rdft<N1, DIR, N>(v, twN);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) v[k1] = ctw<DIR>(v[k1], twN[(n2 * k1) % N]);
 #pragma unroll
-    for (int k1 = 0; k1 < N1; ++k1) p[(N2 * k1 + n2) * es] = v[k1];
+    for (int k1 = 0; k1 < N1; ++k1) p[PADDED ? LP::off_blk(k1, n2) : (N2 * k1 + n2) * es] = v[k1];
   }
   __syncthreads();
   // step 2: N2-point DFTs, one line's N1 work items inside one chunk
@@ -146,16 +160,16 @@ WB_DEV void fft_lines(double2* data, Off off, int es, int nlines, const double2*
     else { line = c * LPC + tid / N1; k1 = tid % N1; }
     const bool act = (tid < LPC * N1) && (line < nlines);
     double2 v[N2];
-    double2* p = data + (act ? off(line) : 0);
+    double2* p = data + (act ? loff(line) : 0);
     if (act) {
 #pragma unroll
-      for (int n2 = 0; n2 < N2; ++n2) v[n2] = p[(N2 * k1 + n2) * es];
+      for (int n2 = 0; n2 < N2; ++n2) v[n2] = p[PADDED ? LP::off_blk(k1, n2) : (N2 * k1 + n2) * es];
       rdft<N2, DIR, N>(v, twN);
     }
     __syncthreads();
     if (act) {
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) p[(k1 + N1 * k2) * es] = v[k2];
+      for (int k2 = 0; k2 < N2; ++k2) p[PADDED ? LP::off(k1 + N1 * k2) : (k1 + N1 * k2) * es] = v[k2];
     }
   }
   __syncthreads();
@@ -165,11 +179,21 @@ struct OffLinear {
   int stride;
   WB_DEV int operator()(int l) const { return l * stride; }
 };
-// Active columns of a plane: x in [0, xhi] and [N - xlo, N).
+// Active columns of a padded plane: x in [0, xhi] and [N - (ncols - nlow), N).
+template <int N>
 struct OffCols {
-  int nlow, n;  // nlow = xhi + 1 columns from 0, the rest from n - (ncols - nlow)
-  int ncols;
-  WB_DEV int operator()(int l) const { return l < nlow ? l : n - ncols + l; }
+  int nlow, ncols;
+  WB_DEV int operator()(int l) const { return LinePad<N>::off(l < nlow ? l : N - ncols + l); }
+};
+
+// Plane of N x N complex values: rows are padded lines (LinePad), row stride RS.
+template <int N>
+struct Plane {
+  static constexpr int RS = LinePad<N>::LEN;
+  static constexpr int SIZE = N * RS;
+  WB_DEV static int at(int x, int y) { return y * RS + LinePad<N>::off(x); }
+  // plane offset of the e-th element in row-major (y*N + x) order
+  WB_DEV static int at_lin(int e) { return at(e % N, e / N); }
 };
 
 }  // namespace wb

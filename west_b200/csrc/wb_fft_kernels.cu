@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, l
                                               const int2* __restrict__ items, StickTab st,
                                               double2* __restrict__ out,
                                               const double2* __restrict__ twg) {
-  constexpr int LS = N + 1;  // padded line stride (odd: conflict-free column reads)
+  constexpr int LS = LinePad<N>::LEN | 1;  // odd line stride: conflict-free transposes
   extern __shared__ double2 sm[];
   double2* tw = sm;
   double2* zb = sm + N;
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, l
   const int q0 = blockIdx.x * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
   load_tw<N>(tw, twg);
-  for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = make_double2(0.0, 0.0);  // pads too
   __syncthreads();
   const int2 it = items[item];
   const double2* a = src + (long)it.x * ld;
@@ -64,22 +64,23 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, l
     const double2 pos = make_double2(a1.x - a2.y, a1.y + a2.x);
     const double2 neg = make_double2(a1.x + a2.y, a2.x - a1.y);
     const int z = qz.y;
+    using LP = LinePad<N>;
     if (qz.x < 2) {  // the (0,0) stick is its own mirror
-      if (z != 0) { zb[(z + N) % N] = pos; zb[(N - z) % N] = neg; }
+      if (z != 0) { zb[LP::off((z + N) % N)] = pos; zb[LP::off((N - z) % N)] = neg; }
       else zb[0] = neg;  // G = 0: the -G store wins, as in the reference loop
     } else {
       const int l = qz.x - 2 * q0;  // slot of the stick holding G; its mirror is l ^ 1
-      zb[l * LS + ((z + N) % N)] = pos;
-      zb[(l ^ 1) * LS + ((N - z) % N)] = neg;
+      zb[l * LS + LP::off((z + N) % N)] = pos;
+      zb[(l ^ 1) * LS + LP::off((N - z) % N)] = neg;
     }
   }
   __syncthreads();
-  fft_lines<N, +1, ZNT, false>(zb, OffLinear{LS}, 1, 2 * nq, tw);
+  fft_lines<N, +1, ZNT, false, true>(zb, OffLinear{LS}, 1, 2 * nq, tw);
   const int ns = 2 * nq;
   double2* o = out + (long)item * N * st.nst + 2 * q0;
   for (int e = threadIdx.x; e < ns * N; e += ZNT) {
     const int s = e % ns, z = e / ns;
-    o[(long)z * st.nst + s] = zb[s * LS + z];
+    o[(long)z * st.nst + s] = zb[s * LS + LinePad<N>::off(z)];
   }
 }
 
@@ -90,7 +91,7 @@ template <int N, class Epi>
 __global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks,
                                               const int2* __restrict__ items, StickTab st,
                                               const double2* __restrict__ twg, Epi epi) {
-  constexpr int LS = N + 1;
+  constexpr int LS = LinePad<N>::LEN | 1;
   extern __shared__ double2 sm[];
   double2* tw = sm;
   double2* zb = sm + N;
@@ -102,23 +103,24 @@ __global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks
   const double2* s0 = sticks + (long)item * N * st.nst + 2 * q0;
   for (int e = threadIdx.x; e < ns * N; e += ZNT) {
     const int s = e % ns, z = e / ns;
-    zb[s * LS + z] = s0[(long)z * st.nst + s];
+    zb[s * LS + LinePad<N>::off(z)] = s0[(long)z * st.nst + s];
   }
   __syncthreads();
-  fft_lines<N, -1, ZNT, false>(zb, OffLinear{LS}, 1, ns, tw);
+  fft_lines<N, -1, ZNT, false, true>(zb, OffLinear{LS}, 1, ns, tw);
   const int2 it = items[item];
   const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
   for (int g = g0 + threadIdx.x; g < g1; g += ZNT) {
     const int2 qz = st.g_qz[g];
     const int z = qz.y;
+    using LP = LinePad<N>;
     double2 ap, am;
     if (qz.x < 2) {
-      ap = zb[(z + N) % N];
-      am = zb[(N - z) % N];
+      ap = zb[LP::off((z + N) % N)];
+      am = zb[LP::off((N - z) % N)];
     } else {
       const int l = qz.x - 2 * q0;
-      ap = zb[l * LS + ((z + N) % N)];
-      am = zb[(l ^ 1) * LS + ((N - z) % N)];
+      ap = zb[l * LS + LP::off((z + N) % N)];
+      am = zb[(l ^ 1) * LS + LP::off((N - z) % N)];
     }
     const double2 fp = make_double2(0.5 * (ap.x + am.x), 0.5 * (ap.y + am.y));
     const double2 fm = make_double2(0.5 * (ap.x - am.x), 0.5 * (ap.y - am.y));
@@ -177,27 +179,30 @@ struct EpiDng {
 // ---------------------------------------------------------------------------
 template <int N>
 WB_DEV void plane_zero(double2* pl) {
-  for (int e = threadIdx.x; e < N * N; e += PNT) pl[e] = make_double2(0.0, 0.0);
+  for (int e = threadIdx.x; e < Plane<N>::SIZE; e += PNT) pl[e] = make_double2(0.0, 0.0);
 }
+// stick positions are y*N + x in row-major plane order
+template <int N>
 WB_DEV void plane_scatter(double2* pl, const double2* __restrict__ sz, const int* __restrict__ pos, int nst) {
   for (int s = threadIdx.x; s < nst; s += PNT) {
     const int p = pos[s];
-    if (p >= 0) pl[p] = sz[s];
+    if (p >= 0) pl[Plane<N>::at_lin(p)] = sz[s];
   }
 }
+template <int N>
 WB_DEV void plane_gather(const double2* pl, double2* __restrict__ sz, const int* __restrict__ pos, int nst) {
   for (int s = threadIdx.x; s < nst; s += PNT) {
     const int p = pos[s];
-    sz[s] = p >= 0 ? pl[p] : make_double2(0.0, 0.0);
+    sz[s] = p >= 0 ? pl[Plane<N>::at_lin(p)] : make_double2(0.0, 0.0);
   }
 }
 template <int N, int DIR>
 WB_DEV void plane_fft_cols(double2* pl, const StickTab& st, const double2* tw) {
-  fft_lines<N, DIR, PNT, true>(pl, OffCols{st.xhi + 1, N, st.ncols}, N, st.ncols, tw);
+  fft_lines<N, DIR, PNT, true, false>(pl, OffCols<N>{st.xhi + 1, st.ncols}, Plane<N>::RS, st.ncols, tw);
 }
 template <int N, int DIR>
 WB_DEV void plane_fft_rows(double2* pl, const double2* tw) {
-  fft_lines<N, DIR, PNT, false>(pl, OffLinear{N}, 1, N, tw);
+  fft_lines<N, DIR, PNT, false, true>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
 }
 
 // psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma)
@@ -213,16 +218,19 @@ __global__ void __launch_bounds__(PNT) k_plane_vloc(double2* __restrict__ sticks
   load_tw<N>(tw, twg);
   plane_zero<N>(pl);
   __syncthreads();
-  plane_scatter(pl, sz, st.st_pos, st.nst);
+  plane_scatter<N>(pl, sz, st.st_pos, st.nst);
   __syncthreads();
   plane_fft_cols<N, +1>(pl, st, tw);
   plane_fft_rows<N, +1>(pl, tw);
   const double* v = vs + (long)z * N * N;
-  for (int e = threadIdx.x; e < N * N; e += PNT) pl[e] = cscale(pl[e], v[e]);
+  for (int e = threadIdx.x; e < N * N; e += PNT) {
+    const int o = Plane<N>::at_lin(e);
+    pl[o] = cscale(pl[o], v[e]);
+  }
   __syncthreads();
   plane_fft_rows<N, -1>(pl, tw);
   plane_fft_cols<N, -1>(pl, st, tw);
-  plane_gather(pl, sz, st.st_pos, st.nst);
+  plane_gather<N>(pl, sz, st.st_pos, st.nst);
 }
 
 // sticks -> full real-space box (complex: two real functions), no scaling
@@ -238,12 +246,12 @@ __global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict
   load_tw<N>(tw, twg);
   plane_zero<N>(pl);
   __syncthreads();
-  plane_scatter(pl, sz, st.st_pos, st.nst);
+  plane_scatter<N>(pl, sz, st.st_pos, st.nst);
   __syncthreads();
   plane_fft_cols<N, +1>(pl, st, tw);
   plane_fft_rows<N, +1>(pl, tw);
   double2* o = box + ((long)item * N + z) * N * N;
-  for (int e = threadIdx.x; e < N * N; e += PNT) o[e] = pl[e];
+  for (int e = threadIdx.x; e < N * N; e += PNT) o[e] = pl[Plane<N>::at_lin(e)];
 }
 
 // RHS of the Sternheimer equation, dfpt_module.f90:245-260:
@@ -265,13 +273,13 @@ __global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ e
   for (int e = threadIdx.x; e < N * N; e += PNT) {
     const double2 d = dv[e];
     const double w = (hi ? d.y : d.x) * inv;
-    pl[e] = cscale(ps[e], w);
+    pl[Plane<N>::at_lin(e)] = cscale(ps[e], w);
   }
   __syncthreads();
   plane_fft_rows<N, -1>(pl, tw);
   plane_fft_cols<N, -1>(pl, st, tw);
   const long item = (long)p * npv + k;
-  plane_gather(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+  plane_gather<N>(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
 }
 
 // Density response, dfpt_module.f90:403-423 and :478:
@@ -304,7 +312,7 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
       __syncthreads();
       plane_zero<N>(pl);
       __syncthreads();
-      plane_scatter(pl, dsticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+      plane_scatter<N>(pl, dsticks + (item * N + z) * st.nst, st.st_pos, st.nst);
       __syncthreads();
       plane_fft_cols<N, +1>(pl, st, tw);
       plane_fft_rows<N, +1>(pl, tw);
@@ -312,7 +320,7 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
       const double o2 = (2 * k + 1 < nocc) ? occ[2 * k + 1] : 0.0;
       const double2* ps = evcr + ((long)k * N + z) * N * N;
       for (int e = threadIdx.x; e < N * N; e += PNT) {
-        const double2 d = pl[e], s = ps[e];
+        const double2 d = pl[Plane<N>::at_lin(e)], s = ps[e];
         const double c = fma(o1 * s.x, d.x, o2 * s.y * d.y);
         if (pi == 0) {
           if (k == 0) ac[e].x = c; else ac[e].x += c;
@@ -323,20 +331,20 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < N * N; e += PNT) pl[e] = cscale(ac[e], scale);
+  for (int e = threadIdx.x; e < N * N; e += PNT) pl[Plane<N>::at_lin(e)] = cscale(ac[e], scale);
   __syncthreads();
   plane_fft_rows<N, -1>(pl, tw);
   plane_fft_cols<N, -1>(pl, st, tw);
-  plane_gather(pl, osticks + ((long)pp * N + z) * st.nst, st.st_pos, st.nst);
+  plane_gather<N>(pl, osticks + ((long)pp * N + z) * st.nst, st.st_pos, st.nst);
 }
 
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
 template <int N>
-static size_t zsmem() { return sizeof(double2) * (N + 2 * ZSG * (N + 1)); }
+static size_t zsmem() { return sizeof(double2) * (N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
 template <int N>
-static size_t psmem() { return sizeof(double2) * (N + N * N); }
+static size_t psmem() { return sizeof(double2) * (N + Plane<N>::SIZE); }
 
 template <int N>
 struct FftN {
