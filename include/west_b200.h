@@ -125,6 +125,27 @@ int wb_get_stats(const wb_ctx* ctx, wb_stats* out);
 /* 0 = off (default); 1 = time every pipeline stage with CUDA events. */
 int wb_set_profiling(wb_ctx* ctx, int level);
 
+/*
+ * Allocation-free form of wb_apply_operator_device.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory while
+ * they run (a host code whose GPU memory is owned by its own pool, a
+ * latency-bound loop that cannot take cudaMalloc's implicit synchronisation,
+ * an allocation policy that forbids allocations after set-up).  Same
+ * arguments and results as wb_apply_operator_device; dvg and dng are device
+ * buffers supplied by the caller.  Every per-call buffer comes from one
+ * file-scope device array of WB_NOALLOC_SCRATCH_BYTES that each GPU loading
+ * the library holds until the process exits; a call whose buffers do not fit
+ * returns WB_ERR_ARG with the size it would need.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that
+ * first call before any stream capture.  All calls, from every context on
+ * the device, share the one array and its leftover contents: calls that
+ * overlap on the GPU (other threads or streams) race and corrupt each other.
+ * Nothing is allocated by this call; the context (wb_ctx_create) must exist.
+ */
+#define WB_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int wb_apply_operator_device_noalloc(wb_ctx* ctx, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng,
+                                     double tr2, int iq, int* unconverged);
+
 /* Message of the last failed call in this thread ("" if none). */
 const char* wb_last_error(void);
 

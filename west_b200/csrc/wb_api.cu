@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -676,3 +677,219 @@ int wb_get_stats(const wb_ctx* c, wb_stats* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of wb_apply_operator_device.
+//
+// For callers that must not allocate device memory while they run: a host
+// code that has handed all of its GPU memory to its own pool allocator, a
+// real-time or latency-bound loop that cannot afford the implicit device
+// synchronisation of cudaMalloc/cudaFree, or a caller whose allocation
+// policy forbids allocations after set-up.  Every per-call buffer (stick
+// buffers, PCG vectors, GEMM partial sums, density accumulators, index
+// tables) is carved out of one file-scope __device__ array of
+// WB_NOALLOC_SCRATCH_BYTES; the context's constant data was allocated once by
+// wb_ctx_create.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[WB_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+struct NoallocDevice {
+  std::once_flag once;
+  void* ptr = nullptr;
+  cudaError_t err = cudaSuccess;
+};
+NoallocDevice g_noalloc_dev[kMaxDevices];
+
+// Device address of the scratch array on the current device, looked up once
+// per device.  The host-side name g_noalloc_scratch is only a stand-in for
+// the symbol: it must never be passed to a kernel.
+int noalloc_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kMaxDevices) return fail(WB_ERR_UNSUPPORTED, "device index too large for the scratch table");
+  NoallocDevice& d = g_noalloc_dev[dev];
+  std::call_once(d.once, [&d] { d.err = cudaGetSymbolAddress(&d.ptr, g_noalloc_scratch); });
+  if (d.err != cudaSuccess || d.ptr == nullptr)
+    return fail(WB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(d.err));
+  *out = static_cast<unsigned char*>(d.ptr);
+  return WB_OK;
+}
+
+// Bump carver over the scratch array (256-byte aligned pieces).  With a null
+// base it only measures.
+struct Carve {
+  unsigned char* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += sizeof(T) * n;
+    return p;
+  }
+};
+
+struct NoallocWs {
+  double2 *aux, *dvbox, *B, *X, *G, *T, *sticks, *sticks2, *acc;
+  double *part, *C, *rho, *ecol, *epcol;
+  unsigned char* conv;
+  int *act, *nact, *unconv;
+  int2 *items, *items_pp, *items_pk;
+  int nsplit;
+};
+
+void noalloc_layout(const wb_ctx* c, int mb, Carve& cv, NoallocWs& w) {
+  const size_t nsys = (size_t)mb * c->nocc;
+  const size_t npw = c->npw;
+  const size_t stk1 = (size_t)c->nr * c->st.nst;
+  const size_t mp = (mb + 1) / 2;
+  const size_t nitems = std::max<size_t>({(nsys + 1) / 2, (size_t)mb * c->npv, mp});
+  w.nsplit = gemm_tn_splits(c->nproj, (int)nsys, 2 * c->npw);
+  w.aux = cv.take<double2>(npw * mb);
+  w.dvbox = cv.take<double2>((size_t)c->nnr * mp);
+  w.B = cv.take<double2>(npw * nsys);
+  w.X = cv.take<double2>(npw * nsys);
+  w.G = cv.take<double2>(npw * nsys);
+  w.T = cv.take<double2>(npw * nsys);
+  w.sticks = cv.take<double2>(stk1 * nitems);
+  w.sticks2 = cv.take<double2>(stk1 * mp);
+  w.acc = cv.take<double2>((size_t)c->nnr * mp);
+  w.part = cv.take<double>((size_t)w.nsplit * nsys * c->nproj);
+  w.C = cv.take<double>(nsys * c->nproj);
+  w.rho = cv.take<double>(nsys);
+  w.ecol = cv.take<double>(nsys);
+  w.epcol = cv.take<double>(nsys);
+  w.conv = cv.take<unsigned char>(nsys);
+  w.act = cv.take<int>(nsys);
+  w.nact = cv.take<int>(4);
+  w.unconv = cv.take<int>(mb);
+  w.items = cv.take<int2>(nsys / 2 + 1);
+  w.items_pp = cv.take<int2>(mp);
+  w.items_pk = cv.take<int2>((size_t)mb * c->npv);
+}
+
+__global__ void k_noalloc_items(int2* __restrict__ pp, int2* __restrict__ pk, int mb, int nocc, int npv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int mp = (mb + 1) / 2;
+  if (i < mp) pp[i] = make_int2(2 * i, (2 * i + 1 < mb) ? 2 * i + 1 : -1);
+  if (i < mb * npv) {
+    const int p = i / npv, k = i % npv;
+    pk[i] = make_int2(p * nocc + 2 * k, (2 * k + 1 < nocc) ? p * nocc + 2 * k + 1 : -1);
+  }
+}
+
+// (H - e + alpha Pv) on the listed columns, with workspace from the scratch array.
+void noalloc_apply_A(wb_ctx* c, const NoallocWs& w, const double2* Xv, double2* Tv, const int* cols,
+                     const int2* items, int n) {
+  const long ld = c->npw;
+  const int K = 2 * c->npw;
+  cudaStream_t s = c->stream;
+  const double* Wsub = c->W.as<double>();
+  int M = c->nproj, nkb = c->nkb;
+  if (c->kinetic_only) {
+    kinetic_hpsi(Xv, Tv, c->g2kin.as<double>(), w.ecol, cols, n, c->npw, ld, s);
+    Wsub = c->W.as<double>() + (size_t)c->nkb * K;
+    M = c->nocc;
+    nkb = 0;
+  } else {
+    const int nit = (n + 1) / 2;
+    fft_zinv(c->fa, Xv, ld, items, nit, w.sticks);
+    fft_plane_vloc(c->fa, w.sticks, nit, c->vs.as<double>());
+    fft_zfwd_hpsi(c->fa, w.sticks, items, nit, Xv, Tv, ld, c->g2kin.as<double>(), w.ecol);
+  }
+  gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, w.nsplit, w.part, s);
+  gamma_reduce(w.part, w.nsplit, M, n, Wsub, K, (const double*)Xv, 2 * ld, cols, c->D.as<double>(), nkb, c->alpha,
+               w.C, s);
+  gemm_nn(Wsub, K, M, w.C, (double*)Tv, 2 * ld, cols, n, K, 1.0, s);
+}
+
+int noalloc_run(wb_ctx* c, const NoallocWs& w, int mb, const double2* dvg, long ld_in, double2* dng, long ld_out,
+                double tr2, int* unconv_host) {
+  cudaStream_t s = c->stream;
+  const int npw = c->npw, nocc = c->nocc, npv = c->npv, N = c->nr;
+  const int nsys = mb * nocc;
+  const long ld = npw;
+  const int K = 2 * npw;
+  const int mp = (mb + 1) / 2;
+  const int nit = std::max(mp, mb * npv);
+  k_noalloc_items<<<(nit + 255) / 256, 256, 0, s>>>(w.items_pp, w.items_pk, mb, nocc, npv);
+  fill_columns(c->et.as<double>(), nocc, nsys, w.ecol, s);
+  fill_columns(c->eprec.as<double>(), nocc, nsys, w.epcol, s);
+  permute_scale(dvg, ld_in, c->perm.as<int>(), c->sqvc.as<double>(), npw, mb, w.aux, ld, s);
+  fft_zinv(c->fa, w.aux, ld, w.items_pp, mp, w.sticks);
+  fft_plane_inv_box(c->fa, w.sticks, mp, w.dvbox);
+  fft_plane_rhs(c->fa, c->evcr.as<double2>(), w.dvbox, npv, mb, w.sticks);
+  fft_zfwd_store(c->fa, w.sticks, w.items_pk, mb * npv, w.B, ld);
+  const double* Wevc = c->W.as<double>() + (size_t)c->nkb * K;
+  gemm_tn(Wevc, K, nocc, (const double*)w.B, 2 * ld, nullptr, nsys, K, w.nsplit, w.part, s);
+  gamma_reduce(w.part, w.nsplit, nocc, nsys, Wevc, K, (const double*)w.B, 2 * ld, nullptr, nullptr, 0, 1.0, w.C, s);
+  gemm_nn(Wevc, K, nocc, w.C, (double*)w.B, 2 * ld, nullptr, nsys, K, -1.0, s);
+  precondition(w.B, w.X, c->g2kin.as<double>(), w.epcol, npw, nsys, ld, s);
+  int iters = 0;
+  if (tr2 >= 0.0) {
+    cg_reset(w.conv, nsys, s);
+    cg_compact(w.conv, nsys, w.act, w.items, w.nact, c->nact_host, s);
+    noalloc_apply_A(c, w, w.X, w.T, w.act, w.items, nsys);
+    sub_into(w.T, w.B, w.G, npw, nsys, ld, s);
+    int nact = nsys;
+    for (int it = 1; it <= c->maxiter; ++it) {
+      cg_prec_rho(w.act, nact, w.G, w.B, c->g2kin.as<double>(), w.epcol, w.rho, w.conv, it, tr2, npw, ld, s);
+      cg_compact(w.conv, nsys, w.act, w.items, w.nact, c->nact_host, s);
+      WB_CU(cudaStreamSynchronize(s));
+      nact = *c->nact_host;
+      iters = it;
+      if (nact == 0) break;
+      c->stats.cg_active_sum += nact;
+      noalloc_apply_A(c, w, w.B, w.T, w.act, w.items, nact);
+      cg_update(w.act, nact, w.X, w.G, w.B, w.T, npw, ld, s);
+    }
+    count_unconverged(w.conv, nocc, mb, w.unconv, s);
+  } else {
+    WB_CU(cudaMemsetAsync(w.unconv, 0, sizeof(int) * mb, s));
+  }
+  c->stats.cg_iterations = std::max(c->stats.cg_iterations, iters);
+  fft_zinv(c->fa, w.X, ld, w.items_pk, mb * npv, w.sticks);
+  const double scale = 2.0 * c->wk / c->omega / ((double)N * N * N);
+  fft_plane_drho(c->fa, w.sticks, c->evcr.as<double2>(), c->occ.as<double>(), nocc, mb, w.acc, scale, w.sticks2);
+  fft_zfwd_dng(c->fa, w.sticks2, w.items_pp, mp, dng, ld_out, c->perm.as<int>(), c->sqvc.as<double>());
+  if (unconv_host) WB_CU(cudaMemcpyAsync(unconv_host, w.unconv, sizeof(int) * mb, cudaMemcpyDeviceToHost, s));
+  WB_CU(cudaStreamSynchronize(s));
+  WB_CU(cudaGetLastError());
+  return WB_OK;
+}
+
+}  // namespace
+
+extern "C" int wb_apply_operator_device_noalloc(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng,
+                                                int ld_dng, double tr2, int iq, int* unconverged) {
+  g_err.clear();
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  if (m < 0) return fail(WB_ERR_ARG, "m < 0");
+  if (iq != 1) return fail(WB_ERR_UNSUPPORTED, "only iq = 1 (Gamma) is provided");
+  if (m > 0 && (!dvg || !dng)) return fail(WB_ERR_ARG, "null dvg or dng");
+  if (ld_dvg < c->npw || ld_dng < c->npw) return fail(WB_ERR_ARG, "leading dimension smaller than npw");
+  if (std::isnan(tr2)) return fail(WB_ERR_ARG, "tr2 is NaN");
+  if (c->precision != WB_PRECISION_FP64) return fail(WB_ERR_UNSUPPORTED, "mixed precision is not built yet");
+  Carve probe{nullptr};
+  NoallocWs w{};
+  noalloc_layout(c, std::max(m, 1), probe, w);
+  if (probe.off > (size_t)WB_NOALLOC_SCRATCH_BYTES)
+    return fail(WB_ERR_ARG, "this call needs " + std::to_string(probe.off) + " bytes of scratch; the allocation-free "
+                "entry point has " + std::to_string((size_t)WB_NOALLOC_SCRATCH_BYTES) +
+                " (WB_NOALLOC_SCRATCH_BYTES): use fewer perturbations per call");
+  WB_CU(cudaSetDevice(c->device));
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(c->device, &base);
+  if (rc) return rc;
+  c->stats = wb_stats{};
+  c->stats.m = m;
+  if (m == 0) return WB_OK;
+  Carve cv{base};
+  noalloc_layout(c, m, cv, w);
+  if (ld_dng > c->npw)
+    WB_CU(cudaMemset2DAsync(reinterpret_cast<double2*>(dng) + c->npw, sizeof(double2) * ld_dng, 0,
+                            sizeof(double2) * (ld_dng - c->npw), m, c->stream));
+  return noalloc_run(c, w, m, reinterpret_cast<const double2*>(dvg), ld_dvg, reinterpret_cast<double2*>(dng), ld_dng,
+                     tr2, unconverged);
+}

@@ -18,10 +18,12 @@ WB_ERR_UNSUPPORTED = -3
 WB_ERR_NOMEM = -4
 WB_PRECISION_FP64 = 0
 WB_PRECISION_MIXED = 1
+WB_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 # Every symbol include/west_b200.h declares.
 EXPORTS = (
     "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
+    "wb_apply_operator_device_noalloc",
     "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling", "wb_last_error", "wb_version",
 )
 NSTAGES = 10
@@ -69,7 +71,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib = ctypes.CDLL(path)
     lib.wb_ctx_create.argtypes = [ctypes.POINTER(_p), ctypes.POINTER(WbSystem), _i]
     lib.wb_ctx_destroy.argtypes = [_p]
-    for name in ("wb_apply_operator", "wb_apply_operator_device"):
+    for name in ("wb_apply_operator", "wb_apply_operator_device", "wb_apply_operator_device_noalloc"):
         getattr(lib, name).argtypes = [_p, _i, _p, _i, _p, _i, _d, _i, _p]
     lib.wb_set_precision.argtypes = [_p, _i]
     lib.wb_set_batch.argtypes = [_p, _i]
