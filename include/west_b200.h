@@ -122,8 +122,10 @@ int wb_set_batch(wb_ctx* ctx, int max_perturbations);
 
 int wb_get_stats(const wb_ctx* ctx, wb_stats* out);
 
-/* 0 = off (default); 1 = time every pipeline stage with CUDA events. */
-int wb_set_profiling(wb_ctx* ctx, int level);
+/* Bit mask of the WB_STAGE_* stages to time with CUDA events (bit s = stage s);
+ * 0 = off (default), WB_PROFILE_ALL = every stage. */
+#define WB_PROFILE_ALL ((1 << WB_NSTAGES) - 1)
+int wb_set_profiling(wb_ctx* ctx, int stage_mask);
 
 /*
  * Allocation-free form of wb_apply_operator_device.  No counterpart in the
@@ -145,6 +147,40 @@ int wb_set_profiling(wb_ctx* ctx, int level);
 #define WB_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int wb_apply_operator_device_noalloc(wb_ctx* ctx, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng,
                                      double tr2, int iq, int* unconverged);
+
+/* PDEP Davidson input keys (westcom wstat_control; Pytools/west_fetch_input.py:31-46). */
+typedef struct wb_davidson_params {
+  int n_pdep_eigen;    /* nvec: PDEP eigenpairs wanted                          */
+  int n_pdep_basis;    /* nvecx = n_pdep_eigen * n_pdep_times                   */
+  int n_pdep_maxiter;  /* Davidson iterations                                   */
+  double tr2_dfpt;     /* PCG threshold of the iterations                        */
+  double trev_pdep;    /* absolute eigenvalue convergence                        */
+  double trev_pdep_rel;/* relative eigenvalue convergence                        */
+} wb_davidson_params;
+
+/* What davidson_diago_gamma reports (exec.davitr of wstat.json). */
+typedef struct wb_davidson_info {
+  int dav_iter;             /* iterations run                                   */
+  int notcnv;               /* roots still unconverged at exit                  */
+  int converged;            /* 1 when every root converged                      */
+  int apply_calls;          /* apply_operator calls                             */
+  long long perturbations;  /* columns pushed through apply_operator            */
+  double seconds;           /* wall time of the solve                           */
+} wb_davidson_info;
+
+/*
+ * The PDEP Davidson eigensolver, davidson_diago_gamma (Wstat/davidson_diago.f90:31-437)
+ * with do_mgs (:909), build_hr_real (Wstat/wstat_tools.f90:345), diagox_dsy (:48),
+ * redistribute_vr_distr_real (:591), update_with_vr_distr_real (:945) and
+ * refresh_with_vr_distr_real (:1245), on one GPU.  dvg0 [ld_dvg0, n_pdep_eigen] is
+ * the randomised starting basis (do_randomize, davidson_diago.f90:1121, host
+ * memory).  Returns the n_pdep_eigen lowest eigenvalues of sqvc chi0 sqvc in
+ * ev, their convergence flags in conv and, when pdep != NULL, the eigenvectors
+ * [ld_pdep, n_pdep_eigen] (host memory).  The subspace eigensolver is a
+ * Jacobi method on the GPU (diagox uses LAPACK DSYEV / cuSOLVER in WEST).
+ */
+int wb_davidson(wb_ctx* ctx, const wb_davidson_params* params, const double* dvg0, int ld_dvg0, double* ev,
+                int* conv, double* pdep, int ld_pdep, wb_davidson_info* info);
 
 /* Message of the last failed call in this thread ("" if none). */
 const char* wb_last_error(void);

@@ -320,3 +320,119 @@ def apply_operator(s, dvg, tr2, maxiter=250, kinetic_only=False, trace=None):
     aux_g = dvg * s.sqvc[:, None]                           # :49-53
     dng, ierr = dfpt(s, aux_g, tr2, maxiter, kinetic_only, trace=trace)  # :58
     return dng * s.sqvc[:, None], ierr                      # :63-67
+
+
+# ----------------------------------------------------------------------------
+# PDEP Davidson (Wstat/davidson_diago.f90, Wstat/wstat_tools.f90), one image
+# ----------------------------------------------------------------------------
+def do_mgs(amat, start, end):
+    """davidson_diago.f90:909-1117: modified Gram-Schmidt of columns [start, end)
+    against [0, start) and among themselves, Gamma dot products; in place."""
+    for k in range(end):
+        if k >= start:                                                   # :1003-1031
+            a = amat[:, k]
+            anorm = 2.0 * (a.real ** 2 + a.imag ** 2).sum() - a[0].real ** 2
+            amat[:, k] = a * (1.0 / np.sqrt(anorm))
+        vec = amat[:, k].copy()                                          # :1035
+        j0 = max(k + 1, start)
+        if j0 >= end:
+            continue
+        blk = amat[:, j0:end]
+        zb = 2.0 * (vec.real[:, None] * blk.real + vec.imag[:, None] * blk.imag).sum(0) \
+            - vec[0].real * blk[0].real                                  # :1056-1085
+        amat[:, j0:end] = blk - np.outer(vec, zb)                         # :1094 (ZGERU)
+
+
+def build_hr(dvg, dng, col_start, col_end, hr, g_e):
+    """wstat_tools.f90:345-468 (build_hr_real): hr(i, j) = <dvg_i|dng_j>_Gamma for
+    i < g_e and j in [col_start, col_end)."""
+    hr[:g_e, col_start:col_end] = glbrak_gamma(dvg[:, :g_e], dng[:, col_start:col_end])
+
+
+def diagox(nbase, nvec, hr):
+    """wstat_tools.f90:208-273 + linear_algebra_kernel.f90:84-200 (DSYEV 'U'):
+    lowest nvec eigenpairs of the upper triangle of hr[:nbase, :nbase]."""
+    a = np.triu(hr[:nbase, :nbase])
+    a = a + np.triu(a, 1).T
+    w, v = np.linalg.eigh(a)
+    return w[:nvec], v[:, :nvec]
+
+
+def davidson_diago_gamma(s, dvg0, nvec, nvecx, tr2_dfpt=1e-16, trev_pdep=1e-3, trev_pdep_rel=1e-1,
+                         n_pdep_maxiter=100, n_dfpt_maxiter=250, apply=None, log=None):
+    """davidson_diago.f90:31-437 on one image from the starting vectors dvg0
+    (the output of do_randomize, davidson_diago.f90:171).  ``apply(dvg, tr2)``
+    defaults to this module's apply_operator.  Returns (ev, conv, dvg[:, :nvec],
+    dav_iter)."""
+    if apply is None:
+        def apply(v, tr2):
+            return apply_operator(s, v, tr2, maxiter=n_dfpt_maxiter)[0]
+    npw = dvg0.shape[0]
+    dvg = np.zeros((npw, nvecx), complex)
+    dng = np.zeros((npw, nvecx), complex)
+    hr = np.zeros((nvecx, nvecx))
+    vr = np.zeros((nvecx, nvecx))
+    ew = np.zeros(nvecx)
+    ev = np.zeros(nvec)
+    conv = np.zeros(nvec, bool)
+    nbase = nvec
+    notcnv = nvec
+    dvg[:, :nvec] = dvg0[:, :nvec]
+    do_mgs(dvg, 0, nvec)                                                   # :175
+    dng[:, :nvec] = apply(dvg[:, :nvec], -1.0)                             # :195-196
+    dvg[:] = dng                                                           # :208
+    do_mgs(dvg, 0, nvec)                                                   # :209
+    tr2 = min(1e-4, 1e8 * tr2_dfpt)                                        # :229
+    dng[:, :nvec] = apply(dvg[:, :nvec], tr2)
+    build_hr(dvg, dng, 0, nvec, hr, nvec)                                  # :236
+    w, v = diagox(nbase, nvec, hr)                                         # :240
+    ew[:nvec] = w
+    vr[:nbase, :nvec] = v
+    ev[:] = ew[:nvec]
+    if log is not None:
+        log.append(dict(dav_iter=-1, ev=ev.copy(), notcnv=notcnv, dfpt_tr2=tr2, diago_dim=nbase))
+    dav_iter = 0
+    for kter in range(1, n_pdep_maxiter + 1):                               # :259
+        dav_iter += 1
+        ishift = np.zeros(nvecx, int)
+        np_ = 0
+        for n in range(nvec):                                              # :273-296
+            if not conv[n]:
+                ishift[nbase + np_] = n
+                ew[nbase + np_] = ev[n]
+                np_ += 1
+        for j in range(nbase, nbase + notcnv):                             # :300, redistribute_vr_distr
+            vr[:, j] = vr[:, ishift[j]]
+        # update_with_vr_distr_real (wstat_tools.f90:945-1092)
+        coef = vr[:nbase, nbase:nbase + notcnv]
+        hg = dvg[:, :nbase] @ coef
+        hg2 = dng[:, :nbase] @ coef
+        dvg[:, nbase:nbase + notcnv] = -ew[nbase:nbase + notcnv][None, :] * hg + hg2
+        do_mgs(dvg, nbase, nbase + notcnv)                                 # :306
+        dng[:, nbase:nbase + notcnv] = apply(dvg[:, nbase:nbase + notcnv], tr2_dfpt)   # :324
+        build_hr(dvg, dng, nbase, nbase + notcnv, hr, nbase + notcnv)     # :331
+        nbase += notcnv
+        w, v = diagox(nbase, nvec, hr)                                     # :340
+        ew[:nvec] = w
+        vr[:, :] = 0.0
+        vr[:nbase, :nvec] = v
+        conv = (np.abs((ew[:nvec] - ev) / ev) < trev_pdep_rel) & (np.abs(ew[:nvec] - ev) < trev_pdep)  # :346
+        notcnv = int((~conv).sum())
+        ev[:] = ew[:nvec]
+        if log is not None:
+            log.append(dict(dav_iter=dav_iter, ev=ev.copy(), notcnv=notcnv, dfpt_tr2=tr2_dfpt, diago_dim=nbase))
+        if notcnv == 0 or nbase + notcnv > nvecx or kter == n_pdep_maxiter:   # :362
+            if notcnv == 0:
+                dvg[:, :nvec] = dvg[:, :nbase] @ vr[:nbase, :nvec]         # refresh_with_vr_distr
+                break
+            if kter == n_pdep_maxiter:
+                break
+            dvg[:, :nvec] = dvg[:, :nbase] @ vr[:nbase, :nvec]             # :397-398
+            dng[:, :nvec] = dng[:, :nbase] @ vr[:nbase, :nvec]
+            nbase = nvec
+            hr[:, :] = 0.0
+            vr[:, :] = 0.0
+            for i in range(nbase):                                         # :404-409
+                hr[i, i] = ev[i]
+                vr[i, i] = 1.0
+    return ev.copy(), conv.copy(), dvg[:, :nvec].copy(), dav_iter

@@ -15,12 +15,11 @@
 #include <string>
 #include <vector>
 
-#include "../../include/west_b200.h"
-#include "wb_internal.h"
+#include "wb_ctx.h"
 
 using namespace wb;
 
-namespace {
+namespace wb {
 
 thread_local std::string g_err;
 
@@ -29,70 +28,7 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-#define WB_CU(call)                                                                            \
-  do {                                                                                         \
-    cudaError_t e_ = (call);                                                                   \
-    if (e_ != cudaSuccess) return fail(WB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-// Grow-only device buffer.
-struct DBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  int ensure(size_t b) {
-    if (b <= bytes) return 0;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    if (cudaMalloc(&p, b) != cudaSuccess) {
-      cudaGetLastError();
-      return -1;
-    }
-    bytes = b;
-    return 0;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  template <class T>
-  T* as() const { return static_cast<T*>(p); }
-};
-
-}  // namespace
-
-struct wb_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int npw = 0, nr = 0, nnr = 0, nocc = 0, nkb = 0, nproj = 0, npv = 0;
-  int maxiter = 0, kinetic_only = 0, precision = WB_PRECISION_FP64, batch_cap = 0;
-  double omega = 0, wk = 0, alpha = 0;
-  StickTab st{};
-  FftArgs fa{};
-  // constant device data
-  DBuf perm, gqz, spg, stpos, tw, g2kin, sqvc, vs, evc, W, D, eprec, et, occ, evcr;
-  // per-call workspace
-  DBuf dvg_in, dng_out, aux, dvbox, B, X, G, T, sticks, sticks2, acc, part, C, rho, conv, act, items, nact,
-      ecol, epcol, unconv, items_pp, items_pk, iota_items;
-  int* nact_host = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  wb_stats stats{};
-  // stage profiling: event pairs recorded on the stream, resolved after the call
-  int prof = 0;
-  std::vector<cudaEvent_t> evpool;
-  size_t evused = 0;
-  struct Mark { int stage, e0, e1; };
-  std::vector<Mark> marks;
-  int ev_get() {
-    if (evused == evpool.size()) {
-      cudaEvent_t e;
-      if (cudaEventCreate(&e) != cudaSuccess) return -1;
-      evpool.push_back(e);
-    }
-    return (int)evused++;
-  }
-};
+}  // namespace wb
 
 namespace {
 
@@ -189,6 +125,15 @@ int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
   c->st.st_pos = c->stpos.as<int>();
   c->st.xhi = xmax;
   c->st.ncols = 2 * xmax + 1;
+  int mmax = 0;
+  for (auto& g : gi) mmax = std::max({mmax, std::abs(g.mx), std::abs(g.my), std::abs(g.mz)});
+  c->st.prune = (4 * mmax < N && N % 4 == 0) ? 1 : 0;
+  if (c->st.prune) {
+    // pruned transforms read every x in the outer quarters, so those columns
+    // are the active set (they are all zero-filled and transformed)
+    c->st.xhi = N / 4 - 1;
+    c->st.ncols = N / 2;
+  }
   return WB_OK;
 }
 
@@ -222,7 +167,7 @@ struct Stage {
     c->stats.stage_launches[st] += launches;
     c->stats.stage_items[st] += items;
     c->stats.launches += launches;
-    if (c->prof) {
+    if (c->prof & (1 << st)) {
       e0 = c->ev_get();
       if (e0 >= 0) cudaEventRecord(c->evpool[e0], c->stream);
     }
@@ -628,7 +573,8 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->D, &c->eprec, &c->et, &c->occ, &c->evcr, &c->dvg_in, &c->dng_out, &c->aux, &c->dvbox, &c->B,
                   &c->X, &c->G, &c->T, &c->sticks, &c->sticks2, &c->acc, &c->part, &c->C, &c->rho, &c->conv,
                   &c->act, &c->items, &c->nact, &c->ecol, &c->epcol, &c->unconv, &c->items_pp, &c->items_pk,
-                  &c->iota_items};
+                  &c->iota_items, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
+                  &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots};
   for (DBuf* b : bufs) b->release();
   if (c->nact_host) cudaFreeHost(c->nact_host);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -663,10 +609,10 @@ int wb_set_batch(wb_ctx* c, int maxp) {
   return WB_OK;
 }
 
-int wb_set_profiling(wb_ctx* c, int level) {
+int wb_set_profiling(wb_ctx* c, int stage_mask) {
   if (!c) return fail(WB_ERR_ARG, "null context");
-  if (level < 0 || level > 1) return fail(WB_ERR_ARG, "profiling level must be 0 or 1");
-  c->prof = level;
+  if (stage_mask < 0 || stage_mask > WB_PROFILE_ALL) return fail(WB_ERR_ARG, "profiling mask out of range");
+  c->prof = stage_mask;
   return WB_OK;
 }
 

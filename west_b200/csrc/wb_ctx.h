@@ -1,0 +1,85 @@
+// Context of the west_b200 library (shared by the translation units that
+// drive it).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/west_b200.h"
+#include "wb_internal.h"
+
+namespace wb {
+
+// Records the message of a failed call (wb_last_error) and returns code.
+int fail(int code, const std::string& msg);
+
+#define WB_CU(call)                                                                            \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return ::wb::fail(WB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Grow-only device buffer.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t b) {
+    if (b <= bytes) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (cudaMalloc(&p, b) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    bytes = b;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace wb
+
+// The opaque handle of the C ABI.
+struct wb_ctx {
+  using DBuf = wb::DBuf;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int npw = 0, nr = 0, nnr = 0, nocc = 0, nkb = 0, nproj = 0, npv = 0;
+  int maxiter = 0, kinetic_only = 0, precision = WB_PRECISION_FP64, batch_cap = 0;
+  double omega = 0, wk = 0, alpha = 0;
+  wb::StickTab st{};
+  wb::FftArgs fa{};
+  // constant device data
+  DBuf perm, gqz, spg, stpos, tw, g2kin, sqvc, vs, evc, W, D, eprec, et, occ, evcr;
+  // per-call workspace
+  DBuf dvg_in, dng_out, aux, dvbox, B, X, G, T, sticks, sticks2, acc, part, C, rho, conv, act, items, nact,
+      ecol, epcol, unconv, items_pp, items_pk, iota_items;
+  int* nact_host = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  wb_stats stats{};
+  // stage profiling: event pairs recorded on the stream, resolved after the call
+  int prof = 0;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+  struct Mark { int stage, e0, e1; };
+  std::vector<Mark> marks;
+  // PDEP Davidson state (wb_davidson)
+  DBuf dav_dvg, dav_dng, dav_tmp, dav_hr, dav_vr, dav_A, dav_V, dav_w, dav_part, dav_coef, dav_dots;
+  int ev_get() {
+    if (evused == evpool.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      evpool.push_back(e);
+    }
+    return (int)evused++;
+  }
+};
+

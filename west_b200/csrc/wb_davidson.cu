@@ -1,0 +1,389 @@
+// PDEP Davidson eigensolver on one GPU (Wstat/davidson_diago.f90:31-437).
+//
+// The host loop follows davidson_diago_gamma step by step (the reference's
+// driver is compiled Fortran; this is its C++ counterpart above the same
+// device kernels).  The basis dvg/dng lives on the device in WEST's |G| order
+// ([column][npw] complex, G = 0 first) and goes through apply_operator by
+// column ranges, like the reference's mstart/mloc slices on one image.
+// Device work: Gamma bra-kets for hr (build_hr_real) on the DMMA split-K
+// GEMM, basis combinations (update_with_vr / refresh_with_vr) on the DMMA
+// accumulation GEMM, modified Gram-Schmidt (do_mgs) as per-vector reductions
+// and rank-1 updates, and a cyclic Jacobi eigensolver (diagox) in one CTA.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "wb_common.cuh"
+#include "wb_ctx.h"
+
+using namespace wb;
+
+namespace {
+
+// hr(col0 + j, rows) <- 2 sum_s part[s][j][r] - W_r(G0) X_j(G0)  (glbrak.f90:39-40)
+__global__ void k_braket_to_hr(const double* __restrict__ part, int nsplit, int M, int ncol,
+                               const double* __restrict__ W, long ldw, const double* __restrict__ X, long ldx,
+                               double* __restrict__ hr, long ldh, int col0) {
+  const int j = blockIdx.x;
+  const double x0 = X[(long)j * ldx];
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double s = 0.0;
+    for (int sp = 0; sp < nsplit; ++sp) s += part[((long)sp * ncol + j) * M + r];
+    hr[(long)(col0 + j) * ldh + r] = 2.0 * s - W[(long)r * ldw] * x0;
+  }
+}
+
+// Coefficients of update_with_vr_distr_real (wstat_tools.f90:1039-1072):
+// C2[j][r] = vr(r, col0 + j), C1[j][r] = -ew(col0 + j) vr(r, col0 + j), r < nrow.
+__global__ void k_vr_coef(const double* __restrict__ vr, long ldv, int nrow, int col0, int ncol,
+                          const double* __restrict__ ew, double* __restrict__ c1, double* __restrict__ c2) {
+  const int j = blockIdx.x;
+  const double e = ew ? -ew[col0 + j] : 0.0;
+  for (int r = threadIdx.x; r < nrow; r += blockDim.x) {
+    const double v = vr[(long)(col0 + j) * ldv + r];
+    c2[(long)j * nrow + r] = v;
+    if (c1) c1[(long)j * nrow + r] = e * v;
+  }
+}
+
+// Gamma self-product and normalisation of one column (do_mgs :1003-1031).
+__global__ void __launch_bounds__(256) k_mgs_normalize(double2* __restrict__ a, int npw) {
+  __shared__ double red[8];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double2 v = a[i];
+    s = fma(v.x, v.x, fma(v.y, v.y, s));
+  }
+  s = block_sum<256>(s, red);
+  const double anorm = 2.0 * s - a[0].x * a[0].x;
+  const double sc = 1.0 / sqrt(anorm);
+  for (int i = threadIdx.x; i < npw; i += 256) a[i] = cscale(a[i], sc);
+}
+
+// zbraket(j) = <vec|a_j>_Gamma for j in [j0, j0 + gridDim.x)  (do_mgs :1056-1085)
+__global__ void __launch_bounds__(256) k_mgs_dots(const double2* __restrict__ a, long ld, int npw, int k, int j0,
+                                                  double* __restrict__ dots) {
+  __shared__ double red[8];
+  const double2* vk = a + (long)k * ld;
+  const double2* vj = a + (long)(j0 + blockIdx.x) * ld;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double2 p = vk[i], q = vj[i];
+    s = fma(p.x, q.x, fma(p.y, q.y, s));
+  }
+  s = block_sum<256>(s, red);
+  if (threadIdx.x == 0) dots[blockIdx.x] = 2.0 * s - vk[0].x * vj[0].x;
+}
+
+// a_j <- a_j - vec zbraket(j)   (ZGERU, do_mgs :1094)
+__global__ void k_mgs_axpy(double2* __restrict__ a, long ld, int npw, int k, int j0, const double* __restrict__ dots) {
+  const int jj = blockIdx.y;
+  const double d = dots[jj];
+  const double2* vk = a + (long)k * ld;
+  double2* vj = a + (long)(j0 + jj) * ld;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
+    const double2 p = vk[i];
+    const double2 q = vj[i];
+    vj[i] = make_double2(fma(-d, p.x, q.x), fma(-d, p.y, q.y));
+  }
+}
+
+// Cyclic two-sided Jacobi on the upper triangle of hr[:n, :n] (what DSYEV 'U'
+// reads in matdiago_dsy, Tools/linear_algebra_kernel.f90:84), round-robin
+// ordering so each round rotates n/2 disjoint (p, q) planes in parallel.
+// One CTA; A and V row-major in global scratch.  Writes the nsel lowest
+// eigenvalues to w and their eigenvectors to vr(:, 0:nsel) (ld ldv).
+__global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ hr, long ldh, int n,
+                                                 double* __restrict__ A, double* __restrict__ V,
+                                                 int nsel, double* __restrict__ w, double* __restrict__ vr,
+                                                 long ldv, int* __restrict__ sweeps_out) {
+  extern __shared__ unsigned char shm[];
+  const int ne = n + (n & 1);
+  const int npairs = ne / 2;
+  double* cs = reinterpret_cast<double*>(shm);           // [npairs] cos
+  double* sn = cs + npairs;                                // [npairs] sin
+  int* pp = reinterpret_cast<int*>(sn + npairs);           // [npairs]
+  int* qq = pp + npairs;                                   // [npairs]
+  int* idx = qq + npairs;                                  // [n]
+  __shared__ double red[2][32];
+  __shared__ int done;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e % n;
+    A[e] = (i <= j) ? hr[(long)j * ldh + i] : hr[(long)i * ldh + j];
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  int sweep = 0;
+  for (; sweep < 60; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e % n;
+      const double v = A[e];
+      if (i == j) dia = fma(v, v, dia); else off = fma(v, v, off);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      dia += __shfl_xor_sync(0xffffffffu, dia, o);
+    }
+    if ((tid & 31) == 0) { red[0][tid >> 5] = off; red[1][tid >> 5] = dia; }
+    __syncthreads();
+    if (tid == 0) {
+      double to = 0.0, td = 0.0;
+      for (int i = 0; i < (nt + 31) / 32; ++i) { to += red[0][i]; td += red[1][i]; }
+      done = (to <= 1e-30 * (td + to)) ? 1 : 0;   // off-diagonal Frobenius norm below 1e-15 of the total
+    }
+    __syncthreads();
+    if (done) break;
+    for (int r = 0; r < ne - 1; ++r) {
+      for (int k = tid; k < npairs; k += nt) {
+        const int a0 = (k == 0) ? 0 : 1 + ((k - 1 + r) % (ne - 1));
+        const int kk = ne - 1 - k;
+        const int b0 = 1 + ((kk - 1 + r) % (ne - 1));
+        const int p = min(a0, b0), q = max(a0, b0);
+        double c = 1.0, s = 0.0;
+        if (q < n) {
+          const double apq = A[p * n + q];
+          if (fabs(apq) > 1e-300) {
+            const double tau = (A[q * n + q] - A[p * n + p]) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+          }
+        }
+        cs[k] = c; sn[k] = s; pp[k] = p; qq[k] = q;
+      }
+      __syncthreads();
+      for (int e = tid; e < npairs * n; e += nt) {      // rows: A <- J^T A
+        const int k = e / n, j = e % n;
+        const int p = pp[k], q = qq[k];
+        if (q >= n || sn[k] == 0.0) continue;
+        const double c = cs[k], s = sn[k];
+        const double ap = A[p * n + j], aq = A[q * n + j];
+        A[p * n + j] = c * ap - s * aq;
+        A[q * n + j] = s * ap + c * aq;
+      }
+      __syncthreads();
+      for (int e = tid; e < npairs * n; e += nt) {      // columns: A <- A J, V <- V J
+        const int k = e / n, i = e % n;
+        const int p = pp[k], q = qq[k];
+        if (q >= n || sn[k] == 0.0) continue;
+        const double c = cs[k], s = sn[k];
+        const double ap = A[i * n + p], aq = A[i * n + q];
+        A[i * n + p] = c * ap - s * aq;
+        A[i * n + q] = s * ap + c * aq;
+        const double vp = V[i * n + p], vq = V[i * n + q];
+        V[i * n + p] = c * vp - s * vq;
+        V[i * n + q] = s * vp + c * vq;
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) {
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    for (int i = 0; i < n; ++i) {                         // selection sort, ascending
+      int best = i;
+      for (int j = i + 1; j < n; ++j)
+        if (A[idx[j] * n + idx[j]] < A[idx[best] * n + idx[best]]) best = j;
+      const int t = idx[i]; idx[i] = idx[best]; idx[best] = t;
+    }
+    *sweeps_out = sweep;
+  }
+  __syncthreads();
+  for (int e = tid; e < nsel * n; e += nt) {
+    const int k = e / n, r = e % n;
+    vr[(long)k * ldv + r] = V[r * n + idx[k]];
+  }
+  for (int k = tid; k < nsel; k += nt) w[k] = A[idx[k] * n + idx[k]];
+}
+
+struct Dav {
+  wb_ctx* c;
+  int npw, nvec, nvecx;
+  long ld;
+  double2 *dvg, *dng, *tmp;
+  double *hr, *vr, *A, *V, *w, *part, *coef, *dots;
+  int* sweeps;
+  int nsplit;
+  cudaStream_t s;
+  int apply_calls = 0;
+  long long applied = 0;
+  std::vector<int> unconv;
+
+  int mgs(int start, int end) {  // do_mgs on columns [start, end)
+    for (int k = 0; k < end; ++k) {
+      if (k >= start) k_mgs_normalize<<<1, 256, 0, s>>>(dvg + (long)k * ld, npw);
+      const int j0 = std::max(k + 1, start);
+      if (j0 >= end) continue;
+      k_mgs_dots<<<end - j0, 256, 0, s>>>(dvg, ld, npw, k, j0, dots);
+      k_mgs_axpy<<<dim3((npw + 255) / 256, end - j0), 256, 0, s>>>(dvg, ld, npw, k, j0, dots);
+    }
+    WB_CU(cudaGetLastError());
+    return WB_OK;
+  }
+  int apply(int col0, int n, double tr2) {
+    unconv.assign(std::max(n, 1), 0);
+    const int rc = wb_apply_operator_device(c, n, reinterpret_cast<const double*>(dvg + (long)col0 * ld), (int)ld,
+                                            reinterpret_cast<double*>(dng + (long)col0 * ld), (int)ld, tr2, 1,
+                                            unconv.data());
+    ++apply_calls;
+    applied += n;
+    return rc;
+  }
+  int build_hr(int col0, int col1, int g_e) {  // hr(0:g_e, col0:col1) = <dvg|dng>
+    const int ncol = col1 - col0, K = 2 * npw;
+    const double* W = reinterpret_cast<const double*>(dvg);
+    const double* X = reinterpret_cast<const double*>(dng + (long)col0 * ld);
+    gemm_tn(W, 2 * ld, g_e, X, 2 * ld, nullptr, ncol, K, nsplit, part, s);
+    k_braket_to_hr<<<ncol, 256, 0, s>>>(part, nsplit, g_e, ncol, W, 2 * ld, X, 2 * ld, hr, nvecx, col0);
+    WB_CU(cudaGetLastError());
+    return WB_OK;
+  }
+  int diagox(int nbase, std::vector<double>& ew_host) {  // lowest nvec eigenpairs of hr[:nbase, :nbase]
+    const int ne = nbase + (nbase & 1);
+    const size_t shm = (size_t)(ne / 2) * (2 * sizeof(double) + 2 * sizeof(int)) + sizeof(int) * nbase + 16;
+    k_jacobi<<<1, 1024, shm, s>>>(hr, nvecx, nbase, A, V, nvec, w, vr, nvecx, sweeps);
+    WB_CU(cudaGetLastError());
+    WB_CU(cudaMemcpyAsync(ew_host.data(), w, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaStreamSynchronize(s));
+    return WB_OK;
+  }
+  // out(:, 0:ncol) = basis(:, 0:nrow) vr(0:nrow, 0:ncol), via tmp
+  int refresh(double2* basis, int nrow, int ncol) {
+    const int K = 2 * npw;
+    k_vr_coef<<<ncol, 256, 0, s>>>(vr, nvecx, nrow, 0, ncol, nullptr, nullptr, coef);
+    gemm_nn(reinterpret_cast<const double*>(basis), 2 * ld, nrow, coef, reinterpret_cast<double*>(tmp), 2 * ld,
+            nullptr, ncol, K, 0.0, s);
+    WB_CU(cudaMemcpyAsync(basis, tmp, sizeof(double2) * ld * ncol, cudaMemcpyDeviceToDevice, s));
+    WB_CU(cudaGetLastError());
+    return WB_OK;
+  }
+};
+
+}  // namespace
+
+extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double* dvg0, int ld_dvg0, double* ev_out,
+                           int* conv_out, double* pdep, int ld_pdep, wb_davidson_info* info) {
+  if (!c || !p || !dvg0 || !ev_out) return fail(WB_ERR_ARG, "null argument");
+  const int nvec = p->n_pdep_eigen, nvecx = p->n_pdep_basis;
+  if (nvec < 1 || nvecx < 2 * nvec)
+    return fail(WB_ERR_ARG, "need n_pdep_eigen >= 1 and n_pdep_basis >= 2 n_pdep_eigen (davidson_diago.f90:107)");
+  if (nvecx > 1024) return fail(WB_ERR_UNSUPPORTED, "n_pdep_basis > 1024 is not provided by the Jacobi eigensolver");
+  if (p->n_pdep_maxiter < 1) return fail(WB_ERR_ARG, "n_pdep_maxiter < 1");
+  if (ld_dvg0 < c->npw || (pdep && ld_pdep < c->npw)) return fail(WB_ERR_ARG, "leading dimension smaller than npw");
+  const auto t0 = std::chrono::steady_clock::now();
+  WB_CU(cudaSetDevice(c->device));
+  Dav d;
+  d.c = c;
+  d.npw = c->npw;
+  d.ld = c->npw;
+  d.nvec = nvec;
+  d.nvecx = nvecx;
+  d.s = c->stream;
+  d.nsplit = gemm_tn_splits(nvecx, nvecx, 2 * c->npw);
+  const size_t colb = sizeof(double2) * d.ld;
+  if (c->dav_dvg.ensure(colb * nvecx) || c->dav_dng.ensure(colb * nvecx) || c->dav_tmp.ensure(colb * nvecx) ||
+      c->dav_hr.ensure(sizeof(double) * nvecx * nvecx) || c->dav_vr.ensure(sizeof(double) * nvecx * nvecx) ||
+      c->dav_A.ensure(sizeof(double) * nvecx * nvecx) || c->dav_V.ensure(sizeof(double) * nvecx * nvecx) ||
+      c->dav_w.ensure(sizeof(double) * nvecx + 64) ||
+      c->dav_part.ensure(sizeof(double) * (size_t)d.nsplit * nvecx * nvecx) ||
+      c->dav_coef.ensure(sizeof(double) * 2 * nvecx * nvecx) || c->dav_dots.ensure(sizeof(double) * (nvecx + 1)))
+    return fail(WB_ERR_NOMEM, "device allocation of the Davidson basis failed");
+  d.dvg = c->dav_dvg.as<double2>();
+  d.dng = c->dav_dng.as<double2>();
+  d.tmp = c->dav_tmp.as<double2>();
+  d.hr = c->dav_hr.as<double>();
+  d.vr = c->dav_vr.as<double>();
+  d.A = c->dav_A.as<double>();
+  d.V = c->dav_V.as<double>();
+  d.w = c->dav_w.as<double>();
+  d.sweeps = reinterpret_cast<int*>(d.w + nvecx);
+  d.part = c->dav_part.as<double>();
+  d.coef = c->dav_coef.as<double>();
+  d.dots = c->dav_dots.as<double>();
+  cudaStream_t s = d.s;
+  WB_CU(cudaMemsetAsync(d.dvg, 0, colb * nvecx, s));
+  WB_CU(cudaMemsetAsync(d.dng, 0, colb * nvecx, s));
+  WB_CU(cudaMemsetAsync(d.hr, 0, sizeof(double) * nvecx * nvecx, s));
+  WB_CU(cudaMemsetAsync(d.vr, 0, sizeof(double) * nvecx * nvecx, s));
+  WB_CU(cudaMemcpy2DAsync(d.dvg, colb, dvg0, sizeof(double2) * ld_dvg0, colb, nvec, cudaMemcpyHostToDevice, s));
+  std::vector<double> ew(nvecx, 0.0), ev(nvec, 0.0), wtmp(nvec);
+  std::vector<int> conv(nvec, 0);
+  int nbase = nvec, notcnv = nvec, rc;
+  // starting steps (davidson_diago.f90:171-247)
+  if ((rc = d.mgs(0, nvec))) return rc;
+  if ((rc = d.apply(0, nvec, -1.0))) return rc;                          // lite solver
+  WB_CU(cudaMemcpyAsync(d.dvg, d.dng, colb * nvecx, cudaMemcpyDeviceToDevice, s));   // dvg = dng
+  if ((rc = d.mgs(0, nvec))) return rc;
+  if ((rc = d.apply(0, nvec, std::min(1e-4, 1e8 * p->tr2_dfpt)))) return rc;
+  if ((rc = d.build_hr(0, nvec, nvec))) return rc;
+  if ((rc = d.diagox(nbase, wtmp))) return rc;
+  for (int i = 0; i < nvec; ++i) ew[i] = ev[i] = wtmp[i];
+  int dav_iter = 0;
+  bool refreshed = false;
+  for (int kter = 1; kter <= p->n_pdep_maxiter; ++kter) {                 // :259
+    ++dav_iter;
+    std::vector<int> ishift(nvecx, 0);
+    int np_ = 0;
+    for (int n = 0; n < nvec; ++n)                                        // :273-296
+      if (!conv[n]) { ishift[nbase + np_] = n; ew[nbase + np_] = ev[n]; ++np_; }
+    for (int j = nbase; j < nbase + notcnv; ++j)                          // redistribute_vr_distr
+      WB_CU(cudaMemcpyAsync(d.vr + (long)j * nvecx, d.vr + (long)ishift[j] * nvecx, sizeof(double) * nvecx,
+                            cudaMemcpyDeviceToDevice, s));
+    WB_CU(cudaMemcpyAsync(d.w, ew.data(), sizeof(double) * nvecx, cudaMemcpyHostToDevice, s));
+    {                                                                      // update_with_vr_distr
+      const int K = 2 * d.npw;
+      double* c1 = d.coef;
+      double* c2 = d.coef + (size_t)nvecx * nvecx;
+      k_vr_coef<<<notcnv, 256, 0, s>>>(d.vr, nvecx, nbase, nbase, notcnv, d.w, c1, c2);
+      double* y = reinterpret_cast<double*>(d.dvg + (long)nbase * d.ld);
+      gemm_nn(reinterpret_cast<const double*>(d.dvg), 2 * d.ld, nbase, c1, y, 2 * d.ld, nullptr, notcnv, K, 0.0, s);
+      gemm_nn(reinterpret_cast<const double*>(d.dng), 2 * d.ld, nbase, c2, y, 2 * d.ld, nullptr, notcnv, K, 1.0, s);
+      WB_CU(cudaGetLastError());
+    }
+    if ((rc = d.mgs(nbase, nbase + notcnv))) return rc;                   // :306
+    if ((rc = d.apply(nbase, notcnv, p->tr2_dfpt))) return rc;             // :324
+    if ((rc = d.build_hr(nbase, nbase + notcnv, nbase + notcnv))) return rc;   // :331
+    nbase += notcnv;
+    if ((rc = d.diagox(nbase, wtmp))) return rc;                          // :340
+    for (int i = 0; i < nvec; ++i) ew[i] = wtmp[i];
+    notcnv = 0;
+    for (int i = 0; i < nvec; ++i) {                                      // :346-347
+      conv[i] = (std::fabs((ew[i] - ev[i]) / ev[i]) < p->trev_pdep_rel) && (std::fabs(ew[i] - ev[i]) < p->trev_pdep);
+      notcnv += conv[i] ? 0 : 1;
+    }
+    for (int i = 0; i < nvec; ++i) ev[i] = ew[i];
+    if (notcnv == 0 || nbase + notcnv > nvecx || kter == p->n_pdep_maxiter) {
+      if (notcnv == 0 || kter == p->n_pdep_maxiter) {
+        if ((rc = d.refresh(d.dvg, nbase, nvec))) return rc;              // eigenvectors for the caller
+        refreshed = true;
+        break;
+      }
+      if ((rc = d.refresh(d.dvg, nbase, nvec))) return rc;                // :397-398
+      if ((rc = d.refresh(d.dng, nbase, nvec))) return rc;
+      nbase = nvec;
+      std::vector<double> eye((size_t)nvecx * nvecx, 0.0), hd((size_t)nvecx * nvecx, 0.0);
+      for (int i = 0; i < nbase; ++i) { hd[(size_t)i * nvecx + i] = ev[i]; eye[(size_t)i * nvecx + i] = 1.0; }
+      WB_CU(cudaMemcpyAsync(d.hr, hd.data(), sizeof(double) * hd.size(), cudaMemcpyHostToDevice, s));
+      WB_CU(cudaMemcpyAsync(d.vr, eye.data(), sizeof(double) * eye.size(), cudaMemcpyHostToDevice, s));
+      WB_CU(cudaStreamSynchronize(s));
+    }
+  }
+  if (!refreshed && (rc = d.refresh(d.dvg, nbase, nvec))) return rc;
+  if (pdep)
+    WB_CU(cudaMemcpy2DAsync(pdep, sizeof(double2) * ld_pdep, d.dvg, colb, colb, nvec, cudaMemcpyDeviceToHost, s));
+  WB_CU(cudaStreamSynchronize(s));
+  std::memcpy(ev_out, ev.data(), sizeof(double) * nvec);
+  if (conv_out) for (int i = 0; i < nvec; ++i) conv_out[i] = conv[i];
+  if (info) {
+    info->dav_iter = dav_iter;
+    info->notcnv = notcnv;
+    info->converged = notcnv == 0 ? 1 : 0;
+    info->apply_calls = d.apply_calls;
+    info->perturbations = d.applied;
+    info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return WB_OK;
+}

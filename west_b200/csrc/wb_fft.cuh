@@ -123,18 +123,37 @@ struct LinePad {
   WB_DEV static int off_blk(int a, int b) { return (N2 + PAD) * a + b; }
 };
 
+// Pruning for lines whose nonzero inputs (inverse) or needed outputs
+// (forward) lie in [0, N/4) u [3N/4, N), as a wavefunction sphere does in a
+// box sized for the density cutoff.  In step 1 element N2*n1 + n2 is live iff
+// n1 is in the outer quarters (needs N1 % 4 == 0); in step 2 output
+// k1 + N1*k2 is live iff k2 is in the outer quarters (needs N2 % 4 == 0).
+// Dead inputs are compile-time zeros and dead outputs are never stored, so the
+// compiler removes their arithmetic.
+enum : int { PRUNE_NONE = 0, PRUNE_IN = 1, PRUNE_OUT = 2 };
+template <int N>
+struct Prune {
+  static constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
+  static constexpr bool IN_OK = (N1 % 4 == 0);
+  static constexpr bool OUT_OK = (N2 % 4 == 0);
+  WB_DEV static constexpr bool in_live(int n1) { return n1 < N1 / 4 || n1 >= N1 - N1 / 4; }
+  WB_DEV static constexpr bool out_live(int k2) { return k2 < N2 / 4 || k2 >= N2 - N2 / 4; }
+};
+
 // Batched line FFTs in shared memory.  Line l starts at data + loff(l).
 // Elements of a line are either padded-contiguous (PADDED, LinePad layout,
 // element stride 1) or strided by es with no padding (columns of a plane,
 // where consecutive threads take consecutive lines).  LINE_FAST puts
-// consecutive threads on consecutive lines.  Must be called by all NT threads
-// of the block (contains barriers).
-template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, class Off>
-WB_DEV void fft_lines(double2* data, Off loff, int es, int nlines, const double2* twN) {
+// consecutive threads on consecutive lines.  The two steps are separate so a
+// kernel can fuse pointwise work between them; fft_lines runs both.  All
+// functions must be called by all NT threads of the block.
+template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off>
+WB_DEV void fft_step1(double2* data, Off loff, int es, int nlines, const double2* twN) {
   using LP = LinePad<N>;
+  using PR = Prune<N>;
+  constexpr bool PIN = (PRUNE == PRUNE_IN) && PR::IN_OK;
   constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
   const int tid = threadIdx.x;
-  // step 1: N1-point DFTs over elements N2*n1 + n2, thread-private
   const int items1 = nlines * N2;
   for (int it = tid; it < items1; it += NT) {
     int line, n2;
@@ -143,15 +162,24 @@ WB_DEV void fft_lines(double2* data, Off loff, int es, int nlines, const double2
     double2* p = data + loff(line);
     double2 v[N1];
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[n1] = p[PADDED ? LP::off_blk(n1, n2) : (N2 * n1 + n2) * es];
+    for (int n1 = 0; n1 < N1; ++n1)
+      v[n1] = (PIN && !PR::in_live(n1)) ? make_double2(0.0, 0.0)
+                                        : p[PADDED ? LP::off_blk(n1, n2) : (N2 * n1 + n2) * es];
     rdft<N1, DIR, N>(v, twN);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) v[k1] = ctw<DIR>(v[k1], twN[(n2 * k1) % N]);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) p[PADDED ? LP::off_blk(k1, n2) : (N2 * k1 + n2) * es] = v[k1];
   }
-  __syncthreads();
-  // step 2: N2-point DFTs, one line's N1 work items inside one chunk
+}
+
+template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off>
+WB_DEV void fft_step2(double2* data, Off loff, int es, int nlines, const double2* twN) {
+  using LP = LinePad<N>;
+  using PR = Prune<N>;
+  constexpr bool POUT = (PRUNE == PRUNE_OUT) && PR::OUT_OK;
+  constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
+  const int tid = threadIdx.x;
   constexpr int LPC = NT / N1;
   const int nchunks = (nlines + LPC - 1) / LPC;
   for (int c = 0; c < nchunks; ++c) {
@@ -169,10 +197,18 @@ WB_DEV void fft_lines(double2* data, Off loff, int es, int nlines, const double2
     __syncthreads();
     if (act) {
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) p[PADDED ? LP::off(k1 + N1 * k2) : (k1 + N1 * k2) * es] = v[k2];
+      for (int k2 = 0; k2 < N2; ++k2)
+        if (!POUT || PR::out_live(k2)) p[PADDED ? LP::off(k1 + N1 * k2) : (k1 + N1 * k2) * es] = v[k2];
     }
   }
   __syncthreads();
+}
+
+template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off>
+WB_DEV void fft_lines(double2* data, Off loff, int es, int nlines, const double2* twN) {
+  fft_step1<N, DIR, NT, LINE_FAST, PADDED, PRUNE>(data, loff, es, nlines, twN);
+  __syncthreads();
+  fft_step2<N, DIR, NT, LINE_FAST, PADDED, PRUNE>(data, loff, es, nlines, twN);
 }
 
 struct OffLinear {

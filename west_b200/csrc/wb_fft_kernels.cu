@@ -36,7 +36,7 @@ WB_DEV void load_tw(double2* tw, const double2* twg) {
 // ---------------------------------------------------------------------------
 // z pass, inverse: sphere coefficients of a pair of columns -> sticks
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, bool PR>
 __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, long ld,
                                               const int2* __restrict__ items, StickTab st,
                                               double2* __restrict__ out,
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, l
     }
   }
   __syncthreads();
-  fft_lines<N, +1, ZNT, false, true>(zb, OffLinear{LS}, 1, 2 * nq, tw);
+  fft_lines<N, +1, ZNT, false, true, PR ? PRUNE_IN : PRUNE_NONE>(zb, OffLinear{LS}, 1, 2 * nq, tw);
   const int ns = 2 * nq;
   double2* o = out + (long)item * N * st.nst + 2 * q0;
   for (int e = threadIdx.x; e < ns * N; e += ZNT) {
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, l
 // ---------------------------------------------------------------------------
 // z pass, forward: sticks -> sphere with the Gamma unpack, then an epilogue
 // ---------------------------------------------------------------------------
-template <int N, class Epi>
+template <int N, bool PR, class Epi>
 __global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks,
                                               const int2* __restrict__ items, StickTab st,
                                               const double2* __restrict__ twg, Epi epi) {
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks
     zb[s * LS + LinePad<N>::off(z)] = s0[(long)z * st.nst + s];
   }
   __syncthreads();
-  fft_lines<N, -1, ZNT, false, true>(zb, OffLinear{LS}, 1, ns, tw);
+  fft_lines<N, -1, ZNT, false, true, PR ? PRUNE_OUT : PRUNE_NONE>(zb, OffLinear{LS}, 1, ns, tw);
   const int2 it = items[item];
   const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
   for (int g = g0 + threadIdx.x; g < g1; g += ZNT) {
@@ -177,9 +177,23 @@ struct EpiDng {
 // ---------------------------------------------------------------------------
 // x-y plane passes
 // ---------------------------------------------------------------------------
-template <int N>
-WB_DEV void plane_zero(double2* pl) {
-  for (int e = threadIdx.x; e < Plane<N>::SIZE; e += PNT) pl[e] = make_double2(0.0, 0.0);
+// Zero what the inverse transforms read: with pruning (PR) only the active
+// columns (which then are all x in [0, N/4) u [3N/4, N)) at live rows (y in
+// the same quarters), otherwise the whole plane.
+template <int N, bool PR>
+WB_DEV void plane_zero(double2* pl, const StickTab& st) {
+  if constexpr (PR && Prune<N>::IN_OK) {
+    constexpr int NL = 2 * (N / 4);
+    const int nc = st.ncols, nlow = st.xhi + 1;
+    for (int e = threadIdx.x; e < NL * nc; e += PNT) {
+      const int l = e % nc, r = e / nc;
+      const int x = l < nlow ? l : N - nc + l;
+      const int y = r < N / 4 ? r : N - NL + r;
+      pl[Plane<N>::at(x, y)] = make_double2(0.0, 0.0);
+    }
+  } else {
+    for (int e = threadIdx.x; e < Plane<N>::SIZE; e += PNT) pl[e] = make_double2(0.0, 0.0);
+  }
 }
 // stick positions are y*N + x in row-major plane order
 template <int N>
@@ -196,17 +210,20 @@ WB_DEV void plane_gather(const double2* pl, double2* __restrict__ sz, const int*
     sz[s] = p >= 0 ? pl[Plane<N>::at_lin(p)] : make_double2(0.0, 0.0);
   }
 }
-template <int N, int DIR>
+// inverse transforms prune inputs, forward transforms prune outputs
+template <int N, int DIR, bool PR>
 WB_DEV void plane_fft_cols(double2* pl, const StickTab& st, const double2* tw) {
-  fft_lines<N, DIR, PNT, true, false>(pl, OffCols<N>{st.xhi + 1, st.ncols}, Plane<N>::RS, st.ncols, tw);
+  constexpr int P = !PR ? PRUNE_NONE : (DIR > 0 ? PRUNE_IN : PRUNE_OUT);
+  fft_lines<N, DIR, PNT, true, false, P>(pl, OffCols<N>{st.xhi + 1, st.ncols}, Plane<N>::RS, st.ncols, tw);
 }
-template <int N, int DIR>
+template <int N, int DIR, bool PR>
 WB_DEV void plane_fft_rows(double2* pl, const double2* tw) {
-  fft_lines<N, DIR, PNT, false, true>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
+  constexpr int P = !PR ? PRUNE_NONE : (DIR > 0 ? PRUNE_IN : PRUNE_OUT);
+  fft_lines<N, DIR, PNT, false, true, P>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
 }
 
 // psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma)
-template <int N>
+template <int N, bool PR>
 __global__ void __launch_bounds__(PNT) k_plane_vloc(double2* __restrict__ sticks, StickTab st,
                                                     const double* __restrict__ vs,
                                                     const double2* __restrict__ twg) {
@@ -216,25 +233,25 @@ __global__ void __launch_bounds__(PNT) k_plane_vloc(double2* __restrict__ sticks
   const int z = blockIdx.x, item = blockIdx.y;
   double2* sz = sticks + ((long)item * N + z) * st.nst;
   load_tw<N>(tw, twg);
-  plane_zero<N>(pl);
+  plane_zero<N, PR>(pl, st);
   __syncthreads();
   plane_scatter<N>(pl, sz, st.st_pos, st.nst);
   __syncthreads();
-  plane_fft_cols<N, +1>(pl, st, tw);
-  plane_fft_rows<N, +1>(pl, tw);
+  plane_fft_cols<N, +1, PR>(pl, st, tw);
+  plane_fft_rows<N, +1, PR>(pl, tw);
   const double* v = vs + (long)z * N * N;
   for (int e = threadIdx.x; e < N * N; e += PNT) {
     const int o = Plane<N>::at_lin(e);
     pl[o] = cscale(pl[o], v[e]);
   }
   __syncthreads();
-  plane_fft_rows<N, -1>(pl, tw);
-  plane_fft_cols<N, -1>(pl, st, tw);
+  plane_fft_rows<N, -1, PR>(pl, tw);
+  plane_fft_cols<N, -1, PR>(pl, st, tw);
   plane_gather<N>(pl, sz, st.st_pos, st.nst);
 }
 
 // sticks -> full real-space box (complex: two real functions), no scaling
-template <int N>
+template <int N, bool PR>
 __global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict__ sticks, StickTab st,
                                                        double2* __restrict__ box,
                                                        const double2* __restrict__ twg) {
@@ -244,19 +261,19 @@ __global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict
   const int z = blockIdx.x, item = blockIdx.y;
   const double2* sz = sticks + ((long)item * N + z) * st.nst;
   load_tw<N>(tw, twg);
-  plane_zero<N>(pl);
+  plane_zero<N, PR>(pl, st);
   __syncthreads();
   plane_scatter<N>(pl, sz, st.st_pos, st.nst);
   __syncthreads();
-  plane_fft_cols<N, +1>(pl, st, tw);
-  plane_fft_rows<N, +1>(pl, tw);
+  plane_fft_cols<N, +1, PR>(pl, st, tw);
+  plane_fft_rows<N, +1, PR>(pl, tw);
   double2* o = box + ((long)item * N + z) * N * N;
   for (int e = threadIdx.x; e < N * N; e += PNT) o[e] = pl[Plane<N>::at_lin(e)];
 }
 
 // RHS of the Sternheimer equation, dfpt_module.f90:245-260:
 // (psi_v1(r) + i psi_v2(r)) * dv_p(r) / N^3 -> forward -> sticks
-template <int N>
+template <int N, bool PR>
 __global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ evcr,
                                                    const double2* __restrict__ dvbox, int npv,
                                                    StickTab st, double2* __restrict__ sticks,
@@ -276,8 +293,8 @@ __global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ e
     pl[Plane<N>::at_lin(e)] = cscale(ps[e], w);
   }
   __syncthreads();
-  plane_fft_rows<N, -1>(pl, tw);
-  plane_fft_cols<N, -1>(pl, st, tw);
+  plane_fft_rows<N, -1, PR>(pl, tw);
+  plane_fft_cols<N, -1, PR>(pl, st, tw);
   const long item = (long)p * npv + k;
   plane_gather<N>(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
 }
@@ -287,7 +304,7 @@ __global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ e
 // then (drho_p1 + i drho_p2) * scale -> forward -> sticks.
 // acc is per-CTA scratch in global memory ([pp][z][N*N] double2), owned
 // element-wise by the thread that writes it.
-template <int N>
+template <int N, bool PR>
 __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ dsticks,
                                                     const double2* __restrict__ evcr,
                                                     const double* __restrict__ occ, int nocc,
@@ -310,12 +327,12 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
     for (int k = 0; k < npv; ++k) {
       const long item = (long)p * npv + k;
       __syncthreads();
-      plane_zero<N>(pl);
+      plane_zero<N, PR>(pl, st);
       __syncthreads();
       plane_scatter<N>(pl, dsticks + (item * N + z) * st.nst, st.st_pos, st.nst);
       __syncthreads();
-      plane_fft_cols<N, +1>(pl, st, tw);
-      plane_fft_rows<N, +1>(pl, tw);
+      plane_fft_cols<N, +1, PR>(pl, st, tw);
+      plane_fft_rows<N, +1, PR>(pl, tw);
       const double o1 = occ[2 * k];
       const double o2 = (2 * k + 1 < nocc) ? occ[2 * k + 1] : 0.0;
       const double2* ps = evcr + ((long)k * N + z) * N * N;
@@ -333,9 +350,88 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
   __syncthreads();
   for (int e = threadIdx.x; e < N * N; e += PNT) pl[Plane<N>::at_lin(e)] = cscale(ac[e], scale);
   __syncthreads();
-  plane_fft_rows<N, -1>(pl, tw);
-  plane_fft_cols<N, -1>(pl, st, tw);
+  plane_fft_rows<N, -1, PR>(pl, tw);
+  plane_fft_cols<N, -1, PR>(pl, st, tw);
   plane_gather<N>(pl, osticks + ((long)pp * N + z) * st.nst, st.st_pos, st.nst);
+}
+
+// Local potential for N1 == N2 boxes (64^3): the inverse-row second step, the
+// V(r)/N^3 product and the forward-row first step run in registers of one
+// thread (the outputs X[k1 + R k2] of the inverse are exactly the inputs
+// x[R n1 + k1] of the forward step for n1 = k2), saving a shared-memory round
+// trip of the whole plane.  The plane's sticks and V values are loaded into
+// registers before the zero fill so their latency overlaps it.
+constexpr int kFusedMaxSticksPerThread = 4;
+
+template <int N>
+__global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(double2* __restrict__ sticks, StickTab st,
+                                                          const double* __restrict__ vs,
+                                                          const double2* __restrict__ twg) {
+  constexpr int R = FftSplit<N>::N1;
+  static_assert(FftSplit<N>::N1 == FftSplit<N>::N2, "fused rows need N1 == N2");
+  constexpr int LPC = PNT / R;
+  constexpr int NCH = (N + LPC - 1) / LPC;
+  constexpr int MS = kFusedMaxSticksPerThread;
+  using LP = LinePad<N>;
+  extern __shared__ double2 sm[];
+  double2* tw = sm;
+  double2* pl = sm + N;
+  const int z = blockIdx.x, item = blockIdx.y, tid = threadIdx.x;
+  double2* sz = sticks + ((long)item * N + z) * st.nst;
+  double2 sv[MS];
+  int sp[MS];
+#pragma unroll
+  for (int i = 0; i < MS; ++i) {
+    const int s = tid + i * PNT;
+    sp[i] = -1;
+    if (s < st.nst) { sp[i] = st.st_pos[s]; sv[i] = sz[s]; }
+  }
+  const int k1 = tid % R;
+  const bool rowthr = tid < LPC * R;
+  double vr[NCH][R];
+  const double* vz = vs + (long)z * N * N;
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) {
+    const int y = c * LPC + tid / R;
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) vr[c][k2] = (rowthr && y < N) ? vz[y * N + k1 + R * k2] : 0.0;
+  }
+  load_tw<N>(tw, twg);
+  plane_zero<N, true>(pl, st);
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < MS; ++i)
+    if (sp[i] >= 0) pl[Plane<N>::at_lin(sp[i])] = sv[i];
+  __syncthreads();
+  plane_fft_cols<N, +1, true>(pl, st, tw);
+  fft_step1<N, +1, PNT, false, true, PRUNE_IN>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) {
+    const int y = c * LPC + tid / R;
+    const bool act = rowthr && y < N;
+    double2* p = pl + (act ? y : 0) * Plane<N>::RS;
+    double2 v[R];
+    if (act) {
+#pragma unroll
+      for (int n2 = 0; n2 < R; ++n2) v[n2] = p[LP::off_blk(k1, n2)];
+      rdft<R, +1, N>(v, tw);                        // X[k1 + R k2], k2 = 0..R-1
+#pragma unroll
+      for (int k2 = 0; k2 < R; ++k2) v[k2] = cscale(v[k2], vr[c][k2]);
+      rdft<R, -1, N>(v, tw);                        // forward step 1 over n1 = k2, thread n2 = k1
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = ctw<-1>(v[q], tw[(k1 * q) % N]);
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) p[LP::off_blk(q, k1)] = v[q];
+    }
+  }
+  __syncthreads();
+  fft_step2<N, -1, PNT, false, true, PRUNE_OUT>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
+  plane_fft_cols<N, -1, true>(pl, st, tw);
+  plane_gather<N>(pl, sz, st.st_pos, st.nst);
 }
 
 // ---------------------------------------------------------------------------
@@ -348,43 +444,76 @@ static size_t psmem() { return sizeof(double2) * (N + Plane<N>::SIZE); }
 
 template <int N>
 struct FftN {
+  static constexpr bool FUSABLE = FftSplit<N>::N1 == FftSplit<N>::N2 && Prune<N>::IN_OK && Prune<N>::OUT_OK;
+  template <bool PR>
+  static void setup_pr() {
+    cudaFuncSetAttribute(k_zinv<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, PR, EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, PR, EpiHpsi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, PR, EpiDng>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_plane_vloc<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    cudaFuncSetAttribute(k_plane_inv_box<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    cudaFuncSetAttribute(k_plane_rhs<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    cudaFuncSetAttribute(k_plane_drho<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+  }
   static void setup() {
-    cudaFuncSetAttribute(k_zinv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_zfwd<N, EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_zfwd<N, EpiHpsi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_zfwd<N, EpiDng>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_plane_vloc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
-    cudaFuncSetAttribute(k_plane_inv_box<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
-    cudaFuncSetAttribute(k_plane_rhs<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
-    cudaFuncSetAttribute(k_plane_drho<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    setup_pr<false>();
+    setup_pr<true>();
+    if constexpr (FUSABLE)
+      cudaFuncSetAttribute(k_plane_vloc_fused<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
   }
   static dim3 zgrid(const StickTab& st, int nitems) { return dim3((st.nsp + ZSG - 1) / ZSG, nitems); }
   static void zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks) {
     if (nitems <= 0) return;
-    k_zinv<N><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+    if (f.st.prune)
+      k_zinv<N, true><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+    else
+      k_zinv<N, false><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
   }
   template <class Epi>
   static void zfwd(const FftArgs& f, const double2* sticks, const int2* items, int nitems, Epi epi) {
     if (nitems <= 0) return;
-    k_zfwd<N, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
+    if (f.st.prune)
+      k_zfwd<N, true, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
+    else
+      k_zfwd<N, false, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
   }
   static void vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs) {
     if (nitems <= 0) return;
-    k_plane_vloc<N><<<dim3(N, nitems), PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+    const dim3 g(N, nitems);
+    if constexpr (FUSABLE) {
+      if (f.st.prune && f.st.nst <= kFusedMaxSticksPerThread * PNT) {
+        k_plane_vloc_fused<N><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+        return;
+      }
+    }
+    if (f.st.prune) k_plane_vloc<N, true><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+    else k_plane_vloc<N, false><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
   }
   static void inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box) {
     if (nitems <= 0) return;
-    k_plane_inv_box<N><<<dim3(N, nitems), PNT, psmem<N>(), f.stream>>>(sticks, f.st, box, f.tw);
+    const dim3 g(N, nitems);
+    if (f.st.prune) k_plane_inv_box<N, true><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, box, f.tw);
+    else k_plane_inv_box<N, false><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, box, f.tw);
   }
   static void rhs(const FftArgs& f, const double2* evcr, const double2* dvbox, int npv, int mb, double2* sticks) {
     if (mb <= 0) return;
-    k_plane_rhs<N><<<dim3(N, npv, mb), PNT, psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
+    const dim3 g(N, npv, mb);
+    if (f.st.prune)
+      k_plane_rhs<N, true><<<g, PNT, psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
+    else
+      k_plane_rhs<N, false><<<g, PNT, psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
   }
   static void drho(const FftArgs& f, const double2* dsticks, const double2* evcr, const double* occ, int nocc,
                    int mb, double2* acc, double scale, double2* osticks) {
     if (mb <= 0) return;
-    k_plane_drho<N><<<dim3(N, (mb + 1) / 2), PNT, psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st,
-                                                                         acc, scale, osticks, f.tw);
+    const dim3 g(N, (mb + 1) / 2);
+    if (f.st.prune)
+      k_plane_drho<N, true><<<g, PNT, psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st, acc, scale,
+                                                              osticks, f.tw);
+    else
+      k_plane_drho<N, false><<<g, PNT, psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st, acc, scale,
+                                                               osticks, f.tw);
   }
 };
 

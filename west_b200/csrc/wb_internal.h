@@ -13,6 +13,7 @@ struct StickTab {
   const int* st_pos;     // [nst] plane offset y*N + x of each stick, -1 = dummy
   int xhi;               // active plane columns: x in [0, xhi] and [N - (ncols - xhi - 1), N)
   int ncols;
+  int prune;             // 1 if every |Miller index| < N/4 (sphere inside the outer quarters)
 };
 
 struct FftArgs {

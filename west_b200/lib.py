@@ -24,7 +24,8 @@ WB_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 EXPORTS = (
     "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
     "wb_apply_operator_device_noalloc",
-    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling", "wb_last_error", "wb_version",
+    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling", "wb_davidson", "wb_last_error",
+    "wb_version",
 )
 NSTAGES = 10
 STAGES = ("vloc_zinv", "vloc_plane", "vloc_zfwd", "gemm_tn", "gemm_reduce", "gemm_nn", "cg", "rhs", "drho",
@@ -52,6 +53,16 @@ class WbStats(ctypes.Structure):
                 ("stage_items", ctypes.c_longlong * 10)]
 
 
+class WbDavidsonParams(ctypes.Structure):
+    _fields_ = [("n_pdep_eigen", _i), ("n_pdep_basis", _i), ("n_pdep_maxiter", _i),
+                ("tr2_dfpt", _d), ("trev_pdep", _d), ("trev_pdep_rel", _d)]
+
+
+class WbDavidsonInfo(ctypes.Structure):
+    _fields_ = [("dav_iter", _i), ("notcnv", _i), ("converged", _i), ("apply_calls", _i),
+                ("perturbations", ctypes.c_longlong), ("seconds", _d)]
+
+
 class WestB200Error(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"west_b200 error {code}: {msg}")
@@ -77,6 +88,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.wb_set_batch.argtypes = [_p, _i]
     lib.wb_set_profiling.argtypes = [_p, _i]
     lib.wb_get_stats.argtypes = [_p, ctypes.POINTER(WbStats)]
+    lib.wb_davidson.argtypes = [_p, ctypes.POINTER(WbDavidsonParams), _p, _i, _p, _p, _p, _i,
+                                ctypes.POINTER(WbDavidsonInfo)]
     lib.wb_last_error.restype = ctypes.c_char_p
     lib.wb_last_error.argtypes = []
     lib.wb_version.argtypes = []

@@ -87,8 +87,16 @@ class ResponseOperator:
     def set_batch(self, max_perturbations: int):
         _lib.check(self._lib.wb_set_batch(self._ctx, int(max_perturbations)))
 
-    def set_profiling(self, level: int):
-        _lib.check(self._lib.wb_set_profiling(self._ctx, int(level)))
+    def set_profiling(self, stages="all"):
+        """Time the named pipeline stages (west_b200.lib.STAGES) with CUDA events;
+        "all", or None / [] to switch off."""
+        if stages == "all":
+            mask = (1 << _lib.NSTAGES) - 1
+        else:
+            mask = 0
+            for name in stages or ():
+                mask |= 1 << _lib.STAGES.index(name)
+        _lib.check(self._lib.wb_set_profiling(self._ctx, mask))
 
     def stats(self) -> dict:
         st = _lib.WbStats()
@@ -120,6 +128,26 @@ class ResponseOperator:
                 sys.stdout.write(f"       ** WARNING : PERT {ipert + 1:8d} iks {1:8d} not converged, "
                                  f"ierr = {ierr[ipert]:8d}\n")
         return ierr
+
+
+    def davidson(self, dvg0, n_pdep_eigen, n_pdep_times=4, n_pdep_maxiter=100, tr2_dfpt=1e-16,
+                 trev_pdep=1e-3, trev_pdep_rel=1e-1):
+        """PDEP Davidson (davidson_diago_gamma, Wstat/davidson_diago.f90:31) from the
+        starting basis dvg0 [npwqx, >= n_pdep_eigen] (do_randomize's output).
+        Returns (ev, conv, pdep eigenvectors [npwqx, n_pdep_eigen], info dict)."""
+        nvec = int(n_pdep_eigen)
+        prm = _lib.WbDavidsonParams(nvec, nvec * int(n_pdep_times), int(n_pdep_maxiter), float(tr2_dfpt),
+                                    float(trev_pdep), float(trev_pdep_rel))
+        d0 = np.asfortranarray(dvg0[:, :nvec], dtype=np.complex128)
+        ev = np.zeros(nvec)
+        conv = np.zeros(nvec, dtype=np.int32)
+        vec = np.zeros((d0.shape[0], nvec), dtype=np.complex128, order="F")
+        info = _lib.WbDavidsonInfo()
+        _lib.check(self._lib.wb_davidson(self._ctx, ctypes.byref(prm), _ptr(d0), d0.shape[0], _ptr(ev), _ptr(conv),
+                                         _ptr(vec), vec.shape[0], ctypes.byref(info)))
+        if self.verbose and not info.converged:
+            sys.stdout.write(f"     WARNING : {info.notcnv:5d} eigenvalues not converged in chidiago\n")
+        return ev, conv.astype(bool), vec, {k: getattr(info, k) for k, _ in info._fields_}
 
 
 def _is_torch_cuda(x) -> bool:
