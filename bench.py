@@ -46,6 +46,7 @@ def _args():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--cpu-sample", type=int, default=1, help="perturbations in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-pdep", action="store_true", help="skip the time-to-PDEP Davidson run")
     return ap.parse_args()
 
 
@@ -310,7 +311,25 @@ def run_b200(args, rank, world, local_rank):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if not args.no_pdep:
+            line["time_to_pdep"] = _time_to_pdep(local_rank)
     return line
+
+
+def _time_to_pdep(device):
+    """Wstat time-to-PDEP on the L = 15 bohr, 20 Ry, 48^3 system: n_pdep_eigen 16,
+    n_pdep_times 4, PCG threshold 1e-10, Davidson tolerance 1e-6, FP64."""
+    from west_b200.system import build_system, randomized_basis
+    from west_b200.wstat import ResponseOperator
+    s = build_system("c1", device="cuda")
+    op = ResponseOperator(s, device=device, verbose=False)
+    dvg0 = randomized_basis(s, 16)
+    ev, conv, _, info = op.davidson(dvg0, 16, n_pdep_times=4, n_pdep_maxiter=100, tr2_dfpt=1e-10,
+                                    trev_pdep=1e-6, trev_pdep_rel=1e-1)
+    return {"workload": "Davidson c1: L=15 bohr, 20 Ry, 48^3, 4 atoms (s), nbnd_occ=8, n_pdep_eigen=16, "
+                        "n_pdep_times=4, tr2_dfpt=1e-10, trev_pdep=1e-6, FP64",
+            "seconds": info["seconds"], "dav_iter": info["dav_iter"], "converged": bool(info["converged"]),
+            "perturbations_applied": info["perturbations"], "ev_lowest": float(ev[0]), "ev_highest": float(ev[-1])}
 
 
 def main():
