@@ -83,6 +83,7 @@ typedef struct wb_stats {
   double stage_ms[WB_NSTAGES];          /* per-stage device time (profiling on) */
   long long stage_launches[WB_NSTAGES]; /* per-stage kernel launches            */
   long long stage_items[WB_NSTAGES];    /* per-stage work items (FFT boxes, columns) */
+  int refinements;         /* FP64 refinement steps (mixed form), 0 in FP64 */
 } wb_stats;
 
 /*
@@ -114,7 +115,13 @@ int wb_apply_operator(wb_ctx* ctx, int m, const double* dvg, int ld_dvg, double*
 int wb_apply_operator_device(wb_ctx* ctx, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng,
                              double tr2, int iq, int* unconverged);
 
-/* WB_PRECISION_FP64 (default) or WB_PRECISION_MIXED. */
+/*
+ * WB_PRECISION_FP64 (default): every step in FP64, the reference's arithmetic.
+ * WB_PRECISION_MIXED: the Sternheimer PCG runs in FP32 (FFTs, projector GEMMs,
+ * vector updates) as correction solves inside an FP64 iterative refinement:
+ * the residual b - A x and its preconditioned norm <r|M^-1 r> are formed in
+ * FP64 and each system stops on the same tr2 test as the FP64 form.
+ */
 int wb_set_precision(wb_ctx* ctx, int mode);
 
 /* Upper bound on perturbations processed per device batch (0 = automatic). */

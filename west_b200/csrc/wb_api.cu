@@ -197,7 +197,8 @@ void pair_items(std::vector<int2>& it, int base, int n) {
 size_t per_pert_bytes(const wb_ctx* c) {
   const size_t vec = sizeof(double2) * (size_t)c->npw * c->nocc;
   const size_t stk = sizeof(double2) * (size_t)c->nr * c->st.nst;
-  return 4 * vec                                   // B, X, G, T
+  const size_t mixed = c->precision == WB_PRECISION_MIXED ? 2 * vec + stk * (size_t)c->npv / 2 : 0;
+  return mixed + 4 * vec                           // B, X, G, T (+ FP32 g, P, T, d and sticks)
          + stk * (size_t)c->npv                    // sticks (RHS / CG pairs / drho items)
          + sizeof(double2) * (size_t)c->nnr * 1    // dvbox + acc (one box per two perturbations each)
          + stk                                     // sticks2 (half per perturbation, rounded up)
@@ -295,6 +296,159 @@ void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const i
   (void)nsys;
 }
 
+// ---------------------------------------------------------------------------
+// mixed form: FP32 correction solves inside FP64 iterative refinement
+// ---------------------------------------------------------------------------
+constexpr double kInnerRhoReduction = 1e-9;  // inner PCG stops at rho < 1e-9 rho(outer residual)
+constexpr int kMaxRefinements = 12;
+
+int ensure_fp32(wb_ctx* c, int nsys, int nitems) {
+  const int K = 2 * c->npw;
+  if (!c->have32) {
+    if (c->W32.ensure(sizeof(float) * (size_t)K * c->nproj + 16) || c->D32.ensure(sizeof(float) * std::max(1, c->nkb * c->nkb)) ||
+        c->g2kin32.ensure(sizeof(float) * c->npw) || c->vs32.ensure(sizeof(float) * (size_t)c->nnr) ||
+        c->tw32.ensure(sizeof(float2) * c->nr))
+      return fail(WB_ERR_NOMEM, "device allocation of FP32 constants failed");
+    to_float(c->W.as<double>(), c->W32.as<float>(), (long)K * c->nproj, c->stream);
+    if (c->nkb) to_float(c->D.as<double>(), c->D32.as<float>(), (long)c->nkb * c->nkb, c->stream);
+    to_float(c->g2kin.as<double>(), c->g2kin32.as<float>(), c->npw, c->stream);
+    to_float(c->vs.as<double>(), c->vs32.as<float>(), c->nnr, c->stream);
+    to_float(c->tw.as<double>(), c->tw32.as<float>(), 2L * c->nr, c->stream);
+    c->fa32.n = c->nr;
+    c->fa32.st = c->st;
+    c->fa32.tw = c->tw32.as<float2>();
+    c->fa32.stream = c->stream;
+    c->have32 = 1;
+  }
+  const size_t vec = sizeof(float2) * (size_t)c->npw * nsys;
+  const int nsplit = gemm_tn_splits32(c->nproj, nsys, K);
+  bool bad = false;
+  bad |= c->g32.ensure(vec) || c->P32.ensure(vec) || c->T32.ensure(vec) || c->d32.ensure(vec);
+  bad |= c->sticks32.ensure(sizeof(float2) * (size_t)c->nr * c->st.nst * nitems) != 0;
+  bad |= c->part32.ensure(sizeof(float) * (size_t)nsplit * nsys * c->nproj) != 0;
+  bad |= c->C32.ensure(sizeof(float) * (size_t)nsys * c->nproj) != 0;
+  bad |= c->ecol32.ensure(sizeof(float) * nsys) || c->rho0.ensure(sizeof(double) * nsys) ||
+         c->rho_in.ensure(sizeof(double) * nsys) || c->conv_in.ensure(nsys + 16) ||
+         c->act_in.ensure(sizeof(int) * nsys) || c->items_in.ensure(sizeof(int2) * (nsys / 2 + 1)) ||
+         c->nact_in.ensure(sizeof(int) * 4);
+  if (bad) return fail(WB_ERR_NOMEM, "device workspace allocation failed for the mixed form");
+  return WB_OK;
+}
+
+// FP32 T = (H - e + alpha Pv) P on the listed columns.
+void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const int2* items, int n, int nsplit) {
+  const long ld = c->npw;
+  const int K = 2 * c->npw;
+  cudaStream_t s = c->stream;
+  const float* W = c->W32.as<float>();
+  int M = c->nproj, nkb = c->nkb;
+  if (c->kinetic_only) {
+    Stage g(c, WB_STAGE_VLOC_ZFWD, 1, n);
+    kinetic_hpsi32(Pv, Tv, c->g2kin32.as<float>(), c->ecol32.as<float>(), cols, n, c->npw, ld, s);
+    W += (size_t)c->nkb * K;
+    M = c->nocc;
+    nkb = 0;
+  } else {
+    const int nit = (n + 1) / 2;
+    {
+      Stage g(c, WB_STAGE_VLOC_ZINV, 1, nit);
+      fft_zinv32(c->fa32, Pv, ld, items, nit, c->sticks32.as<float2>());
+    }
+    {
+      Stage g(c, WB_STAGE_VLOC_PLANE, 1, nit);
+      fft_plane_vloc32(c->fa32, c->sticks32.as<float2>(), nit, c->vs32.as<float>());
+    }
+    {
+      Stage g(c, WB_STAGE_VLOC_ZFWD, 1, nit);
+      fft_zfwd_hpsi32(c->fa32, c->sticks32.as<float2>(), items, nit, Pv, Tv, ld, c->g2kin32.as<float>(),
+                      c->ecol32.as<float>());
+    }
+    c->stats.fft_boxes += 2 * nit;
+  }
+  {
+    Stage g(c, WB_STAGE_GEMM_TN, 1, n);
+    gemm_tn32(W, K, M, (const float*)Pv, 2 * ld, cols, n, K, nsplit, c->part32.as<float>(), s);
+  }
+  {
+    Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
+    gamma_reduce32(c->part32.as<float>(), nsplit, M, n, W, K, (const float*)Pv, 2 * ld, cols, c->D32.as<float>(), nkb,
+                   (float)c->alpha, c->C32.as<float>(), s);
+  }
+  {
+    Stage g(c, WB_STAGE_GEMM_NN, 1, n);
+    gemm_nn32_acc(W, K, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, s);
+  }
+}
+
+// Solves (H - e_v + alpha Pv) x_v = b_v for all systems of the batch: FP64
+// residuals and tests, FP32 masked PCG corrections.  X holds the initial
+// guess on entry (dfpt_module.f90:348) and the solution on exit.
+int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
+  cudaStream_t s = c->stream;
+  const int npw = c->npw, nocc = c->nocc, nsys = mb * nocc;
+  const long ld = npw;
+  int rc = ensure_fp32(c, nsys, std::max((nsys + 1) / 2, 1));
+  if (rc) return rc;
+  const int nsplit32 = gemm_tn_splits32(c->nproj, nsys, 2 * npw);
+  double2 *B = c->B.as<double2>(), *X = c->X.as<double2>(), *T = c->T.as<double2>();
+  unsigned char* conv = c->conv.as<unsigned char>();
+  int* act = c->act.as<int>();
+  int2* items = c->items.as<int2>();
+  unsigned char* cin = c->conv_in.as<unsigned char>();
+  int* ain = c->act_in.as<int>();
+  int2* iin = c->items_in.as<int2>();
+  to_float(c->ecol.as<double>(), c->ecol32.as<float>(), nsys, s);
+  cg_reset(conv, nsys, s);
+  cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+  int nact = nsys, inner_total = 0;
+  for (int outer = 0; outer < kMaxRefinements; ++outer) {
+    apply_A(c, X, T, act, items, nact, nsys, nsplit);                    // FP64 A x
+    {
+      Stage g(c, WB_STAGE_CG, 2, nact);
+      refine_residual(act, nact, B, T, c->g2kin.as<double>(), c->epcol.as<double>(), tr2, conv,
+                      c->rho0.as<double>(), c->g32.as<float2>(), c->d32.as<float2>(), npw, ld, s);
+      cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
+    }
+    WB_CU(cudaStreamSynchronize(s));
+    nact = *c->nact_host;
+    if (nact == 0 || outer == kMaxRefinements - 1) break;
+    c->stats.refinements += 1;
+    WB_CU(cudaMemcpyAsync(cin, conv, nsys, cudaMemcpyDeviceToDevice, s));
+    cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
+    int nin = nact;
+    for (int it = 1; it <= c->maxiter; ++it) {
+      {
+        Stage g(c, WB_STAGE_CG, 2, nin);
+        cg_prec_rho32(ain, nin, c->g32.as<float2>(), c->P32.as<float2>(), c->g2kin.as<double>(),
+                      c->epcol.as<double>(), c->rho_in.as<double>(), cin, it, kInnerRhoReduction,
+                      c->rho0.as<double>(), npw, ld, s);
+        cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
+      }
+      WB_CU(cudaStreamSynchronize(s));
+      nin = *c->nact_host;
+      if (nin == 0) break;
+      ++inner_total;
+      c->stats.cg_active_sum += nin;
+      apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), ain, iin, nin, nsplit32);
+      {
+        Stage g(c, WB_STAGE_CG, 1, nin);
+        cg_update32(ain, nin, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(), c->T32.as<float2>(), npw,
+                    ld, s);
+      }
+    }
+    {
+      Stage g(c, WB_STAGE_CG, 1, nact);
+      refine_accumulate(act, nact, X, c->d32.as<float2>(), npw, ld, s);  // x += d (FP64)
+    }
+  }
+  {
+    Stage g(c, WB_STAGE_CG, 1, mb);
+    count_unconverged(conv, nocc, mb, c->unconv.as<int>(), s);
+  }
+  *iters_out = inner_total;
+  return WB_OK;
+}
+
 int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, long ld_out, double tr2,
               int* unconv_host) {
   cudaStream_t s = c->stream;
@@ -346,7 +500,10 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
   }
   // 6. PCG                                           (dfpt_module.f90:350-361)
   int iters = 0;
-  if (tr2 >= 0.0) {
+  if (tr2 >= 0.0 && c->precision == WB_PRECISION_MIXED) {
+    int rc = cg_mixed(c, mb, tr2, nsplit, &iters);
+    if (rc) return rc;
+  } else if (tr2 >= 0.0) {
     unsigned char* conv = c->conv.as<unsigned char>();
     int* act = c->act.as<int>();
     int2* items = c->items.as<int2>();
@@ -411,7 +568,6 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
   if (m > 0 && (!dvg || !dng)) return fail(WB_ERR_ARG, "null dvg or dng");
   if (ld_dvg < c->npw || ld_dng < c->npw) return fail(WB_ERR_ARG, "leading dimension smaller than npw");
   if (std::isnan(tr2)) return fail(WB_ERR_ARG, "tr2 is NaN");
-  if (c->precision != WB_PRECISION_FP64) return fail(WB_ERR_UNSUPPORTED, "mixed precision is not built yet");
   WB_CU(cudaSetDevice(c->device));
   c->stats = wb_stats{};
   c->marks.clear();
@@ -574,7 +730,9 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->X, &c->G, &c->T, &c->sticks, &c->sticks2, &c->acc, &c->part, &c->C, &c->rho, &c->conv,
                   &c->act, &c->items, &c->nact, &c->ecol, &c->epcol, &c->unconv, &c->items_pp, &c->items_pk,
                   &c->iota_items, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
-                  &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots};
+                  &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots, &c->W32, &c->D32, &c->g2kin32,
+                  &c->vs32, &c->tw32, &c->g32, &c->P32, &c->T32, &c->d32, &c->sticks32, &c->part32, &c->C32,
+                  &c->ecol32, &c->rho0, &c->rho_in, &c->conv_in, &c->act_in, &c->items_in, &c->nact_in};
   for (DBuf* b : bufs) b->release();
   if (c->nact_host) cudaFreeHost(c->nact_host);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -597,8 +755,7 @@ int wb_apply_operator_device(wb_ctx* c, int m, const double* dvg, int ld_dvg, do
 
 int wb_set_precision(wb_ctx* c, int mode) {
   if (!c) return fail(WB_ERR_ARG, "null context");
-  if (mode == WB_PRECISION_FP64) { c->precision = mode; return WB_OK; }
-  if (mode == WB_PRECISION_MIXED) return fail(WB_ERR_UNSUPPORTED, "mixed precision is not built yet");
+  if (mode == WB_PRECISION_FP64 || mode == WB_PRECISION_MIXED) { c->precision = mode; return WB_OK; }
   return fail(WB_ERR_ARG, "unknown precision mode");
 }
 

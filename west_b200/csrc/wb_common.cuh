@@ -11,23 +11,33 @@
 
 namespace wb {
 
-WB_DEV double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-WB_DEV double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-WB_DEV double2 cmul(double2 a, double2 b) {
-  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+// Complex helpers for double2 (FP64) and float2 (FP32 inner solves).
+template <class C> struct RealOf;
+template <> struct RealOf<double2> { using type = double; };
+template <> struct RealOf<float2> { using type = float; };
+template <class C> using real_t = typename RealOf<C>::type;
+
+template <class C> WB_DEV C mkc(real_t<C> x, real_t<C> y);
+template <> WB_DEV double2 mkc<double2>(double x, double y) { return make_double2(x, y); }
+template <> WB_DEV float2 mkc<float2>(float x, float y) { return make_float2(x, y); }
+
+template <class C> WB_DEV C cadd(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
+template <class C> WB_DEV C csub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
+template <class C> WB_DEV C cmul(C a, C b) {
+  return mkc<C>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
-WB_DEV double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-WB_DEV double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+template <class C> WB_DEV C cscale(C a, real_t<C> s) { return mkc<C>(a.x * s, a.y * s); }
+template <class C> WB_DEV C cconj(C a) { return mkc<C>(a.x, -a.y); }
 // multiply by (i * sign), sign = +1 or -1
-template <int S>
-WB_DEV double2 cmul_i(double2 a) {
-  return S > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <int S, class C>
+WB_DEV C cmul_i(C a) {
+  return S > 0 ? mkc<C>(-a.y, a.x) : mkc<C>(a.y, -a.x);
 }
 // twiddle with direction: DIR = +1 uses w, DIR = -1 uses conj(w)
-template <int DIR>
-WB_DEV double2 ctw(double2 a, double2 w) {
+template <int DIR, class C>
+WB_DEV C ctw(C a, C w) {
   if (DIR > 0) return cmul(a, w);
-  return make_double2(fma(a.x, w.x, a.y * w.y), fma(a.y, w.x, -a.x * w.y));
+  return mkc<C>(fma(a.x, w.x, a.y * w.y), fma(a.y, w.x, -a.x * w.y));
 }
 
 // Block-wide sum of one double per thread; result valid in every thread.

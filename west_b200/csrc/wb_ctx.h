@@ -71,6 +71,11 @@ struct wb_ctx {
   size_t evused = 0;
   struct Mark { int stage, e0, e1; };
   std::vector<Mark> marks;
+  // mixed form: FP32 constants (made on first use) and workspace
+  int have32 = 0;
+  wb::FftArgs32 fa32{};
+  DBuf W32, D32, g2kin32, vs32, tw32, g32, P32, T32, d32, sticks32, part32, C32, ecol32, rho0, rho_in, conv_in,
+      act_in, items_in, nact_in;
   // PDEP Davidson state (wb_davidson)
   DBuf dav_dvg, dav_dng, dav_tmp, dav_hr, dav_vr, dav_A, dav_V, dav_w, dav_part, dav_coef, dav_dots;
   int ev_get() {

@@ -50,38 +50,41 @@ template <> struct Factor2<12> { static constexpr int A = 4, B = 3; };
 template <> struct Factor2<16> { static constexpr int A = 4, B = 4; };
 
 // In-register DFT of size R: v[k] <- sum_n v[n] exp(DIR 2 pi i n k / R).
-// NT is the length of the shared twiddle table twN (R divides NT).
-template <int R, int DIR, int NT>
-WB_DEV void rdft(double2* v, const double2* twN) {
+// NT is the length of the shared twiddle table twN (R divides NT).  C is
+// double2 or float2.
+template <int R, int DIR, int NT, class C>
+WB_DEV void rdft(C* v, const C* twN) {
+  using T = real_t<C>;
   if constexpr (R == 1) {
     return;
   } else if constexpr (R == 2) {
-    double2 a = v[0], b = v[1];
+    C a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   } else if constexpr (R == 3) {
-    double2 t1 = cadd(v[1], v[2]);
-    double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-    double2 d = csub(v[1], v[2]);
-    double2 t3 = cmul_i<DIR>(make_double2(kS3 * d.x, kS3 * d.y));
+    C t1 = cadd(v[1], v[2]);
+    C t2 = mkc<C>(v[0].x - T(0.5) * t1.x, v[0].y - T(0.5) * t1.y);
+    C d = csub(v[1], v[2]);
+    C t3 = cmul_i<DIR>(mkc<C>(T(kS3) * d.x, T(kS3) * d.y));
     v[0] = cadd(v[0], t1);
     v[1] = cadd(t2, t3);
     v[2] = csub(t2, t3);
   } else if constexpr (R == 4) {
-    double2 a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
-    double2 c = cadd(v[1], v[3]), d = cmul_i<DIR>(csub(v[1], v[3]));
+    C a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
+    C c = cadd(v[1], v[3]), d = cmul_i<DIR>(csub(v[1], v[3]));
     v[0] = cadd(a, c);
     v[2] = csub(a, c);
     v[1] = cadd(b, d);
     v[3] = csub(b, d);
   } else if constexpr (R == 5) {
-    double2 x0 = v[0];
-    double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-    double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-    double2 a1 = make_double2(x0.x + kC51 * t1.x + kC52 * t2.x, x0.y + kC51 * t1.y + kC52 * t2.y);
-    double2 a2 = make_double2(x0.x + kC52 * t1.x + kC51 * t2.x, x0.y + kC52 * t1.y + kC51 * t2.y);
-    double2 b1 = cmul_i<DIR>(make_double2(kS51 * t3.x + kS52 * t4.x, kS51 * t3.y + kS52 * t4.y));
-    double2 b2 = cmul_i<DIR>(make_double2(kS52 * t3.x - kS51 * t4.x, kS52 * t3.y - kS51 * t4.y));
+    const T c51 = T(kC51), c52 = T(kC52), s51 = T(kS51), s52 = T(kS52);
+    C x0 = v[0];
+    C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+    C t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+    C a1 = mkc<C>(x0.x + c51 * t1.x + c52 * t2.x, x0.y + c51 * t1.y + c52 * t2.y);
+    C a2 = mkc<C>(x0.x + c52 * t1.x + c51 * t2.x, x0.y + c52 * t1.y + c51 * t2.y);
+    C b1 = cmul_i<DIR>(mkc<C>(s51 * t3.x + s52 * t4.x, s51 * t3.y + s52 * t4.y));
+    C b2 = cmul_i<DIR>(mkc<C>(s52 * t3.x - s51 * t4.x, s52 * t3.y - s51 * t4.y));
     v[0] = cadd(x0, cadd(t1, t2));
     v[1] = cadd(a1, b1);
     v[4] = csub(a1, b1);
@@ -89,7 +92,7 @@ WB_DEV void rdft(double2* v, const double2* twN) {
     v[3] = csub(a2, b2);
   } else {
     constexpr int A = Factor2<R>::A, B = Factor2<R>::B;
-    double2 z[B][A];
+    C z[B][A];
 #pragma unroll
     for (int b = 0; b < B; ++b) {
 #pragma unroll
@@ -101,7 +104,7 @@ WB_DEV void rdft(double2* v, const double2* twN) {
     }
 #pragma unroll
     for (int k1 = 0; k1 < A; ++k1) {
-      double2 t[B];
+      C t[B];
 #pragma unroll
       for (int b = 0; b < B; ++b) t[b] = z[b][k1];
       rdft<B, DIR, NT>(t, twN);
@@ -147,8 +150,8 @@ struct Prune {
 // consecutive threads on consecutive lines.  The two steps are separate so a
 // kernel can fuse pointwise work between them; fft_lines runs both.  All
 // functions must be called by all NT threads of the block.
-template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off>
-WB_DEV void fft_step1(double2* data, Off loff, int es, int nlines, const double2* twN) {
+template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off, class C>
+WB_DEV void fft_step1(C* data, Off loff, int es, int nlines, const C* twN) {
   using LP = LinePad<N>;
   using PR = Prune<N>;
   constexpr bool PIN = (PRUNE == PRUNE_IN) && PR::IN_OK;
@@ -159,11 +162,11 @@ WB_DEV void fft_step1(double2* data, Off loff, int es, int nlines, const double2
     int line, n2;
     if (LINE_FAST) { line = it % nlines; n2 = it / nlines; }
     else { line = it / N2; n2 = it % N2; }
-    double2* p = data + loff(line);
-    double2 v[N1];
+    C* p = data + loff(line);
+    C v[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1)
-      v[n1] = (PIN && !PR::in_live(n1)) ? make_double2(0.0, 0.0)
+      v[n1] = (PIN && !PR::in_live(n1)) ? mkc<C>(0, 0)
                                         : p[PADDED ? LP::off_blk(n1, n2) : (N2 * n1 + n2) * es];
     rdft<N1, DIR, N>(v, twN);
 #pragma unroll
@@ -173,8 +176,8 @@ WB_DEV void fft_step1(double2* data, Off loff, int es, int nlines, const double2
   }
 }
 
-template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off>
-WB_DEV void fft_step2(double2* data, Off loff, int es, int nlines, const double2* twN) {
+template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off, class C>
+WB_DEV void fft_step2(C* data, Off loff, int es, int nlines, const C* twN) {
   using LP = LinePad<N>;
   using PR = Prune<N>;
   constexpr bool POUT = (PRUNE == PRUNE_OUT) && PR::OUT_OK;
@@ -187,8 +190,8 @@ WB_DEV void fft_step2(double2* data, Off loff, int es, int nlines, const double2
     if (LINE_FAST) { line = c * LPC + tid % LPC; k1 = tid / LPC; }
     else { line = c * LPC + tid / N1; k1 = tid % N1; }
     const bool act = (tid < LPC * N1) && (line < nlines);
-    double2 v[N2];
-    double2* p = data + (act ? loff(line) : 0);
+    C v[N2];
+    C* p = data + (act ? loff(line) : 0);
     if (act) {
 #pragma unroll
       for (int n2 = 0; n2 < N2; ++n2) v[n2] = p[PADDED ? LP::off_blk(k1, n2) : (N2 * k1 + n2) * es];
@@ -204,8 +207,8 @@ WB_DEV void fft_step2(double2* data, Off loff, int es, int nlines, const double2
   __syncthreads();
 }
 
-template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off>
-WB_DEV void fft_lines(double2* data, Off loff, int es, int nlines, const double2* twN) {
+template <int N, int DIR, int NT, bool LINE_FAST, bool PADDED, int PRUNE = PRUNE_NONE, class Off, class C>
+WB_DEV void fft_lines(C* data, Off loff, int es, int nlines, const C* twN) {
   fft_step1<N, DIR, NT, LINE_FAST, PADDED, PRUNE>(data, loff, es, nlines, twN);
   __syncthreads();
   fft_step2<N, DIR, NT, LINE_FAST, PADDED, PRUNE>(data, loff, es, nlines, twN);

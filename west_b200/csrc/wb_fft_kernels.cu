@@ -28,41 +28,41 @@ constexpr int ZSG = 16;     // stick pairs per CTA in the z passes
 constexpr int ZNT = 256;
 constexpr int PNT = 256;
 
-template <int N>
-WB_DEV void load_tw(double2* tw, const double2* twg) {
+template <int N, class C>
+WB_DEV void load_tw(C* tw, const C* twg) {
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
 }
 
 // ---------------------------------------------------------------------------
 // z pass, inverse: sphere coefficients of a pair of columns -> sticks
 // ---------------------------------------------------------------------------
-template <int N, bool PR>
-__global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, long ld,
+template <int N, bool PR, class C>
+__global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld,
                                               const int2* __restrict__ items, StickTab st,
-                                              double2* __restrict__ out,
-                                              const double2* __restrict__ twg) {
+                                              C* __restrict__ out,
+                                              const C* __restrict__ twg) {
   constexpr int LS = LinePad<N>::LEN | 1;  // odd line stride: conflict-free transposes
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* zb = sm + N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* zb = tw + N;
   const int item = blockIdx.y;
   const int q0 = blockIdx.x * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
   load_tw<N>(tw, twg);
-  for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = make_double2(0.0, 0.0);  // pads too
+  for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = mkc<C>(0, 0);  // pads too
   __syncthreads();
   const int2 it = items[item];
-  const double2* a = src + (long)it.x * ld;
-  const double2* b = src + (long)(it.y >= 0 ? it.y : it.x) * ld;
+  const C* a = src + (long)it.x * ld;
+  const C* b = src + (long)(it.y >= 0 ? it.y : it.x) * ld;
   const bool two = it.y >= 0;
   const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
   for (int g = g0 + threadIdx.x; g < g1; g += ZNT) {
     const int2 qz = st.g_qz[g];
-    const double2 a1 = a[g];
-    const double2 a2 = two ? b[g] : make_double2(0.0, 0.0);
+    const C a1 = a[g];
+    const C a2 = two ? b[g] : mkc<C>(0, 0);
     // pos = a1 + i a2 ; neg = conj(a1 - i a2)
-    const double2 pos = make_double2(a1.x - a2.y, a1.y + a2.x);
-    const double2 neg = make_double2(a1.x + a2.y, a2.x - a1.y);
+    const C pos = mkc<C>(a1.x - a2.y, a1.y + a2.x);
+    const C neg = mkc<C>(a1.x + a2.y, a2.x - a1.y);
     const int z = qz.y;
     using LP = LinePad<N>;
     if (qz.x < 2) {  // the (0,0) stick is its own mirror
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, l
   __syncthreads();
   fft_lines<N, +1, ZNT, false, true, PR ? PRUNE_IN : PRUNE_NONE>(zb, OffLinear{LS}, 1, 2 * nq, tw);
   const int ns = 2 * nq;
-  double2* o = out + (long)item * N * st.nst + 2 * q0;
+  C* o = out + (long)item * N * st.nst + 2 * q0;
   for (int e = threadIdx.x; e < ns * N; e += ZNT) {
     const int s = e % ns, z = e / ns;
     o[(long)z * st.nst + s] = zb[s * LS + LinePad<N>::off(z)];
@@ -87,20 +87,20 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const double2* __restrict__ src, l
 // ---------------------------------------------------------------------------
 // z pass, forward: sticks -> sphere with the Gamma unpack, then an epilogue
 // ---------------------------------------------------------------------------
-template <int N, bool PR, class Epi>
-__global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks,
+template <int N, bool PR, class C, class Epi>
+__global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
                                               const int2* __restrict__ items, StickTab st,
-                                              const double2* __restrict__ twg, Epi epi) {
+                                              const C* __restrict__ twg, Epi epi) {
   constexpr int LS = LinePad<N>::LEN | 1;
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* zb = sm + N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* zb = tw + N;
   const int item = blockIdx.y;
   const int q0 = blockIdx.x * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
   const int ns = 2 * nq;
   load_tw<N>(tw, twg);
-  const double2* s0 = sticks + (long)item * N * st.nst + 2 * q0;
+  const C* s0 = sticks + (long)item * N * st.nst + 2 * q0;
   for (int e = threadIdx.x; e < ns * N; e += ZNT) {
     const int s = e % ns, z = e / ns;
     zb[s * LS + LinePad<N>::off(z)] = s0[(long)z * st.nst + s];
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks
     const int2 qz = st.g_qz[g];
     const int z = qz.y;
     using LP = LinePad<N>;
-    double2 ap, am;
+    C ap, am;
     if (qz.x < 2) {
       ap = zb[LP::off((z + N) % N)];
       am = zb[LP::off((N - z) % N)];
@@ -122,9 +122,10 @@ __global__ void __launch_bounds__(ZNT) k_zfwd(const double2* __restrict__ sticks
       ap = zb[l * LS + LP::off((z + N) % N)];
       am = zb[(l ^ 1) * LS + LP::off((N - z) % N)];
     }
-    const double2 fp = make_double2(0.5 * (ap.x + am.x), 0.5 * (ap.y + am.y));
-    const double2 fm = make_double2(0.5 * (ap.x - am.x), 0.5 * (ap.y - am.y));
-    epi(g, it, make_double2(fp.x, fm.y), make_double2(fp.y, -fm.x));
+    using T = real_t<C>;
+    const C fp = mkc<C>(T(0.5) * (ap.x + am.x), T(0.5) * (ap.y + am.y));
+    const C fm = mkc<C>(T(0.5) * (ap.x - am.x), T(0.5) * (ap.y - am.y));
+    epi(g, it, mkc<C>(fp.x, fm.y), mkc<C>(fp.y, -fm.x));
   }
 }
 
@@ -139,25 +140,29 @@ struct EpiStore {
 
 // T = (V psi + g2kin psi with Im(G=0) = 0) - e psi   (h_psi then
 // apply_sternheimerop_to_m_wfcs.f90:65-74; KB and alpha Pv follow as GEMMs)
-struct EpiHpsi {
-  const double2* P;
-  double2* T;
+template <class C>
+struct EpiHpsiT {
+  using T = real_t<C>;
+  const C* P;
+  C* Tv;
   long ld;
-  const double* g2kin;
-  const double* ecol;
-  WB_DEV void one(int g, int c, double2 vp) const {
-    const double2 p = P[(long)c * ld + g];
-    const double k = g2kin[g];
-    double2 h = make_double2(fma(k, p.x, vp.x), fma(k, p.y, vp.y));
-    if (g == 0) h.y = 0.0;
-    const double e = ecol[c];
-    T[(long)c * ld + g] = make_double2(fma(-e, p.x, h.x), fma(-e, p.y, h.y));
+  const T* g2kin;
+  const T* ecol;
+  WB_DEV void one(int g, int c, C vp) const {
+    const C p = P[(long)c * ld + g];
+    const T k = g2kin[g];
+    C h = mkc<C>(fma(k, p.x, vp.x), fma(k, p.y, vp.y));
+    if (g == 0) h.y = T(0);
+    const T e = ecol[c];
+    Tv[(long)c * ld + g] = mkc<C>(fma(-e, p.x, h.x), fma(-e, p.y, h.y));
   }
-  WB_DEV void operator()(int g, int2 it, double2 b1, double2 b2) const {
+  WB_DEV void operator()(int g, int2 it, C b1, C b2) const {
     one(g, it.x, b1);
     if (it.y >= 0) one(g, it.y, b2);
   }
 };
+using EpiHpsi = EpiHpsiT<double2>;
+using EpiHpsi32 = EpiHpsiT<float2>;
 
 // dng(perm(g), p) = sqvc(g) * drho_G(g), G = 0 zeroed
 // (dfpt_module.f90:485-487,502-503 and apply_operator.f90:63-67)
@@ -180,8 +185,8 @@ struct EpiDng {
 // Zero what the inverse transforms read: with pruning (PR) only the active
 // columns (which then are all x in [0, N/4) u [3N/4, N)) at live rows (y in
 // the same quarters), otherwise the whole plane.
-template <int N, bool PR>
-WB_DEV void plane_zero(double2* pl, const StickTab& st) {
+template <int N, bool PR, class C>
+WB_DEV void plane_zero(C* pl, const StickTab& st) {
   if constexpr (PR && Prune<N>::IN_OK) {
     constexpr int NL = 2 * (N / 4);
     const int nc = st.ncols, nlow = st.xhi + 1;
@@ -189,49 +194,49 @@ WB_DEV void plane_zero(double2* pl, const StickTab& st) {
       const int l = e % nc, r = e / nc;
       const int x = l < nlow ? l : N - nc + l;
       const int y = r < N / 4 ? r : N - NL + r;
-      pl[Plane<N>::at(x, y)] = make_double2(0.0, 0.0);
+      pl[Plane<N>::at(x, y)] = mkc<C>(0, 0);
     }
   } else {
-    for (int e = threadIdx.x; e < Plane<N>::SIZE; e += PNT) pl[e] = make_double2(0.0, 0.0);
+    for (int e = threadIdx.x; e < Plane<N>::SIZE; e += PNT) pl[e] = mkc<C>(0, 0);
   }
 }
 // stick positions are y*N + x in row-major plane order
-template <int N>
-WB_DEV void plane_scatter(double2* pl, const double2* __restrict__ sz, const int* __restrict__ pos, int nst) {
+template <int N, class C>
+WB_DEV void plane_scatter(C* pl, const C* __restrict__ sz, const int* __restrict__ pos, int nst) {
   for (int s = threadIdx.x; s < nst; s += PNT) {
     const int p = pos[s];
     if (p >= 0) pl[Plane<N>::at_lin(p)] = sz[s];
   }
 }
-template <int N>
-WB_DEV void plane_gather(const double2* pl, double2* __restrict__ sz, const int* __restrict__ pos, int nst) {
+template <int N, class C>
+WB_DEV void plane_gather(const C* pl, C* __restrict__ sz, const int* __restrict__ pos, int nst) {
   for (int s = threadIdx.x; s < nst; s += PNT) {
     const int p = pos[s];
-    sz[s] = p >= 0 ? pl[Plane<N>::at_lin(p)] : make_double2(0.0, 0.0);
+    sz[s] = p >= 0 ? pl[Plane<N>::at_lin(p)] : mkc<C>(0, 0);
   }
 }
 // inverse transforms prune inputs, forward transforms prune outputs
-template <int N, int DIR, bool PR>
-WB_DEV void plane_fft_cols(double2* pl, const StickTab& st, const double2* tw) {
+template <int N, int DIR, bool PR, class C>
+WB_DEV void plane_fft_cols(C* pl, const StickTab& st, const C* tw) {
   constexpr int P = !PR ? PRUNE_NONE : (DIR > 0 ? PRUNE_IN : PRUNE_OUT);
   fft_lines<N, DIR, PNT, true, false, P>(pl, OffCols<N>{st.xhi + 1, st.ncols}, Plane<N>::RS, st.ncols, tw);
 }
-template <int N, int DIR, bool PR>
-WB_DEV void plane_fft_rows(double2* pl, const double2* tw) {
+template <int N, int DIR, bool PR, class C>
+WB_DEV void plane_fft_rows(C* pl, const C* tw) {
   constexpr int P = !PR ? PRUNE_NONE : (DIR > 0 ? PRUNE_IN : PRUNE_OUT);
   fft_lines<N, DIR, PNT, false, true, P>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
 }
 
 // psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma)
-template <int N, bool PR>
-__global__ void __launch_bounds__(PNT) k_plane_vloc(double2* __restrict__ sticks, StickTab st,
-                                                    const double* __restrict__ vs,
-                                                    const double2* __restrict__ twg) {
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* pl = sm + N;
+template <int N, bool PR, class C>
+__global__ void __launch_bounds__(PNT) k_plane_vloc(C* __restrict__ sticks, StickTab st,
+                                                    const real_t<C>* __restrict__ vs,
+                                                    const C* __restrict__ twg) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* pl = tw + N;
   const int z = blockIdx.x, item = blockIdx.y;
-  double2* sz = sticks + ((long)item * N + z) * st.nst;
+  C* sz = sticks + ((long)item * N + z) * st.nst;
   load_tw<N>(tw, twg);
   plane_zero<N, PR>(pl, st);
   __syncthreads();
@@ -239,7 +244,7 @@ __global__ void __launch_bounds__(PNT) k_plane_vloc(double2* __restrict__ sticks
   __syncthreads();
   plane_fft_cols<N, +1, PR>(pl, st, tw);
   plane_fft_rows<N, +1, PR>(pl, tw);
-  const double* v = vs + (long)z * N * N;
+  const real_t<C>* v = vs + (long)z * N * N;
   for (int e = threadIdx.x; e < N * N; e += PNT) {
     const int o = Plane<N>::at_lin(e);
     pl[o] = cscale(pl[o], v[e]);
@@ -255,9 +260,9 @@ template <int N, bool PR>
 __global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict__ sticks, StickTab st,
                                                        double2* __restrict__ box,
                                                        const double2* __restrict__ twg) {
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* pl = sm + N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* tw = reinterpret_cast<double2*>(smraw);
+  double2* pl = tw + N;
   const int z = blockIdx.x, item = blockIdx.y;
   const double2* sz = sticks + ((long)item * N + z) * st.nst;
   load_tw<N>(tw, twg);
@@ -278,9 +283,9 @@ __global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ e
                                                    const double2* __restrict__ dvbox, int npv,
                                                    StickTab st, double2* __restrict__ sticks,
                                                    const double2* __restrict__ twg) {
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* pl = sm + N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* tw = reinterpret_cast<double2*>(smraw);
+  double2* pl = tw + N;
   const int z = blockIdx.x, k = blockIdx.y, p = blockIdx.z;
   load_tw<N>(tw, twg);
   const double2* ps = evcr + ((long)k * N + z) * N * N;
@@ -311,9 +316,9 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
                                                     int mb, StickTab st, double2* __restrict__ acc,
                                                     double scale, double2* __restrict__ osticks,
                                                     const double2* __restrict__ twg) {
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* pl = sm + N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2* tw = reinterpret_cast<double2*>(smraw);
+  double2* pl = tw + N;
   const int z = blockIdx.x, pp = blockIdx.y;
   const int npv = (nocc + 1) / 2;
   load_tw<N>(tw, twg);
@@ -363,22 +368,23 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
 // registers before the zero fill so their latency overlaps it.
 constexpr int kFusedMaxSticksPerThread = 4;
 
-template <int N>
-__global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(double2* __restrict__ sticks, StickTab st,
-                                                          const double* __restrict__ vs,
-                                                          const double2* __restrict__ twg) {
+template <int N, class C>
+__global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sticks, StickTab st,
+                                                             const real_t<C>* __restrict__ vs,
+                                                             const C* __restrict__ twg) {
+  using T = real_t<C>;
   constexpr int R = FftSplit<N>::N1;
   static_assert(FftSplit<N>::N1 == FftSplit<N>::N2, "fused rows need N1 == N2");
   constexpr int LPC = PNT / R;
   constexpr int NCH = (N + LPC - 1) / LPC;
   constexpr int MS = kFusedMaxSticksPerThread;
   using LP = LinePad<N>;
-  extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* pl = sm + N;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  C* pl = tw + N;
   const int z = blockIdx.x, item = blockIdx.y, tid = threadIdx.x;
-  double2* sz = sticks + ((long)item * N + z) * st.nst;
-  double2 sv[MS];
+  C* sz = sticks + ((long)item * N + z) * st.nst;
+  C sv[MS];
   int sp[MS];
 #pragma unroll
   for (int i = 0; i < MS; ++i) {
@@ -388,13 +394,13 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(double2* __restrict
   }
   const int k1 = tid % R;
   const bool rowthr = tid < LPC * R;
-  double vr[NCH][R];
-  const double* vz = vs + (long)z * N * N;
+  T vr[NCH][R];
+  const T* vz = vs + (long)z * N * N;
 #pragma unroll
   for (int c = 0; c < NCH; ++c) {
     const int y = c * LPC + tid / R;
 #pragma unroll
-    for (int k2 = 0; k2 < R; ++k2) vr[c][k2] = (rowthr && y < N) ? vz[y * N + k1 + R * k2] : 0.0;
+    for (int k2 = 0; k2 < R; ++k2) vr[c][k2] = (rowthr && y < N) ? vz[y * N + k1 + R * k2] : T(0);
   }
   load_tw<N>(tw, twg);
   plane_zero<N, true>(pl, st);
@@ -410,8 +416,8 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(double2* __restrict
   for (int c = 0; c < NCH; ++c) {
     const int y = c * LPC + tid / R;
     const bool act = rowthr && y < N;
-    double2* p = pl + (act ? y : 0) * Plane<N>::RS;
-    double2 v[R];
+    C* p = pl + (act ? y : 0) * Plane<N>::RS;
+    C v[R];
     if (act) {
 #pragma unroll
       for (int n2 = 0; n2 < R; ++n2) v[n2] = p[LP::off_blk(k1, n2)];
@@ -437,21 +443,21 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(double2* __restrict
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-template <int N>
-static size_t zsmem() { return sizeof(double2) * (N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
-template <int N>
-static size_t psmem() { return sizeof(double2) * (N + Plane<N>::SIZE); }
+template <int N, class C = double2>
+static size_t zsmem() { return sizeof(C) * (N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
+template <int N, class C = double2>
+static size_t psmem() { return sizeof(C) * (N + Plane<N>::SIZE); }
 
 template <int N>
 struct FftN {
   static constexpr bool FUSABLE = FftSplit<N>::N1 == FftSplit<N>::N2 && Prune<N>::IN_OK && Prune<N>::OUT_OK;
   template <bool PR>
   static void setup_pr() {
-    cudaFuncSetAttribute(k_zinv<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_zfwd<N, PR, EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_zfwd<N, PR, EpiHpsi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_zfwd<N, PR, EpiDng>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
-    cudaFuncSetAttribute(k_plane_vloc<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    cudaFuncSetAttribute(k_zinv<N, PR, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, PR, double2, EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, PR, double2, EpiHpsi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_zfwd<N, PR, double2, EpiDng>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N>());
+    cudaFuncSetAttribute(k_plane_vloc<N, PR, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
     cudaFuncSetAttribute(k_plane_inv_box<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
     cudaFuncSetAttribute(k_plane_rhs<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
     cudaFuncSetAttribute(k_plane_drho<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
@@ -459,36 +465,78 @@ struct FftN {
   static void setup() {
     setup_pr<false>();
     setup_pr<true>();
-    if constexpr (FUSABLE)
-      cudaFuncSetAttribute(k_plane_vloc_fused<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+    if constexpr (FUSABLE) {
+      cudaFuncSetAttribute(k_plane_vloc_fused<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+      cudaFuncSetAttribute(k_plane_vloc_fused<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)psmem<N, float2>());
+    }
+    for (int pr = 0; pr < 2; ++pr) {
+      auto zi = pr ? k_zinv<N, true, float2> : k_zinv<N, false, float2>;
+      auto zf = pr ? k_zfwd<N, true, float2, EpiHpsi32> : k_zfwd<N, false, float2, EpiHpsi32>;
+      auto pv = pr ? k_plane_vloc<N, true, float2> : k_plane_vloc<N, false, float2>;
+      cudaFuncSetAttribute(zi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, float2>());
+      cudaFuncSetAttribute(zf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, float2>());
+      cudaFuncSetAttribute(pv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N, float2>());
+    }
+  }
+  // FP32 local potential of the mixed-precision inner PCG
+  static void zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks) {
+    if (nitems <= 0) return;
+    if (f.st.prune)
+      k_zinv<N, true, float2><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(src, ld, items, f.st,
+                                                                                         sticks, f.tw);
+    else
+      k_zinv<N, false, float2><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(src, ld, items, f.st,
+                                                                                          sticks, f.tw);
+  }
+  static void vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs) {
+    if (nitems <= 0) return;
+    const dim3 g(N, nitems);
+    if constexpr (FUSABLE) {
+      if (f.st.prune && f.st.nst <= kFusedMaxSticksPerThread * PNT) {
+        k_plane_vloc_fused<N, float2><<<g, PNT, psmem<N, float2>(), f.stream>>>(sticks, f.st, vs, f.tw);
+        return;
+      }
+    }
+    if (f.st.prune) k_plane_vloc<N, true, float2><<<g, PNT, psmem<N, float2>(), f.stream>>>(sticks, f.st, vs, f.tw);
+    else k_plane_vloc<N, false, float2><<<g, PNT, psmem<N, float2>(), f.stream>>>(sticks, f.st, vs, f.tw);
+  }
+  static void zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, EpiHpsi32 epi) {
+    if (nitems <= 0) return;
+    if (f.st.prune)
+      k_zfwd<N, true, float2, EpiHpsi32><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(
+          sticks, items, f.st, f.tw, epi);
+    else
+      k_zfwd<N, false, float2, EpiHpsi32><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(
+          sticks, items, f.st, f.tw, epi);
   }
   static dim3 zgrid(const StickTab& st, int nitems) { return dim3((st.nsp + ZSG - 1) / ZSG, nitems); }
   static void zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks) {
     if (nitems <= 0) return;
     if (f.st.prune)
-      k_zinv<N, true><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+      k_zinv<N, true, double2><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
     else
-      k_zinv<N, false><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+      k_zinv<N, false, double2><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
   }
   template <class Epi>
   static void zfwd(const FftArgs& f, const double2* sticks, const int2* items, int nitems, Epi epi) {
     if (nitems <= 0) return;
     if (f.st.prune)
-      k_zfwd<N, true, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
+      k_zfwd<N, true, double2, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
     else
-      k_zfwd<N, false, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
+      k_zfwd<N, false, double2, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
   }
   static void vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs) {
     if (nitems <= 0) return;
     const dim3 g(N, nitems);
     if constexpr (FUSABLE) {
       if (f.st.prune && f.st.nst <= kFusedMaxSticksPerThread * PNT) {
-        k_plane_vloc_fused<N><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+        k_plane_vloc_fused<N, double2><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
         return;
       }
     }
-    if (f.st.prune) k_plane_vloc<N, true><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
-    else k_plane_vloc<N, false><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+    if (f.st.prune) k_plane_vloc<N, true, double2><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+    else k_plane_vloc<N, false, double2><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
   }
   static void inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box) {
     if (nitems <= 0) return;
@@ -562,6 +610,22 @@ void fft_zfwd_hpsi(const FftArgs& f, const double2* sticks, const int2* items, i
 void fft_zfwd_dng(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dng, long ld,
                   const int* perm, const double* sqvc) {
 #define X(n) case n: FftN<n>::zfwd(f, sticks, items, nitems, EpiDng{dng, ld, perm, sqvc}); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks) {
+#define X(n) case n: FftN<n>::zinv32(f, src, ld, items, nitems, sticks); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_plane_vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs) {
+#define X(n) case n: FftN<n>::vloc32(f, sticks, nitems, vs); break;
+  WB_DISPATCH(f.n, )
+#undef X
+}
+void fft_zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, const float2* P,
+                     float2* T, long ld, const float* g2kin, const float* ecol) {
+#define X(n) case n: FftN<n>::zfwd_hpsi32(f, sticks, items, nitems, EpiHpsi32{P, T, ld, g2kin, ecol}); break;
   WB_DISPATCH(f.n, )
 #undef X
 }

@@ -23,7 +23,19 @@ struct FftArgs {
   cudaStream_t stream;
 };
 
+// FP32 twin of FftArgs for the mixed-precision inner solves.
+struct FftArgs32 {
+  int n;
+  StickTab st;
+  const float2* tw;
+  cudaStream_t stream;
+};
+
 bool fft_supported(int n);
+void fft_zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks);
+void fft_plane_vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs);
+void fft_zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, const float2* P,
+                     float2* T, long ld, const float* g2kin, const float* ecol);
 void fft_setup(int n);
 void fft_zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks);
 void fft_zfwd_store(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dst, long ld);
@@ -68,5 +80,26 @@ void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int*
 void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
                long ld, cudaStream_t s);
 void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cudaStream_t s);
+
+// ---- mixed form: FP32 inner PCG and FP64 refinement (wb_la.cu) ----
+void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* g2kin, const double* eprec_col,
+                   double* rho_prev, unsigned char* conv, int iter, double tr2, const double* rel, int npw, long ld,
+                   cudaStream_t s);
+void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
+                 cudaStream_t s);
+void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* g2kin,
+                     const double* eprec_col, double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32,
+                     int npw, long ld, cudaStream_t s);
+void refine_accumulate(const int* act, int nact, double2* X, const float2* d32, int npw, long ld, cudaStream_t s);
+void kinetic_hpsi32(const float2* P, float2* T, const float* g2kin, const float* ecol, const int* cols, int ncol,
+                    int npw, long ld, cudaStream_t s);
+void to_float(const double* a, float* b, long n, cudaStream_t s);
+int gemm_tn_splits32(int M, int ncol, int K);
+void gemm_tn32(const float* W, long ldw, int M, const float* X, long ldx, const int* cols, int ncol, int K, int nsplit,
+               float* part, cudaStream_t s);
+void gamma_reduce32(const float* part, int nsplit, int M, int ncol, const float* W, long ldw, const float* X, long ldx,
+                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s);
+void gemm_nn32_acc(const float* W, long ldw, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
+                   cudaStream_t s);
 
 }  // namespace wb

@@ -6,6 +6,8 @@
 // (Re, Im interleaved), exactly as WEST passes them to DGEMM at Gamma
 // (glbrak.f90:37-40, apply_alpha_pc_to_m_wfcs.f90:65-72).
 #include "wb_common.cuh"
+#include <algorithm>
+
 #include "wb_internal.h"
 
 namespace wb {
@@ -297,28 +299,34 @@ void cg_reset(unsigned char* conv, int nsys, cudaStream_t s) {
   k_cg_reset<<<(nsys + 255) / 256, 256, 0, s>>>(conv, nsys);
 }
 
-// h = g / max(1, g2kin/eprec); rho = <h|g>_Gamma; converged if rho < tr2;
-// otherwise P = -h + (rho / rho_prev) P  (P = -h at the first iteration).
-__global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act, const double2* __restrict__ g,
-                                                     double2* __restrict__ P, const double* __restrict__ g2kin,
+// h = g / max(1, g2kin/eprec); rho = <h|g>_Gamma; converged if rho < thr_j
+// (thr_j = tr2 * rel_j when rel != nullptr, else tr2); otherwise
+// P = -h + (rho / rho_prev) P  (P = -h at the first iteration).  C is the
+// vector type (double2, or float2 in the mixed form); scalars are FP64.
+template <class C>
+__global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act, const C* __restrict__ g,
+                                                     C* __restrict__ P, const double* __restrict__ g2kin,
                                                      const double* __restrict__ eprec_col, double* rho_prev,
-                                                     unsigned char* conv, int iter, double tr2, int npw, long ld) {
+                                                     unsigned char* conv, int iter, double tr2,
+                                                     const double* __restrict__ rel, int npw, long ld) {
+  using T = real_t<C>;
   __shared__ double red[16];
   const int j = act[blockIdx.x];
-  const double2* gj = g + (long)j * ld;
-  double2* pj = P + (long)j * ld;
+  const C* gj = g + (long)j * ld;
+  C* pj = P + (long)j * ld;
   const double ep = eprec_col[j];
   double t = 0.0, t0 = 0.0;
   for (int i = threadIdx.x; i < npw; i += 256) {
     const double den = fmax(1.0, g2kin[i] / ep);
-    const double2 gv = gj[i];
-    const double hx = gv.x / den, hy = gv.y / den;
-    t = fma(hx, gv.x, fma(hy, gv.y, t));
-    if (i == 0) t0 = hx * gv.x;
+    const C gv = gj[i];
+    const double hx = (double)gv.x / den, hy = (double)gv.y / den;
+    t = fma(hx, (double)gv.x, fma(hy, (double)gv.y, t));
+    if (i == 0) t0 = hx * (double)gv.x;
   }
   const double2 s = block_sum2<256>(t, t0, red);
   const double rho = 2.0 * s.x - s.y;
-  const bool c = rho < tr2;
+  const double thr = rel ? tr2 * rel[j] : tr2;
+  const bool c = rho < thr;
   if (c) {
     if (threadIdx.x == 0) conv[j] = 1;
     return;
@@ -328,13 +336,13 @@ __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act
   if (threadIdx.x == 0) rho_prev[j] = rho;
   for (int i = threadIdx.x; i < npw; i += 256) {
     const double den = fmax(1.0, g2kin[i] / ep);
-    const double2 gv = gj[i];
-    const double hx = gv.x / den, hy = gv.y / den;
+    const C gv = gj[i];
+    const double hx = (double)gv.x / den, hy = (double)gv.y / den;
     if (iter == 1) {
-      pj[i] = make_double2(-hx, -hy);
+      pj[i] = mkc<C>(T(-hx), T(-hy));
     } else {
-      const double2 pv = pj[i];
-      pj[i] = make_double2(fma(beta, pv.x, -hx), fma(beta, pv.y, -hy));
+      const C pv = pj[i];
+      pj[i] = mkc<C>(T(fma(beta, (double)pv.x, -hx)), T(fma(beta, (double)pv.y, -hy)));
     }
   }
 }
@@ -342,7 +350,14 @@ void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const d
                  const double* eprec_col, double* rho_prev, unsigned char* conv, int iter, double tr2, int npw,
                  long ld, cudaStream_t s) {
   if (nact <= 0) return;
-  k_cg_prec_rho<<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, npw, ld);
+  k_cg_prec_rho<double2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, nullptr, npw,
+                                              ld);
+}
+void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* g2kin, const double* eprec_col,
+                   double* rho_prev, unsigned char* conv, int iter, double tr2, const double* rel, int npw, long ld,
+                   cudaStream_t s) {
+  if (nact <= 0) return;
+  k_cg_prec_rho<float2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, rel, npw, ld);
 }
 
 // Active list in increasing system order (map_lbnd2ibnd, :356-382) and the
@@ -390,37 +405,297 @@ void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int*
 }
 
 // a = <P|g>, c = <P|T> (Gamma); x -= (a/c) P ; g -= (a/c) T     (:253-322)
-__global__ void __launch_bounds__(256) k_cg_update(const int* __restrict__ act, double2* __restrict__ x,
-                                                   double2* __restrict__ g, const double2* __restrict__ P,
-                                                   const double2* __restrict__ T, int npw, long ld) {
+template <class C>
+__global__ void __launch_bounds__(256) k_cg_update(const int* __restrict__ act, C* __restrict__ x,
+                                                   C* __restrict__ g, const C* __restrict__ P,
+                                                   const C* __restrict__ T, int npw, long ld) {
+  using R = real_t<C>;
   __shared__ double red[16];
   const int j = act[blockIdx.x];
-  const double2* pj = P + (long)j * ld;
-  const double2* tj = T + (long)j * ld;
-  double2* gj = g + (long)j * ld;
-  double2* xj = x + (long)j * ld;
+  const C* pj = P + (long)j * ld;
+  const C* tj = T + (long)j * ld;
+  C* gj = g + (long)j * ld;
+  C* xj = x + (long)j * ld;
   double a = 0.0, c = 0.0;
   for (int i = threadIdx.x; i < npw; i += 256) {
-    const double2 p = pj[i], gv = gj[i], t = tj[i];
-    double da = fma(p.x, gv.x, p.y * gv.y);
-    double dc = fma(p.x, t.x, p.y * t.y);
-    if (i == 0) { da -= 0.5 * p.x * gv.x; dc -= 0.5 * p.x * t.x; }
+    const C p = pj[i], gv = gj[i], t = tj[i];
+    double da = fma((double)p.x, (double)gv.x, (double)p.y * (double)gv.y);
+    double dc = fma((double)p.x, (double)t.x, (double)p.y * (double)t.y);
+    if (i == 0) { da -= 0.5 * (double)p.x * (double)gv.x; dc -= 0.5 * (double)p.x * (double)t.x; }
     a += da;
     c += dc;
   }
   const double2 s = block_sum2<256>(a, c, red);
-  const double r = (2.0 * s.x) / (2.0 * s.y);
+  const double rd = (2.0 * s.x) / (2.0 * s.y);
+  const R r = R(rd);
   for (int i = threadIdx.x; i < npw; i += 256) {
-    const double2 p = pj[i], t = tj[i];
-    double2 xv = xj[i], gv = gj[i];
-    xj[i] = make_double2(fma(-r, p.x, xv.x), fma(-r, p.y, xv.y));
-    gj[i] = make_double2(fma(-r, t.x, gv.x), fma(-r, t.y, gv.y));
+    const C p = pj[i], t = tj[i];
+    C xv = xj[i], gv = gj[i];
+    xj[i] = mkc<C>(fma(-r, p.x, xv.x), fma(-r, p.y, xv.y));
+    gj[i] = mkc<C>(fma(-r, t.x, gv.x), fma(-r, t.y, gv.y));
   }
 }
 void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
                long ld, cudaStream_t s) {
   if (nact <= 0) return;
-  k_cg_update<<<nact, 256, 0, s>>>(act, x, g, P, T, npw, ld);
+  k_cg_update<double2><<<nact, 256, 0, s>>>(act, x, g, P, T, npw, ld);
+}
+void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
+                 cudaStream_t s) {
+  if (nact <= 0) return;
+  k_cg_update<float2><<<nact, 256, 0, s>>>(act, x, g, P, T, npw, ld);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 iterative refinement around the FP32 PCG (mixed form)
+// ---------------------------------------------------------------------------
+// R = B - T (FP64); rho = <M^-1 R|R>_Gamma; converged if rho < tr2 (the test of
+// linsolve_sternheimer_m_wfcts.f90:215-216 on the true FP64 residual).
+// Otherwise the FP32 correction solve starts from d = 0 with g = -R.
+__global__ void __launch_bounds__(256) k_refine_residual(const int* __restrict__ act, const double2* __restrict__ B,
+                                                         const double2* __restrict__ T,
+                                                         const double* __restrict__ g2kin,
+                                                         const double* __restrict__ eprec_col, double tr2,
+                                                         unsigned char* conv, double* rho0, float2* __restrict__ g32,
+                                                         float2* __restrict__ d32, int npw, long ld) {
+  __shared__ double red[16];
+  const int j = act[blockIdx.x];
+  const double2* bj = B + (long)j * ld;
+  const double2* tj = T + (long)j * ld;
+  const double ep = eprec_col[j];
+  double t = 0.0, t0 = 0.0;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double2 b = bj[i], a = tj[i];
+    const double rx = b.x - a.x, ry = b.y - a.y;
+    const double den = fmax(1.0, g2kin[i] / ep);
+    t = fma(rx / den, rx, fma(ry / den, ry, t));
+    if (i == 0) t0 = rx / den * rx;
+  }
+  const double2 s = block_sum2<256>(t, t0, red);
+  const double rho = 2.0 * s.x - s.y;
+  const bool c = rho < tr2;
+  if (threadIdx.x == 0) { conv[j] = c ? 1 : 0; rho0[j] = rho; }
+  if (c) return;
+  float2* gj = g32 + (long)j * ld;
+  float2* dj = d32 + (long)j * ld;
+  for (int i = threadIdx.x; i < npw; i += 256) {
+    const double2 b = bj[i], a = tj[i];
+    gj[i] = make_float2((float)(a.x - b.x), (float)(a.y - b.y));
+    dj[i] = make_float2(0.f, 0.f);
+  }
+}
+void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* g2kin,
+                     const double* eprec_col, double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32,
+                     int npw, long ld, cudaStream_t s) {
+  if (nact <= 0) return;
+  k_refine_residual<<<nact, 256, 0, s>>>(act, B, T, g2kin, eprec_col, tr2, conv, rho0, g32, d32, npw, ld);
+}
+
+// x += d for the listed columns
+__global__ void k_refine_accumulate(const int* __restrict__ act, double2* __restrict__ X,
+                                    const float2* __restrict__ d32, int npw, long ld) {
+  const int j = act[blockIdx.y];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
+    const float2 d = d32[(long)j * ld + i];
+    double2 x = X[(long)j * ld + i];
+    X[(long)j * ld + i] = make_double2(x.x + (double)d.x, x.y + (double)d.y);
+  }
+}
+void refine_accumulate(const int* act, int nact, double2* X, const float2* d32, int npw, long ld, cudaStream_t s) {
+  if (nact <= 0) return;
+  k_refine_accumulate<<<dim3((npw + 255) / 256, nact), 256, 0, s>>>(act, X, d32, npw, ld);
+}
+
+// FP32 T = g2kin P (Im at G=0 zeroed) - e P for the kinetic-only operator
+__global__ void k_kinetic_hpsi32(const float2* __restrict__ P, float2* __restrict__ T, const float* __restrict__ g2kin,
+                                 const float* __restrict__ ecol, const int* __restrict__ cols, int npw, long ld) {
+  const int c = cols ? cols[blockIdx.y] : blockIdx.y;
+  const float e = ecol[c];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
+    const float2 p = P[(long)c * ld + i];
+    float2 h = make_float2(p.x * g2kin[i], p.y * g2kin[i]);
+    if (i == 0) h.y = 0.f;
+    T[(long)c * ld + i] = make_float2(fmaf(-e, p.x, h.x), fmaf(-e, p.y, h.y));
+  }
+}
+void kinetic_hpsi32(const float2* P, float2* T, const float* g2kin, const float* ecol, const int* cols, int ncol,
+                    int npw, long ld, cudaStream_t s) {
+  if (ncol <= 0) return;
+  k_kinetic_hpsi32<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(P, T, g2kin, ecol, cols, npw, ld);
+}
+
+__global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+void to_float(const double* a, float* b, long n, cudaStream_t s) {
+  if (n <= 0) return;
+  k_to_float<<<(int)std::min<long>((n + 255) / 256, 4096), 256, 0, s>>>(a, b, n);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 bra-ket GEMMs of the inner solve (SIMT FFMA, shared-memory tiles)
+// ---------------------------------------------------------------------------
+// part[s][j][r] = sum_{k in split s} W[r][k] X[col j][k]; tile 64 r x 64 j, k step 16
+__global__ void __launch_bounds__(256) k_gemm_tn_f32(const float* __restrict__ W, long ldw, int M,
+                                                     const float* __restrict__ X, long ldx,
+                                                     const int* __restrict__ cols, int ncol, int K, int kchunk,
+                                                     float* __restrict__ part) {
+  __shared__ float Ws[16][64 + 4];
+  __shared__ float Xs[16][64 + 4];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  const int r0 = blockIdx.x * 64, j0 = blockIdx.y * 64, split = blockIdx.z;
+  const int kb = split * kchunk, ke = min(K, kb + kchunk);
+  float acc[4][4] = {};
+  // loader: 64 rows x 8 float2 per operand, two per thread
+  const int lrow = tid / 8, lk = (tid % 8) * 2;
+  const float* wrow[2];
+  const float* xrow[2];
+  bool wok[2], xok[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = r0 + lrow + 32 * h;
+    wok[h] = r < M;
+    wrow[h] = W + (long)(wok[h] ? r : 0) * ldw;
+    const int j = j0 + lrow + 32 * h;
+    xok[h] = j < ncol;
+    const int cj = xok[h] ? (cols ? cols[j] : j) : 0;
+    xrow[h] = X + (long)cj * ldx;
+  }
+  for (int k0 = kb; k0 < ke; k0 += 16) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int k = k0 + lk;
+      float2 wv = make_float2(0.f, 0.f), xv = make_float2(0.f, 0.f);
+      if (wok[h] && k < ke) wv = *reinterpret_cast<const float2*>(wrow[h] + k);
+      if (xok[h] && k < ke) xv = *reinterpret_cast<const float2*>(xrow[h] + k);
+      Ws[lk][lrow + 32 * h] = wv.x; Ws[lk + 1][lrow + 32 * h] = wv.y;
+      Xs[lk][lrow + 32 * h] = xv.x; Xs[lk + 1][lrow + 32 * h] = xv.y;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) { a[i] = Ws[kk][ty * 4 + i]; b[i] = Xs[kk][tx * 4 + i]; }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] = fmaf(a[i], b[q], acc[i][q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = r0 + ty * 4 + i, j = j0 + tx * 4 + q;
+      if (r < M && j < ncol) part[((long)split * ncol + j) * M + r] = acc[i][q];
+    }
+}
+
+int gemm_tn_splits32(int M, int ncol, int K) {
+  const int tiles = ((M + 63) / 64) * ((ncol + 63) / 64);
+  int ns = (2 * 148 * 2 + tiles - 1) / tiles;
+  const int maxs = (K + 511) / 512;
+  if (ns > maxs) ns = maxs;
+  if (ns < 1) ns = 1;
+  return ns;
+}
+
+void gemm_tn32(const float* W, long ldw, int M, const float* X, long ldx, const int* cols, int ncol, int K, int nsplit,
+               float* part, cudaStream_t s) {
+  if (ncol <= 0 || M <= 0) return;
+  int kchunk = (K + nsplit - 1) / nsplit;
+  kchunk = (kchunk + 15) / 16 * 16;
+  dim3 grid((M + 63) / 64, (ncol + 63) / 64, nsplit);
+  k_gemm_tn_f32<<<grid, 256, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, K, kchunk, part);
+}
+
+__global__ void __launch_bounds__(256) k_gamma_reduce32(const float* __restrict__ part, int nsplit, int M, int ncol,
+                                                        const float* __restrict__ W, long ldw,
+                                                        const float* __restrict__ X, long ldx,
+                                                        const int* __restrict__ cols, const float* __restrict__ D,
+                                                        int nkb, float alpha, float* __restrict__ C) {
+  extern __shared__ float Sf[];
+  const int j = blockIdx.x;
+  const int col = cols ? cols[j] : j;
+  const float x0 = X[(long)col * ldx];
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    float sum = 0.f;
+    for (int sp = 0; sp < nsplit; ++sp) sum += part[((long)sp * ncol + j) * M + r];
+    Sf[r] = 2.f * sum - W[(long)r * ldw] * x0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    float c;
+    if (r < nkb) {
+      c = 0.f;
+      for (int q = 0; q < nkb; ++q) c = fmaf(D[r + (long)q * nkb], Sf[q], c);
+    } else {
+      c = alpha * Sf[r];
+    }
+    C[(long)j * M + r] = c;
+  }
+}
+void gamma_reduce32(const float* part, int nsplit, int M, int ncol, const float* W, long ldw, const float* X, long ldx,
+                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s) {
+  if (ncol <= 0 || M <= 0) return;
+  k_gamma_reduce32<<<ncol, 256, sizeof(float) * M, s>>>(part, nsplit, M, ncol, W, ldw, X, ldx, cols, D, nkb, alpha, C);
+}
+
+// Y[col j][k] += sum_r W[r][k] C[j][r]; tile 128 k x 32 j, r step 16
+__global__ void __launch_bounds__(256) k_gemm_nn_f32(const float* __restrict__ W, long ldw, int M,
+                                                     const float* __restrict__ C, float* __restrict__ Y, long ldy,
+                                                     const int* __restrict__ cols, int ncol, int K) {
+  __shared__ float Ws[16][128 + 4];
+  __shared__ float Cs[16][32 + 1];
+  const int tid = threadIdx.x, tx = tid % 32, ty = tid / 32;
+  const int k0 = blockIdx.x * 128, j0 = blockIdx.y * 32;
+  float acc[4][4] = {};  // [k i][j q]: k = k0 + tx*4 + i, j = j0 + ty*4 + q
+  for (int rb = 0; rb < M; rb += 16) {
+    for (int e = tid; e < 16 * 64; e += 256) {           // W tile: 16 r x 64 float2
+      const int rr = e / 64, kk = (e % 64) * 2;
+      const int r = rb + rr, k = k0 + kk;
+      float2 v = make_float2(0.f, 0.f);
+      if (r < M && k < K) v = *reinterpret_cast<const float2*>(W + (long)r * ldw + k);
+      Ws[rr][kk] = v.x; Ws[rr][kk + 1] = v.y;
+    }
+    for (int e = tid; e < 16 * 32; e += 256) {           // C tile: 16 r x 32 j
+      const int rr = e % 16, jj = e / 16;
+      const int r = rb + rr, j = j0 + jj;
+      Cs[rr][jj] = (r < M && j < ncol) ? C[(long)j * M + r] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int rr = 0; rr < 16; ++rr) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) { a[i] = Ws[rr][tx * 4 + i]; b[i] = Cs[rr][ty * 4 + i]; }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] = fmaf(a[i], b[q], acc[i][q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int j = j0 + ty * 4 + q;
+    if (j >= ncol) continue;
+    const int col = cols ? cols[j] : j;
+    float* y = Y + (long)col * ldy;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int k = k0 + tx * 4 + i;
+      if (k < K) y[k] += acc[i][q];
+    }
+  }
+}
+void gemm_nn32_acc(const float* W, long ldw, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
+                   cudaStream_t s) {
+  if (ncol <= 0 || M <= 0) return;
+  dim3 grid((K + 127) / 128, (ncol + 31) / 32);
+  k_gemm_nn_f32<<<grid, 256, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, K);
 }
 
 __global__ void k_count_unconverged(const unsigned char* __restrict__ conv, int nocc, int mb, int* __restrict__ out) {

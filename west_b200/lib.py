@@ -50,7 +50,7 @@ class WbStats(ctypes.Structure):
     _fields_ = [("m", _i), ("cg_iterations", _i), ("cg_active_sum", ctypes.c_longlong),
                 ("fft_boxes", ctypes.c_longlong), ("launches", ctypes.c_longlong), ("ms_total", _d),
                 ("stage_ms", _d * 10), ("stage_launches", ctypes.c_longlong * 10),
-                ("stage_items", ctypes.c_longlong * 10)]
+                ("stage_items", ctypes.c_longlong * 10), ("refinements", _i)]
 
 
 class WbDavidsonParams(ctypes.Structure):
