@@ -327,12 +327,18 @@ def run_b200(args, rank, world, local_rank):
     st_mixed = op.stats()
     dng_mixed = dng_d.cpu().numpy().T
     err_mixed = float(np.linalg.norm(dng_mixed - dng_val) / np.linalg.norm(dng_val))
+    op.set_profiling("all")
+    op.apply_operator(m, dvg_d, dng_d, TR2)
+    mixed_stages = op.stats()["stages"]
+    op.set_profiling(None)
     op.set_precision("fp64")
     if rank == 0:
         v_mixed = world * m * args.steps / (ms_mixed * 1e-3)
         line["mixed"] = {"value": v_mixed, "unit": UNIT, "ms_per_step": ms_mixed / args.steps,
                          "speedup_vs_fp64": v_mixed / value, "dng_rel_err_vs_fp64": err_mixed,
                          "refinements": st_mixed["refinements"], "inner_iterations": st_mixed["cg_iterations"],
+                         "stage_share": {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in mixed_stages.values())), 4)
+                                         for k, v in mixed_stages.items()},
                          "precision": "FP32 PCG corrections + FP32 FFTs and projector GEMMs, FP64 refinement"}
         if not args.no_pdep:
             line["mixed"]["time_to_pdep"] = _time_to_pdep(local_rank, "mixed")

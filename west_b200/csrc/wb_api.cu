@@ -299,7 +299,7 @@ void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const i
 // ---------------------------------------------------------------------------
 // mixed form: FP32 correction solves inside FP64 iterative refinement
 // ---------------------------------------------------------------------------
-constexpr double kInnerRhoReduction = 1e-9;  // inner PCG stops at rho < 1e-9 rho(outer residual)
+constexpr double kInnerRhoReduction = 1e-9;  // inner PCG target: rho below 1e-9 of the outer residual's
 constexpr int kMaxRefinements = 12;
 
 int ensure_fp32(wb_ctx* c, int nsys, int nitems) {
@@ -380,9 +380,11 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
   }
 }
 
-// Solves (H - e_v + alpha Pv) x_v = b_v for all systems of the batch: FP64
-// residuals and tests, FP32 masked PCG corrections.  X holds the initial
-// guess on entry (dfpt_module.f90:348) and the solution on exit.
+// Solves (H - e_v + alpha Pv) x_v = b_v for all systems of the batch with an
+// FP32 masked PCG whose residual is replaced, at each refinement, by the FP64
+// residual b - A x of the FP64 solution (reliable updates); convergence is
+// tested on the FP64 residual with the reference's rho < tr2.  X holds the
+// initial guess on entry (dfpt_module.f90:348) and the solution on exit.
 int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
   cudaStream_t s = c->stream;
   const int npw = c->npw, nocc = c->nocc, nsys = mb * nocc;
@@ -416,18 +418,24 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     WB_CU(cudaMemcpyAsync(cin, conv, nsys, cudaMemcpyDeviceToDevice, s));
     cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
     int nin = nact;
-    for (int it = 1; it <= c->maxiter; ++it) {
+    // the FP32 PCG continues across refinements (search directions and rho
+    // kept, only the residual replaced by the FP64 one), so the iteration
+    // counter and the n_dfpt_maxiter budget are shared
+    while (inner_total < c->maxiter) {
+      const int it = inner_total + 1;
       {
         Stage g(c, WB_STAGE_CG, 2, nin);
+        // stop at rho < max(1e-9 rho_outer, tr2): the first correction from x0 is the
+        // reference's own PCG (same Krylov space, same stopping test)
         cg_prec_rho32(ain, nin, c->g32.as<float2>(), c->P32.as<float2>(), c->g2kin.as<double>(),
                       c->epcol.as<double>(), c->rho_in.as<double>(), cin, it, kInnerRhoReduction,
-                      c->rho0.as<double>(), npw, ld, s);
+                      c->rho0.as<double>(), tr2, npw, ld, s);
         cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
       }
       WB_CU(cudaStreamSynchronize(s));
       nin = *c->nact_host;
-      if (nin == 0) break;
       ++inner_total;
+      if (nin == 0) break;
       c->stats.cg_active_sum += nin;
       apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), ain, iin, nin, nsplit32);
       {

@@ -82,9 +82,10 @@ void cg_update(const int* act, int nact, double2* x, double2* g, const double2* 
 void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cudaStream_t s);
 
 // ---- mixed form: FP32 inner PCG and FP64 refinement (wb_la.cu) ----
+// inner test: rho < max(eta * rel[j], floor)
 void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* g2kin, const double* eprec_col,
-                   double* rho_prev, unsigned char* conv, int iter, double tr2, const double* rel, int npw, long ld,
-                   cudaStream_t s);
+                   double* rho_prev, unsigned char* conv, int iter, double eta, const double* rel, double floor,
+                   int npw, long ld, cudaStream_t s);
 void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
                  cudaStream_t s);
 void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* g2kin,

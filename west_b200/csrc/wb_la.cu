@@ -300,7 +300,7 @@ void cg_reset(unsigned char* conv, int nsys, cudaStream_t s) {
 }
 
 // h = g / max(1, g2kin/eprec); rho = <h|g>_Gamma; converged if rho < thr_j
-// (thr_j = tr2 * rel_j when rel != nullptr, else tr2); otherwise
+// (thr_j = max(tr2 * rel_j, floor) when rel != nullptr, else tr2); otherwise
 // P = -h + (rho / rho_prev) P  (P = -h at the first iteration).  C is the
 // vector type (double2, or float2 in the mixed form); scalars are FP64.
 template <class C>
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act
                                                      C* __restrict__ P, const double* __restrict__ g2kin,
                                                      const double* __restrict__ eprec_col, double* rho_prev,
                                                      unsigned char* conv, int iter, double tr2,
-                                                     const double* __restrict__ rel, int npw, long ld) {
+                                                     const double* __restrict__ rel, double floor, int npw, long ld) {
   using T = real_t<C>;
   __shared__ double red[16];
   const int j = act[blockIdx.x];
@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act
   }
   const double2 s = block_sum2<256>(t, t0, red);
   const double rho = 2.0 * s.x - s.y;
-  const double thr = rel ? tr2 * rel[j] : tr2;
+  const double thr = rel ? fmax(tr2 * rel[j], floor) : tr2;
   const bool c = rho < thr;
   if (c) {
     if (threadIdx.x == 0) conv[j] = 1;
@@ -350,14 +350,15 @@ void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const d
                  const double* eprec_col, double* rho_prev, unsigned char* conv, int iter, double tr2, int npw,
                  long ld, cudaStream_t s) {
   if (nact <= 0) return;
-  k_cg_prec_rho<double2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, nullptr, npw,
-                                              ld);
+  k_cg_prec_rho<double2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, nullptr, 0.0,
+                                              npw, ld);
 }
 void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* g2kin, const double* eprec_col,
-                   double* rho_prev, unsigned char* conv, int iter, double tr2, const double* rel, int npw, long ld,
-                   cudaStream_t s) {
+                   double* rho_prev, unsigned char* conv, int iter, double eta, const double* rel, double floor,
+                   int npw, long ld, cudaStream_t s) {
   if (nact <= 0) return;
-  k_cg_prec_rho<float2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, rel, npw, ld);
+  k_cg_prec_rho<float2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, eta, rel, floor, npw,
+                                             ld);
 }
 
 // Active list in increasing system order (map_lbnd2ibnd, :356-382) and the
