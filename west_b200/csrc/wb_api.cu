@@ -299,7 +299,7 @@ void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const i
 // ---------------------------------------------------------------------------
 // mixed form: FP32 correction solves inside FP64 iterative refinement
 // ---------------------------------------------------------------------------
-constexpr double kInnerRhoReduction = 1e-9;  // inner PCG target: rho below 1e-9 of the outer residual's
+constexpr double kInnerRhoReduction = 1e-10;  // inner PCG target: rho below 1e-10 of the outer residual's
 constexpr int kMaxRefinements = 12;
 
 int ensure_fp32(wb_ctx* c, int nsys, int nitems) {
@@ -380,11 +380,11 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
   }
 }
 
-// Solves (H - e_v + alpha Pv) x_v = b_v for all systems of the batch with an
-// FP32 masked PCG whose residual is replaced, at each refinement, by the FP64
-// residual b - A x of the FP64 solution (reliable updates); convergence is
-// tested on the FP64 residual with the reference's rho < tr2.  X holds the
-// initial guess on entry (dfpt_module.f90:348) and the solution on exit.
+// Solves (H - e_v + alpha Pv) x_v = b_v for all systems of the batch by FP64
+// iterative refinement: FP64 residual r = b - A x, the reference's test
+// <r|M^-1 r> < tr2, then an FP32 masked PCG for A d = r (restarted from d = 0)
+// and x += d in FP64.  X holds the initial guess on entry
+// (dfpt_module.f90:348) and the solution on exit.
 int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
   cudaStream_t s = c->stream;
   const int npw = c->npw, nocc = c->nocc, nsys = mb * nocc;
@@ -407,8 +407,8 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     apply_A(c, X, T, act, items, nact, nsys, nsplit);                    // FP64 A x
     {
       Stage g(c, WB_STAGE_CG, 2, nact);
-      refine_residual(act, nact, B, T, c->g2kin.as<double>(), c->epcol.as<double>(), tr2, conv,
-                      c->rho0.as<double>(), c->g32.as<float2>(), c->d32.as<float2>(), npw, ld, s);
+      refine_residual(act, nact, B, T, c->iprec.as<double>(), nocc, tr2, conv, c->rho0.as<double>(),
+                      c->g32.as<float2>(), c->d32.as<float2>(), npw, ld, s);
       cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
     }
     WB_CU(cudaStreamSynchronize(s));
@@ -418,24 +418,21 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     WB_CU(cudaMemcpyAsync(cin, conv, nsys, cudaMemcpyDeviceToDevice, s));
     cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
     int nin = nact;
-    // the FP32 PCG continues across refinements (search directions and rho
-    // kept, only the residual replaced by the FP64 one), so the iteration
-    // counter and the n_dfpt_maxiter budget are shared
-    while (inner_total < c->maxiter) {
-      const int it = inner_total + 1;
+    // each refinement restarts the FP32 PCG from d = 0 on the FP64 residual;
+    // the refinements share the n_dfpt_maxiter budget
+    for (int it = 1; inner_total < c->maxiter; ++it) {
       {
         Stage g(c, WB_STAGE_CG, 2, nin);
-        // stop at rho < max(1e-9 rho_outer, tr2): the first correction from x0 is the
+        // stop at rho < max(1e-10 rho_outer, tr2): the first correction from x0 is the
         // reference's own PCG (same Krylov space, same stopping test)
-        cg_prec_rho32(ain, nin, c->g32.as<float2>(), c->P32.as<float2>(), c->g2kin.as<double>(),
-                      c->epcol.as<double>(), c->rho_in.as<double>(), cin, it, kInnerRhoReduction,
-                      c->rho0.as<double>(), tr2, npw, ld, s);
+        cg_prec_rho32(ain, nin, c->g32.as<float2>(), c->P32.as<float2>(), c->iprec.as<double>(), nocc,
+                      c->rho_in.as<double>(), cin, it, kInnerRhoReduction, c->rho0.as<double>(), tr2, npw, ld, s);
         cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
       }
       WB_CU(cudaStreamSynchronize(s));
       nin = *c->nact_host;
-      ++inner_total;
       if (nin == 0) break;
+      ++inner_total;
       c->stats.cg_active_sum += nin;
       apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), ain, iin, nin, nsplit32);
       {
@@ -504,7 +501,7 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
                  1.0, c->C.as<double>(), s);
     gemm_nn(Wevc, K, nocc, c->C.as<double>(), (double*)B, 2 * ld, nullptr, nsys, K, -1.0, s);
     // 5. dpsi = precondition(dvpsi)                    (dfpt_module.f90:348)
-    precondition(B, X, c->g2kin.as<double>(), c->epcol.as<double>(), npw, nsys, ld, s);
+    precondition(B, X, c->iprec.as<double>(), nocc, npw, nsys, ld, s);
   }
   // 6. PCG                                           (dfpt_module.f90:350-361)
   int iters = 0;
@@ -529,8 +526,7 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
     for (int it = 1; it <= c->maxiter; ++it) {                   // :146
       {
         Stage g(c, WB_STAGE_CG, 2, nact);
-        cg_prec_rho(act, nact, G, B, c->g2kin.as<double>(), c->epcol.as<double>(), c->rho.as<double>(), conv, it,
-                    tr2, npw, ld, s);
+        cg_prec_rho(act, nact, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, it, tr2, npw, ld, s);
         cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
       }
       WB_CU(cudaStreamSynchronize(s));
@@ -716,6 +712,8 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
       c->sticks.ensure(sizeof(double2) * (size_t)N * c->st.nst * c->npv))
     return bail(fail(WB_ERR_NOMEM, "device allocation failed"));
   set_eprec(c->evc.as<double2>(), c->g2kin.as<double>(), npw, c->nocc, c->eprec.as<double>(), c->stream);
+  if (c->iprec.ensure(sizeof(double) * (size_t)npw * c->nocc)) return bail(fail(WB_ERR_NOMEM, "device allocation failed"));
+  make_iprec(c->g2kin.as<double>(), c->eprec.as<double>(), npw, c->nocc, c->iprec.as<double>(), c->stream);
   std::vector<int2> ib;
   pair_items(ib, 0, c->nocc);
   if (cudaMemcpy(c->iota_items.p, ib.data(), sizeof(int2) * ib.size(), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -734,7 +732,7 @@ int wb_ctx_destroy(wb_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DBuf* bufs[] = {&c->perm, &c->gqz, &c->spg, &c->stpos, &c->tw, &c->g2kin, &c->sqvc, &c->vs, &c->evc, &c->W,
-                  &c->D, &c->eprec, &c->et, &c->occ, &c->evcr, &c->dvg_in, &c->dng_out, &c->aux, &c->dvbox, &c->B,
+                  &c->D, &c->eprec, &c->et, &c->occ, &c->evcr, &c->iprec, &c->dvg_in, &c->dng_out, &c->aux, &c->dvbox, &c->B,
                   &c->X, &c->G, &c->T, &c->sticks, &c->sticks2, &c->acc, &c->part, &c->C, &c->rho, &c->conv,
                   &c->act, &c->items, &c->nact, &c->ecol, &c->epcol, &c->unconv, &c->items_pp, &c->items_pk,
                   &c->iota_items, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
@@ -936,7 +934,7 @@ int noalloc_run(wb_ctx* c, const NoallocWs& w, int mb, const double2* dvg, long 
   gemm_tn(Wevc, K, nocc, (const double*)w.B, 2 * ld, nullptr, nsys, K, w.nsplit, w.part, s);
   gamma_reduce(w.part, w.nsplit, nocc, nsys, Wevc, K, (const double*)w.B, 2 * ld, nullptr, nullptr, 0, 1.0, w.C, s);
   gemm_nn(Wevc, K, nocc, w.C, (double*)w.B, 2 * ld, nullptr, nsys, K, -1.0, s);
-  precondition(w.B, w.X, c->g2kin.as<double>(), w.epcol, npw, nsys, ld, s);
+  precondition(w.B, w.X, c->iprec.as<double>(), nocc, npw, nsys, ld, s);
   int iters = 0;
   if (tr2 >= 0.0) {
     cg_reset(w.conv, nsys, s);
@@ -945,7 +943,7 @@ int noalloc_run(wb_ctx* c, const NoallocWs& w, int mb, const double2* dvg, long 
     sub_into(w.T, w.B, w.G, npw, nsys, ld, s);
     int nact = nsys;
     for (int it = 1; it <= c->maxiter; ++it) {
-      cg_prec_rho(w.act, nact, w.G, w.B, c->g2kin.as<double>(), w.epcol, w.rho, w.conv, it, tr2, npw, ld, s);
+      cg_prec_rho(w.act, nact, w.G, w.B, c->iprec.as<double>(), nocc, w.rho, w.conv, it, tr2, npw, ld, s);
       cg_compact(w.conv, nsys, w.act, w.items, w.nact, c->nact_host, s);
       WB_CU(cudaStreamSynchronize(s));
       nact = *c->nact_host;

@@ -58,7 +58,7 @@ struct wb_ctx {
   wb::StickTab st{};
   wb::FftArgs fa{};
   // constant device data
-  DBuf perm, gqz, spg, stpos, tw, g2kin, sqvc, vs, evc, W, D, eprec, et, occ, evcr;
+  DBuf perm, gqz, spg, stpos, tw, g2kin, sqvc, vs, evc, W, D, eprec, et, occ, evcr, iprec;
   // per-call workspace
   DBuf dvg_in, dng_out, aux, dvbox, B, X, G, T, sticks, sticks2, acc, part, C, rho, conv, act, items, nact,
       ecol, epcol, unconv, items_pp, items_pk, iota_items;

@@ -64,17 +64,19 @@ void gemm_nn(const double* W, long ldw, int M, const double* C, double* Y, long 
 
 void permute_scale(const double2* dvg, long ld_in, const int* perm, const double* sqvc, int npw, int m,
                    double2* aux, long ld_out, cudaStream_t s);
-void precondition(const double2* f, double2* pf, const double* g2kin, const double* eprec_col, int npw, int ncol,
-                  long ld, cudaStream_t s);
+// iprec[v][i] = 1 / max(1, g2kin[i] / eprec[v])
+void make_iprec(const double* g2kin, const double* eprec, int npw, int nocc, double* iprec, cudaStream_t s);
+// column j uses band j % nocc
+void precondition(const double2* f, double2* pf, const double* iprec, int nocc, int npw, int ncol, long ld,
+                  cudaStream_t s);
 void sub_into(const double2* a, const double2* b, double2* out, int npw, int ncol, long ld, cudaStream_t s);
 void kinetic_hpsi(const double2* P, double2* T, const double* g2kin, const double* ecol, const int* cols, int ncol,
                   int npw, long ld, cudaStream_t s);
 void set_eprec(const double2* evc, const double* g2kin, int npw, int nocc, double* eprec, cudaStream_t s);
 void fill_columns(const double* per_band, int nocc, int nsys, double* out, cudaStream_t s);
 void cg_reset(unsigned char* conv, int nsys, cudaStream_t s);
-void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* g2kin,
-                 const double* eprec_col, double* rho_prev, unsigned char* conv, int iter, double tr2, int npw,
-                 long ld, cudaStream_t s);
+void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* iprec, int nocc,
+                 double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s);
 void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int* nact_dev, int* nact_host,
                 cudaStream_t s);
 void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
@@ -83,14 +85,14 @@ void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cu
 
 // ---- mixed form: FP32 inner PCG and FP64 refinement (wb_la.cu) ----
 // inner test: rho < max(eta * rel[j], floor)
-void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* g2kin, const double* eprec_col,
+void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* iprec, int nocc,
                    double* rho_prev, unsigned char* conv, int iter, double eta, const double* rel, double floor,
                    int npw, long ld, cudaStream_t s);
 void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
                  cudaStream_t s);
-void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* g2kin,
-                     const double* eprec_col, double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32,
-                     int npw, long ld, cudaStream_t s);
+void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* iprec, int nocc,
+                     double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32, int npw, long ld,
+                     cudaStream_t s);
 void refine_accumulate(const int* act, int nact, double2* X, const float2* d32, int npw, long ld, cudaStream_t s);
 void kinetic_hpsi32(const float2* P, float2* T, const float* g2kin, const float* ecol, const int* cols, int ncol,
                     int npw, long ld, cudaStream_t s);

@@ -216,22 +216,33 @@ void permute_scale(const double2* dvg, long ld_in, const int* perm, const double
   k_permute_scale<<<dim3((npw + 255) / 256, m), 256, 0, s>>>(dvg, ld_in, perm, sqvc, npw, aux, ld_out);
 }
 
+// 1 / max(1, g2kin / eprec_v) per band and G: the preconditioner of
+// precondition_m_wfcts.f90:35-51 and linsolve_sternheimer_m_wfcts.f90:150-160,
+// applied by multiplication.
+__global__ void k_make_iprec(const double* __restrict__ g2kin, const double* __restrict__ eprec, int npw, int nocc,
+                             double* __restrict__ iprec) {
+  const int v = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x)
+    iprec[(long)v * npw + i] = 1.0 / fmax(1.0, g2kin[i] / eprec[v]);
+}
+void make_iprec(const double* g2kin, const double* eprec, int npw, int nocc, double* iprec, cudaStream_t s) {
+  k_make_iprec<<<dim3((npw + 255) / 256, nocc), 256, 0, s>>>(g2kin, eprec, npw, nocc, iprec);
+}
+
 // pf = f / max(1, g2kin / eprec)         (precondition_m_wfcts.f90:35-51)
 __global__ void k_precondition(const double2* __restrict__ f, double2* __restrict__ pf,
-                               const double* __restrict__ g2kin, const double* __restrict__ eprec_col, int npw,
-                               long ld) {
+                               const double* __restrict__ iprec, int nocc, int npw, long ld) {
   const int j = blockIdx.y;
-  const double ep = eprec_col[j];
+  const double* ip = iprec + (long)(j % nocc) * npw;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
-    const double den = fmax(1.0, g2kin[i] / ep);
     const double2 v = f[(long)j * ld + i];
-    pf[(long)j * ld + i] = make_double2(v.x / den, v.y / den);
+    pf[(long)j * ld + i] = make_double2(v.x * ip[i], v.y * ip[i]);
   }
 }
-void precondition(const double2* f, double2* pf, const double* g2kin, const double* eprec_col, int npw, int ncol,
-                  long ld, cudaStream_t s) {
+void precondition(const double2* f, double2* pf, const double* iprec, int nocc, int npw, int ncol, long ld,
+                  cudaStream_t s) {
   if (ncol <= 0) return;
-  k_precondition<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(f, pf, g2kin, eprec_col, npw, ld);
+  k_precondition<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(f, pf, iprec, nocc, npw, ld);
 }
 
 __global__ void k_sub_into(const double2* __restrict__ a, const double2* __restrict__ b, double2* __restrict__ out,
@@ -305,8 +316,8 @@ void cg_reset(unsigned char* conv, int nsys, cudaStream_t s) {
 // vector type (double2, or float2 in the mixed form); scalars are FP64.
 template <class C>
 __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act, const C* __restrict__ g,
-                                                     C* __restrict__ P, const double* __restrict__ g2kin,
-                                                     const double* __restrict__ eprec_col, double* rho_prev,
+                                                     C* __restrict__ P, const double* __restrict__ iprec, int nocc,
+                                                     double* rho_prev,
                                                      unsigned char* conv, int iter, double tr2,
                                                      const double* __restrict__ rel, double floor, int npw, long ld) {
   using T = real_t<C>;
@@ -314,12 +325,12 @@ __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act
   const int j = act[blockIdx.x];
   const C* gj = g + (long)j * ld;
   C* pj = P + (long)j * ld;
-  const double ep = eprec_col[j];
+  const double* ip = iprec + (long)(j % nocc) * npw;
   double t = 0.0, t0 = 0.0;
   for (int i = threadIdx.x; i < npw; i += 256) {
-    const double den = fmax(1.0, g2kin[i] / ep);
+    const double w = ip[i];
     const C gv = gj[i];
-    const double hx = (double)gv.x / den, hy = (double)gv.y / den;
+    const double hx = (double)gv.x * w, hy = (double)gv.y * w;
     t = fma(hx, (double)gv.x, fma(hy, (double)gv.y, t));
     if (i == 0) t0 = hx * (double)gv.x;
   }
@@ -335,9 +346,9 @@ __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act
   __syncthreads();
   if (threadIdx.x == 0) rho_prev[j] = rho;
   for (int i = threadIdx.x; i < npw; i += 256) {
-    const double den = fmax(1.0, g2kin[i] / ep);
+    const double w = ip[i];
     const C gv = gj[i];
-    const double hx = (double)gv.x / den, hy = (double)gv.y / den;
+    const double hx = (double)gv.x * w, hy = (double)gv.y * w;
     if (iter == 1) {
       pj[i] = mkc<C>(T(-hx), T(-hy));
     } else {
@@ -346,19 +357,17 @@ __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act
     }
   }
 }
-void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* g2kin,
-                 const double* eprec_col, double* rho_prev, unsigned char* conv, int iter, double tr2, int npw,
-                 long ld, cudaStream_t s) {
+void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* iprec, int nocc,
+                 double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s) {
   if (nact <= 0) return;
-  k_cg_prec_rho<double2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, tr2, nullptr, 0.0,
-                                              npw, ld);
+  k_cg_prec_rho<double2><<<nact, 256, 0, s>>>(act, g, P, iprec, nocc, rho_prev, conv, iter, tr2, nullptr, 0.0, npw,
+                                              ld);
 }
-void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* g2kin, const double* eprec_col,
+void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* iprec, int nocc,
                    double* rho_prev, unsigned char* conv, int iter, double eta, const double* rel, double floor,
                    int npw, long ld, cudaStream_t s) {
   if (nact <= 0) return;
-  k_cg_prec_rho<float2><<<nact, 256, 0, s>>>(act, g, P, g2kin, eprec_col, rho_prev, conv, iter, eta, rel, floor, npw,
-                                             ld);
+  k_cg_prec_rho<float2><<<nact, 256, 0, s>>>(act, g, P, iprec, nocc, rho_prev, conv, iter, eta, rel, floor, npw, ld);
 }
 
 // Active list in increasing system order (map_lbnd2ibnd, :356-382) and the
@@ -455,22 +464,21 @@ void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P
 // Otherwise the FP32 correction solve starts from d = 0 with g = -R.
 __global__ void __launch_bounds__(256) k_refine_residual(const int* __restrict__ act, const double2* __restrict__ B,
                                                          const double2* __restrict__ T,
-                                                         const double* __restrict__ g2kin,
-                                                         const double* __restrict__ eprec_col, double tr2,
+                                                         const double* __restrict__ iprec, int nocc, double tr2,
                                                          unsigned char* conv, double* rho0, float2* __restrict__ g32,
                                                          float2* __restrict__ d32, int npw, long ld) {
   __shared__ double red[16];
   const int j = act[blockIdx.x];
   const double2* bj = B + (long)j * ld;
   const double2* tj = T + (long)j * ld;
-  const double ep = eprec_col[j];
+  const double* ip = iprec + (long)(j % nocc) * npw;
   double t = 0.0, t0 = 0.0;
   for (int i = threadIdx.x; i < npw; i += 256) {
     const double2 b = bj[i], a = tj[i];
     const double rx = b.x - a.x, ry = b.y - a.y;
-    const double den = fmax(1.0, g2kin[i] / ep);
-    t = fma(rx / den, rx, fma(ry / den, ry, t));
-    if (i == 0) t0 = rx / den * rx;
+    const double w = ip[i];
+    t = fma(rx * w, rx, fma(ry * w, ry, t));
+    if (i == 0) t0 = rx * w * rx;
   }
   const double2 s = block_sum2<256>(t, t0, red);
   const double rho = 2.0 * s.x - s.y;
@@ -485,11 +493,11 @@ __global__ void __launch_bounds__(256) k_refine_residual(const int* __restrict__
     dj[i] = make_float2(0.f, 0.f);
   }
 }
-void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* g2kin,
-                     const double* eprec_col, double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32,
-                     int npw, long ld, cudaStream_t s) {
+void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* iprec, int nocc,
+                     double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32, int npw, long ld,
+                     cudaStream_t s) {
   if (nact <= 0) return;
-  k_refine_residual<<<nact, 256, 0, s>>>(act, B, T, g2kin, eprec_col, tr2, conv, rho0, g32, d32, npw, ld);
+  k_refine_residual<<<nact, 256, 0, s>>>(act, B, T, iprec, nocc, tr2, conv, rho0, g32, d32, npw, ld);
 }
 
 // x += d for the listed columns
