@@ -201,7 +201,11 @@ def run_b200(args, rank, world, local_rank):
     m = args.m
     op = ResponseOperator(s, device=local_rank, verbose=False)
     npw = s.npw
-    dvg_h = perturbations(s, m, seed=1234 + rank)
+    # one global batch of m * world perturbations, cyclically sharded over the
+    # ranks as WEST shards them over images (weak scaling: m per rank)
+    from west_b200.distribute import PertDistribution
+    dist_p = PertDistribution(m * world, world, rank)
+    dvg_h = np.asfortranarray(perturbations(s, m * world, seed=1234)[:, dist_p.local_columns()])
     dvg_d = torch.from_numpy(np.ascontiguousarray(dvg_h.T)).cuda()      # [m, npw] = Fortran [npw, m]
     dng_d = torch.zeros_like(dvg_d)
     dvg_p = torch.from_numpy(np.ascontiguousarray(dvg_h.T)).pin_memory()
