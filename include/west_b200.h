@@ -189,6 +189,20 @@ typedef struct wb_davidson_info {
 int wb_davidson(wb_ctx* ctx, const wb_davidson_params* params, const double* dvg0, int ld_dvg0, double* ev,
                 int* conv, double* pdep, int ld_pdep, wb_davidson_info* info);
 
+/*
+ * PDEP database in WEST's format: pdep_db_write (IO_kernel/pdep_db.f90:56) with
+ * pdep_merge_and_write_G (IO_kernel/pdep_io.f90:35) and pdep_db_read (pdep_db.f90:212)
+ * with pdep_read_G_and_distribute (pdep_io.f90:158).  One stream file per
+ * eigenvector, Q<iq>E<j>.dat: 32 int32 header (210405, little-endian flag,
+ * npw) then npw complex128 coefficients; summary.json with the cell
+ * (cell = a1, a2, a3 in bohr then b1, b2, b3 in bohr^-1: 18 doubles), iq, q,
+ * eigenval and eigenvec.  pdep [ld, n] complex, host memory.  Gamma only (iq = 1).
+ * Host-only: no GPU work.
+ */
+int wb_pdep_db_write(const char* dir, int iq, const double* q_cryst, const double* cell, int n_pdep_eigen,
+                     const double* ev, const double* pdep, int ld, int npw);
+int wb_pdep_db_read(const char* dir, int iq, int nglob, double* ev, double* pdep, int ld, int npw);
+
 /* Message of the last failed call in this thread ("" if none). */
 const char* wb_last_error(void);
 

@@ -9,9 +9,12 @@
 //           order).  Reads and writes of one line overlap, so a barrier
 //           separates them.
 // The small DFTs (2, 3, 4, 5 and composites up to 16) are fully unrolled
-// register code.  Twiddles W_N^j = exp(+2 pi i j / N) come from a per-N table
-// in shared memory (computed on the host); DIR = +1 is QE's invfft sign,
-// DIR = -1 the fwfft sign.  No normalisation is applied here.
+// register code.  Twiddles come from a 2N-entry table in shared memory
+// (computed on the host): entries [0, N) are W_N^j = exp(+2 pi i j / N) in
+// natural order, entries [N, 2N) hold the step-1 factors W_N^(n2 k1) at
+// N + k1 N2 + n2, so the lanes of one step read consecutive entries instead of
+// entries k1 apart (a bank conflict).  DIR = +1 is QE's invfft sign, DIR = -1
+// the fwfft sign.  No normalisation is applied here.
 #pragma once
 #include "wb_common.cuh"
 
@@ -170,7 +173,7 @@ WB_DEV void fft_step1(C* data, Off loff, int es, int nlines, const C* twN) {
                                         : p[PADDED ? LP::off_blk(n1, n2) : (N2 * n1 + n2) * es];
     rdft<N1, DIR, N>(v, twN);
 #pragma unroll
-    for (int k1 = 1; k1 < N1; ++k1) v[k1] = ctw<DIR>(v[k1], twN[(n2 * k1) % N]);
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = ctw<DIR>(v[k1], twN[N + k1 * N2 + n2]);
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) p[PADDED ? LP::off_blk(k1, n2) : (N2 * k1 + n2) * es] = v[k1];
   }

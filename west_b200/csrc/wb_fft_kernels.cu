@@ -28,9 +28,14 @@ constexpr int ZSG = 16;     // stick pairs per CTA in the z passes
 constexpr int ZNT = 256;
 constexpr int PNT = 256;
 
+// 2N-entry twiddle table: natural order, then the step-1 factors (wb_fft.cuh)
 template <int N, class C>
 WB_DEV void load_tw(C* tw, const C* twg) {
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = twg[i];
+  constexpr int N2 = FftSplit<N>::N2;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    tw[i] = twg[i];
+    tw[N + i] = twg[((i % N2) * (i / N2)) % N];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -44,7 +49,7 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld
   constexpr int LS = LinePad<N>::LEN | 1;  // odd line stride: conflict-free transposes
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
-  C* zb = tw + N;
+  C* zb = tw + 2 * N;
   const int item = blockIdx.y;
   const int q0 = blockIdx.x * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
@@ -94,7 +99,7 @@ __global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
   constexpr int LS = LinePad<N>::LEN | 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
-  C* zb = tw + N;
+  C* zb = tw + 2 * N;
   const int item = blockIdx.y;
   const int q0 = blockIdx.x * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(PNT) k_plane_vloc(C* __restrict__ sticks, Stic
                                                     const C* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
-  C* pl = tw + N;
+  C* pl = tw + 2 * N;
   const int z = blockIdx.x, item = blockIdx.y;
   C* sz = sticks + ((long)item * N + z) * st.nst;
   load_tw<N>(tw, twg);
@@ -262,7 +267,7 @@ __global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict
                                                        const double2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* tw = reinterpret_cast<double2*>(smraw);
-  double2* pl = tw + N;
+  double2* pl = tw + 2 * N;
   const int z = blockIdx.x, item = blockIdx.y;
   const double2* sz = sticks + ((long)item * N + z) * st.nst;
   load_tw<N>(tw, twg);
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ e
                                                    const double2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* tw = reinterpret_cast<double2*>(smraw);
-  double2* pl = tw + N;
+  double2* pl = tw + 2 * N;
   const int z = blockIdx.x, k = blockIdx.y, p = blockIdx.z;
   load_tw<N>(tw, twg);
   const double2* ps = evcr + ((long)k * N + z) * N * N;
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
                                                     const double2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* tw = reinterpret_cast<double2*>(smraw);
-  double2* pl = tw + N;
+  double2* pl = tw + 2 * N;
   const int z = blockIdx.x, pp = blockIdx.y;
   const int npv = (nocc + 1) / 2;
   load_tw<N>(tw, twg);
@@ -381,7 +386,7 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
   using LP = LinePad<N>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* tw = reinterpret_cast<C*>(smraw);
-  C* pl = tw + N;
+  C* pl = tw + 2 * N;
   const int z = blockIdx.x, item = blockIdx.y, tid = threadIdx.x;
   C* sz = sticks + ((long)item * N + z) * st.nst;
   C sv[MS];
@@ -426,7 +431,7 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
       for (int k2 = 0; k2 < R; ++k2) v[k2] = cscale(v[k2], vr[c][k2]);
       rdft<R, -1, N>(v, tw);                        // forward step 1 over n1 = k2, thread n2 = k1
 #pragma unroll
-      for (int q = 1; q < R; ++q) v[q] = ctw<-1>(v[q], tw[(k1 * q) % N]);
+      for (int q = 1; q < R; ++q) v[q] = ctw<-1>(v[q], tw[N + q * R + k1]);
     }
     __syncthreads();
     if (act) {
@@ -444,9 +449,9 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
 // host launchers
 // ---------------------------------------------------------------------------
 template <int N, class C = double2>
-static size_t zsmem() { return sizeof(C) * (N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
+static size_t zsmem() { return sizeof(C) * (2 * N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
 template <int N, class C = double2>
-static size_t psmem() { return sizeof(C) * (N + Plane<N>::SIZE); }
+static size_t psmem() { return sizeof(C) * (2 * N + Plane<N>::SIZE); }
 
 template <int N>
 struct FftN {

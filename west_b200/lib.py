@@ -24,8 +24,8 @@ WB_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 EXPORTS = (
     "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
     "wb_apply_operator_device_noalloc",
-    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling", "wb_davidson", "wb_last_error",
-    "wb_version",
+    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling", "wb_davidson", "wb_pdep_db_write",
+    "wb_pdep_db_read", "wb_last_error", "wb_version",
 )
 NSTAGES = 10
 STAGES = ("vloc_zinv", "vloc_plane", "vloc_zfwd", "gemm_tn", "gemm_reduce", "gemm_nn", "cg", "rhs", "drho",
@@ -90,6 +90,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.wb_get_stats.argtypes = [_p, ctypes.POINTER(WbStats)]
     lib.wb_davidson.argtypes = [_p, ctypes.POINTER(WbDavidsonParams), _p, _i, _p, _p, _p, _i,
                                 ctypes.POINTER(WbDavidsonInfo)]
+    lib.wb_pdep_db_write.argtypes = [ctypes.c_char_p, _i, _p, _p, _i, _p, _p, _i, _i]
+    lib.wb_pdep_db_read.argtypes = [ctypes.c_char_p, _i, _i, _p, _p, _i, _i]
     lib.wb_last_error.restype = ctypes.c_char_p
     lib.wb_last_error.argtypes = []
     lib.wb_version.argtypes = []
