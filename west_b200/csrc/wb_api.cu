@@ -318,14 +318,30 @@ int ensure_fp32(wb_ctx* c, int nsys, int nitems) {
     c->fa32.st = c->st;
     c->fa32.tw = c->tw32.as<float2>();
     c->fa32.stream = c->stream;
+    // the projector and Pv GEMMs on tensor cores: W split once into bf16 hi/lo tiles
+    const int Msub = c->kinetic_only ? c->nocc : c->nproj;
+    const double* Wsub = c->W.as<double>() + (c->kinetic_only ? (size_t)c->nkb * K : 0);
+    if (umma_supported(Msub)) {
+      if (c->umma_braket_w.ensure(umma_braket_bytes(Msub, K)) || c->umma_update_w.ensure(umma_update_bytes(Msub, K)) ||
+          c->umma_err.ensure(sizeof(int)))
+        return fail(WB_ERR_NOMEM, "device allocation of the bf16 projector tiles failed");
+      umma_setup();
+      umma_presplit(Wsub, K, Msub, K, c->umma_braket_w.p, c->umma_update_w.p, c->stream);
+      WB_CU(cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), c->stream));
+      WB_CU(cudaGetLastError());
+      c->umma = 1;
+      c->umma_M = Msub;
+    }
     c->have32 = 1;
   }
   const size_t vec = sizeof(float2) * (size_t)c->npw * nsys;
   const int nsplit = gemm_tn_splits32(c->nproj, nsys, K);
+  size_t part_floats = (size_t)nsplit * nsys * c->nproj;
+  if (c->umma) part_floats = std::max(part_floats, umma_part_floats(c->umma_M, nsys, K));
   bool bad = false;
   bad |= c->g32.ensure(vec) || c->P32.ensure(vec) || c->T32.ensure(vec) || c->d32.ensure(vec);
   bad |= c->sticks32.ensure(sizeof(float2) * (size_t)c->nr * c->st.nst * nitems) != 0;
-  bad |= c->part32.ensure(sizeof(float) * (size_t)nsplit * nsys * c->nproj) != 0;
+  bad |= c->part32.ensure(sizeof(float) * part_floats) != 0;
   bad |= c->C32.ensure(sizeof(float) * (size_t)nsys * c->nproj) != 0;
   bad |= c->ecol32.ensure(sizeof(float) * nsys) || c->rho0.ensure(sizeof(double) * nsys) ||
          c->rho_in.ensure(sizeof(double) * nsys) || c->conv_in.ensure(nsys + 16) ||
@@ -367,7 +383,11 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
   }
   {
     Stage g(c, WB_STAGE_GEMM_TN, 1, n);
-    gemm_tn32(W, K, M, (const float*)Pv, 2 * ld, cols, n, K, nsplit, c->part32.as<float>(), s);
+    if (c->umma)
+      nsplit = umma_braket(c->umma_braket_w.p, M, (const float*)Pv, 2 * ld, cols, n, K, c->part32.as<float>(),
+                           c->umma_err.as<int>(), s);
+    else
+      gemm_tn32(W, K, M, (const float*)Pv, 2 * ld, cols, n, K, nsplit, c->part32.as<float>(), s);
   }
   {
     Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
@@ -376,7 +396,10 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
   }
   {
     Stage g(c, WB_STAGE_GEMM_NN, 1, n);
-    gemm_nn32_acc(W, K, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, s);
+    if (c->umma)
+      umma_update(c->umma_update_w.p, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, c->umma_err.as<int>(), s);
+    else
+      gemm_nn32_acc(W, K, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, s);
   }
 }
 
@@ -451,6 +474,15 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     count_unconverged(conv, nocc, mb, c->unconv.as<int>(), s);
   }
   *iters_out = inner_total;
+  if (c->umma) {  // a bounded wait of a tensor-core GEMM that ran out leaves its code here
+    int e = 0;
+    WB_CU(cudaMemcpyAsync(&e, c->umma_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaStreamSynchronize(s));
+    if (e) {
+      cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), s);
+      return fail(WB_ERR_CUDA, "tensor-core GEMM wait limit reached (code " + std::to_string(e) + ")");
+    }
+  }
   return WB_OK;
 }
 
@@ -738,7 +770,8 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->iota_items, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
                   &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots, &c->W32, &c->D32, &c->g2kin32,
                   &c->vs32, &c->tw32, &c->g32, &c->P32, &c->T32, &c->d32, &c->sticks32, &c->part32, &c->C32,
-                  &c->ecol32, &c->rho0, &c->rho_in, &c->conv_in, &c->act_in, &c->items_in, &c->nact_in};
+                  &c->ecol32, &c->rho0, &c->rho_in, &c->conv_in, &c->act_in, &c->items_in, &c->nact_in,
+                  &c->umma_braket_w, &c->umma_update_w, &c->umma_err};
   for (DBuf* b : bufs) b->release();
   if (c->nact_host) cudaFreeHost(c->nact_host);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);

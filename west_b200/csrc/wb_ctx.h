@@ -76,6 +76,10 @@ struct wb_ctx {
   wb::FftArgs32 fa32{};
   DBuf W32, D32, g2kin32, vs32, tw32, g32, P32, T32, d32, sticks32, part32, C32, ecol32, rho0, rho_in, conv_in,
       act_in, items_in, nact_in;
+  // tensor-core GEMMs of the mixed form: W split into bf16 hi/lo tiles, and the
+  // error word their bounded waits write
+  int umma = 0, umma_M = 0;
+  DBuf umma_braket_w, umma_update_w, umma_err;
   // PDEP Davidson state (wb_davidson)
   DBuf dav_dvg, dav_dng, dav_tmp, dav_hr, dav_vr, dav_A, dav_V, dav_w, dav_part, dav_coef, dav_dots;
   int ev_get() {

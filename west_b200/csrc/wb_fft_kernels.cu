@@ -399,14 +399,7 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
   }
   const int k1 = tid % R;
   const bool rowthr = tid < LPC * R;
-  T vr[NCH][R];
   const T* vz = vs + (long)z * N * N;
-#pragma unroll
-  for (int c = 0; c < NCH; ++c) {
-    const int y = c * LPC + tid / R;
-#pragma unroll
-    for (int k2 = 0; k2 < R; ++k2) vr[c][k2] = (rowthr && y < N) ? vz[y * N + k1 + R * k2] : T(0);
-  }
   load_tw<N>(tw, twg);
   plane_zero<N, true>(pl, st);
   __syncthreads();
@@ -424,11 +417,14 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
     C* p = pl + (act ? y : 0) * Plane<N>::RS;
     C v[R];
     if (act) {
+      T vr[R];                                      // V(r) of this row, loaded here to keep registers free
+#pragma unroll
+      for (int k2 = 0; k2 < R; ++k2) vr[k2] = __ldg(vz + y * N + k1 + R * k2);
 #pragma unroll
       for (int n2 = 0; n2 < R; ++n2) v[n2] = p[LP::off_blk(k1, n2)];
       rdft<R, +1, N>(v, tw);                        // X[k1 + R k2], k2 = 0..R-1
 #pragma unroll
-      for (int k2 = 0; k2 < R; ++k2) v[k2] = cscale(v[k2], vr[c][k2]);
+      for (int k2 = 0; k2 < R; ++k2) v[k2] = cscale(v[k2], vr[k2]);
       rdft<R, -1, N>(v, tw);                        // forward step 1 over n1 = k2, thread n2 = k1
 #pragma unroll
       for (int q = 1; q < R; ++q) v[q] = ctw<-1>(v[q], tw[N + q * R + k1]);

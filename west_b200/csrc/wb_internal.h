@@ -105,4 +105,20 @@ void gamma_reduce32(const float* part, int nsplit, int M, int ncol, const float*
 void gemm_nn32_acc(const float* W, long ldw, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
                    cudaStream_t s);
 
+// split-BF16x3 tcgen05 GEMMs of the FP32 inner solve (wb_umma.cu)
+bool umma_supported(int M);
+int umma_np(int M);
+void umma_setup();
+void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split);
+size_t umma_part_floats(int M, int nsys, int K);
+size_t umma_braket_bytes(int M, int K);
+size_t umma_update_bytes(int M, int K);
+void umma_presplit(const double* W, long ldw, int M, int K, void* braket_tiles, void* update_tiles, cudaStream_t s);
+// part[s][j][r] = sum over split s of W[r][k] X[cols[j]][k]; returns the number of splits
+int umma_braket(const void* tiles, int M, const float* X, long ldx, const int* cols, int ncol, int K, float* part,
+                int* err, cudaStream_t s);
+// Y[cols[j]][k] += sum_r W[r][k] C[j][r]
+void umma_update(const void* tiles, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
+                 int* err, cudaStream_t s);
+
 }  // namespace wb
