@@ -47,6 +47,7 @@ def _args():
     ap.add_argument("--cpu-sample", type=int, default=1, help="perturbations in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pdep", action="store_true", help="skip the time-to-PDEP Davidson run")
+    ap.add_argument("--no-multi", action="store_true", help="skip the three-system uneven batch")
     return ap.parse_args()
 
 
@@ -254,6 +255,10 @@ def run_b200(args, rank, world, local_rank):
     op.apply_operator(m, dvg_d, dng_d, TR2)
     share_stats = op.stats()["stages"]
     op.set_profiling(None)
+    # the same workload with the PCG loop as one CUDA-graph launch per call (the
+    # library default; the timed region above runs eagerly so that the local-
+    # potential stage can be timed with events)
+    ms_graph = _timed_steps(op, m, dvg_d, dng_d, args, barrier, max_over_ranks)
     value = world * m * args.steps / (ms * 1e-3)
     dng_val = dng_d.cpu().numpy().T.copy()
 
@@ -287,7 +292,7 @@ def run_b200(args, rank, world, local_rank):
         achieved = per_launch_bytes / per_launch_s / 1e9
         flops = 2.0 * items * 5.0 * N ** 3 * math.log2(N ** 3)  # nominal radix-2 count, full box
         fp64_ach = flops / (t_ms * 1e-3) / 1e12
-        traffic = _profiled_traffic()
+        traffic = _profiled_traffic(items / nl)
         steps_ms = ms / args.steps
         stage_share = {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in share_stats.values())), 4)
                        for k, v in share_stats.items()}
@@ -312,6 +317,10 @@ def run_b200(args, rank, world, local_rank):
                                   "frac": fp64_ach / fp64_peak}},
             "stage_share": stage_share,
             "work": {"cg_active_sum": act_sum, "fft_boxes": boxes},
+            "graphs": {"value": world * m * args.steps / (ms_graph * 1e-3), "unit": UNIT,
+                       "ms_per_step": ms_graph / args.steps,
+                       "note": "PCG loop as one CUDA graph launch (conditional WHILE node) per call, no stage "
+                               "events; the headline value times the eager loop with the vloc stage events"},
         }
         if cpu:
             line["cpu_baseline"] = cpu
@@ -319,15 +328,7 @@ def run_b200(args, rank, world, local_rank):
             line["time_to_pdep"] = _time_to_pdep(local_rank, "fp64")
     # the mixed form on the same inputs: throughput and its dng error against FP64
     op.set_precision("mixed")
-    for _ in range(args.warmup):
-        op.apply_operator(m, dvg_d, dng_d, TR2)
-    barrier(); torch.cuda.synchronize()
-    f0 = torch.cuda.Event(enable_timing=True); f1 = torch.cuda.Event(enable_timing=True)
-    f0.record()
-    for _ in range(args.steps):
-        op.apply_operator(m, dvg_d, dng_d, TR2)
-    f1.record(); torch.cuda.synchronize()
-    ms_mixed = max_over_ranks(f0.elapsed_time(f1))
+    ms_mixed = _timed_steps(op, m, dvg_d, dng_d, args, barrier, max_over_ranks)
     st_mixed = op.stats()
     dng_mixed = dng_d.cpu().numpy().T
     err_mixed = float(np.linalg.norm(dng_mixed - dng_val) / np.linalg.norm(dng_val))
@@ -346,7 +347,73 @@ def run_b200(args, rank, world, local_rank):
                          "precision": "FP32 PCG corrections + FP32 FFTs and projector GEMMs, FP64 refinement"}
         if not args.no_pdep:
             line["mixed"]["time_to_pdep"] = _time_to_pdep(local_rank, "mixed")
+    del op
+    if rank == 0 and world == 1 and not args.no_multi:
+        try:
+            line["batched_uneven"] = _batched_uneven(local_rank, args)
+        except Exception as e:  # a failed side measurement must not lose the headline line
+            line["batched_uneven"] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
     return line
+
+
+def _timed_steps(op, m, dvg_d, dng_d, args, barrier, max_over_ranks):
+    """Warm-up then args.steps calls, CUDA events around them; ms (max over ranks)."""
+    import torch
+    for _ in range(args.warmup):
+        op.apply_operator(m, dvg_d, dng_d, TR2)
+    barrier(); torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True); f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        op.apply_operator(m, dvg_d, dng_d, TR2)
+    f1.record(); torch.cuda.synchronize()
+    return max_over_ranks(f0.elapsed_time(f1))
+
+
+def _batched_uneven(device, args):
+    """Three ground states of uneven size in one wb_apply_operator_multi call, mixed
+    form: L = 15/20/25 bohr, 48^3/64^3/80^3, nbnd_occ 8/32/64, 64/128/64
+    perturbations (256 applications per step), against the same three calls
+    made one after another."""
+    import torch
+    from west_b200.system import build_system, perturbations
+    from west_b200.wstat import ResponseOperator, apply_operator_multi
+    names, ms = ("c4a", "c4b", "c4c"), (64, 128, 64)
+    t0 = time.time()
+    systems = [build_system(n, device="cuda") for n in names]
+    t_sys = time.time() - t0
+    ops = [ResponseOperator(s, device=device, verbose=False) for s in systems]
+    for op in ops:
+        op.set_precision("mixed")
+    dvgs = [torch.from_numpy(np.ascontiguousarray(perturbations(s, m, seed=1234 + i).T)).cuda()
+            for i, (s, m) in enumerate(zip(systems, ms))]
+    dngs = [torch.zeros_like(d) for d in dvgs]
+    steps = max(1, min(args.steps, 3))
+
+    def multi():
+        apply_operator_multi(ops, dvgs, dngs, TR2)
+
+    def sequential():
+        for op, d, o, m in zip(ops, dvgs, dngs, ms):
+            op.apply_operator(m, d, o, TR2)
+
+    out = {}
+    for name, fn in (("multi", multi), ("sequential", sequential)):
+        fn()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for _ in range(steps):
+            fn()
+        torch.cuda.synchronize()
+        out[name] = (time.perf_counter() - w0) / steps
+    napp = sum(ms)
+    return {"workload": "c4 mixed: L=15/20/25 bohr, 48^3/64^3/80^3, nbnd_occ=8/32/64, m=64/128/64 "
+                        "(256 perturbations), tr2=1e-10, one wb_apply_operator_multi call per step",
+            "value": napp / out["multi"], "unit": UNIT, "ms_per_step": 1e3 * out["multi"],
+            "sequential_value": napp / out["sequential"], "speedup_vs_sequential": out["sequential"] / out["multi"],
+            "npw": [int(s.npw) for s in systems], "steps": steps, "system_build_s": round(t_sys, 1),
+            "cg_iterations": [op.stats()["cg_iterations"] for op in ops],
+            "timing": "host wall clock around the synchronous call (several library streams)"}
 
 
 def _time_to_pdep(device, precision):
@@ -391,11 +458,13 @@ def main():
             dist.destroy_process_group()
 
 
-def _profiled_traffic():
-    """DRAM bytes per launch of the vloc FFT stage from the committed ncu summary, if any."""
+def _profiled_traffic(items_per_launch):
+    """DRAM bytes per launch of the vloc FFT stage: the per-item traffic of the
+    committed 1-pass ncu capture (profiles/vloc_fft_traffic.json) times the
+    items per launch of this run; None if the summary is missing."""
     p = os.path.join(ROOT, "profiles", "vloc_fft_traffic.json")
     try:
-        return json.load(open(p))["dram_bytes_per_launch"]
+        return json.load(open(p))["dram_bytes_per_item_fp64"] * items_per_launch
     except Exception:
         return None
 

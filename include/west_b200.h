@@ -135,6 +135,44 @@ int wb_get_stats(const wb_ctx* ctx, wb_stats* out);
 int wb_set_profiling(wb_ctx* ctx, int stage_mask);
 
 /*
+ * Several ground states in one call (uneven cells, bands and batch sizes):
+ * context i maps dvg[i] [ld_dvg[i], m[i]] to dng[i] exactly as
+ * wb_apply_operator (on_device = 0: host arrays) or wb_apply_operator_device
+ * (on_device = 1) would.  No counterpart in the reference, whose images each
+ * hold one system.  The contexts run concurrently, one host thread and one
+ * CUDA stream each, their PCG loops as graph launches, so the GPU interleaves
+ * the systems' kernels and the SMs a system leaves when it converges go to
+ * the others.  unconverged[i] may be NULL.  Returns the first failure.
+ */
+int wb_apply_operator_multi(int nctx, wb_ctx* const* ctx, const int* m, const double* const* dvg, const int* ld_dvg,
+                            double* const* dng, const int* ld_dng, double tr2, int iq, int* const* unconverged,
+                            int on_device);
+
+/* Launch shapes chosen by the library's autotuner, which times the candidates
+ * on the first batch of each form (FP64, mixed) on the batch's own buffers
+ * before its PCG loop starts, then keeps them for the context. */
+typedef struct wb_tuning {
+  int autotune;              /* 1: tune on first use (default); 0: built-in shapes   */
+  int tuned_fp64;            /* 1 once the FP64 form was tuned                        */
+  int tuned_mixed;           /* 1 once the mixed form was tuned                       */
+  int dmma_ctas_per_sm;      /* FP64 bra-ket split-K target, CTAs per SM (1, 2, 4)    */
+  int tc_braket_ctas_per_sm; /* tcgen05 bra-ket split-K target, CTAs per SM (1..3)    */
+  int tc_update_systems;     /* systems per CTA of the tcgen05 update (64, 128; 0 default) */
+  int plane_fused_fp64;      /* 1: one-pass fused plane kernel in the FP64 operator   */
+  int plane_fused_mixed;     /* 1: the same in the FP32 inner operator                */
+  float tuning_ms;           /* host time spent tuning                                */
+} wb_tuning;
+int wb_get_tuning(const wb_ctx* ctx, wb_tuning* out);
+int wb_set_autotune(wb_ctx* ctx, int enable);
+
+/* CUDA graphs for the PCG loops: 1 (default) runs each batch's masked PCG
+ * loop from one graph launch whose conditional WHILE node tests convergence on
+ * the device; 0 runs it eagerly, reading the active count back to the host
+ * every iteration.  Stage profiling always runs eagerly.  Same results either
+ * way. */
+int wb_set_graphs(wb_ctx* ctx, int enable);
+
+/*
  * Allocation-free form of wb_apply_operator_device.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory while
  * they run (a host code whose GPU memory is owned by its own pool, a

@@ -35,27 +35,24 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layout_matches_header():
-    """Offsets of wb_system / wb_stats as a C compiler sees them."""
-    fields = [f for f, _ in L.WbSystem._fields_]
-    sfields = [f for f, _ in L.WbStats._fields_]
+    """Size and field offsets of every struct of the header as a C compiler sees them."""
+    structs = {"wb_system": L.WbSystem, "wb_stats": L.WbStats, "wb_davidson_params": L.WbDavidsonParams,
+               "wb_davidson_info": L.WbDavidsonInfo, "wb_tuning": L.WbTuning}
     src = "#include <stdio.h>\n#include <stddef.h>\n#include \"west_b200.h\"\nint main(){\n"
-    src += 'printf("%zu\\n", sizeof(wb_system));\n'
-    for f in fields:
-        src += f'printf("%zu\\n", offsetof(wb_system, {f}));\n'
-    src += 'printf("%zu\\n", sizeof(wb_stats));\n'
-    for f in sfields:
-        src += f'printf("%zu\\n", offsetof(wb_stats, {f}));\n'
+    expect = []
+    for cname, py in structs.items():
+        src += f'printf("%zu\\n", sizeof({cname}));\n'
+        expect.append(ctypes.sizeof(py))
+        for f, _ in py._fields_:
+            src += f'printf("%zu\\n", offsetof({cname}, {f}));\n'
+            expect.append(getattr(py, f).offset)
     src += "return 0;}\n"
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c"); exe = os.path.join(d, "t")
         open(c, "w").write(src)
         subprocess.run(["gcc", "-I", os.path.dirname(HEADER), c, "-o", exe], check=True)
         vals = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
-    assert vals[0] == ctypes.sizeof(L.WbSystem)
-    assert vals[1:1 + len(fields)] == [getattr(L.WbSystem, f).offset for f in fields]
-    k = 1 + len(fields)
-    assert vals[k] == ctypes.sizeof(L.WbStats)
-    assert vals[k + 1:] == [getattr(L.WbStats, f).offset for f in sfields]
+    assert vals == expect
 
 
 def _sys_struct(tiny, **over):
@@ -103,4 +100,8 @@ def test_null_context_calls_fail_cleanly():
     assert lib.wb_apply_operator(None, 1, None, 1, None, 1, 1e-10, 1, None) == L.WB_ERR_ARG
     assert lib.wb_set_precision(None, 0) == L.WB_ERR_ARG
     assert lib.wb_set_batch(None, 4) == L.WB_ERR_ARG
+    assert lib.wb_set_graphs(None, 1) == L.WB_ERR_ARG
+    assert lib.wb_set_autotune(None, 1) == L.WB_ERR_ARG
+    assert lib.wb_get_tuning(None, None) == L.WB_ERR_ARG
+    assert lib.wb_apply_operator_multi(1, None, None, None, None, None, None, 1e-10, 1, None, 0) == L.WB_ERR_ARG
     assert lib.wb_ctx_destroy(None) == L.WB_OK

@@ -7,12 +7,14 @@
 // convergence mask, so every system follows exactly the reference's per-band
 // iteration while the FFTs and GEMMs see thousands of columns per launch.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "wb_ctx.h"
@@ -217,12 +219,14 @@ int choose_batch(wb_ctx* c, int m) {
 }
 
 int ensure_workspace(wb_ctx* c, int mb, long ld_in, long ld_out) {
-  const size_t nsys = (size_t)mb * c->nocc;
+  const size_t nsys = (size_t)std::max(mb * c->nocc, c->cap_nsys);
+  c->cap_nsys = (int)nsys;
+  mb = (int)(nsys / c->nocc);
   const size_t vec = sizeof(double2) * (size_t)c->npw * nsys;
   const size_t stk1 = sizeof(double2) * (size_t)c->nr * c->st.nst;
   const size_t mp = (mb + 1) / 2;
   const size_t nitems = std::max<size_t>({(nsys + 1) / 2, (size_t)mb * c->npv, mp, (size_t)c->npv});
-  const int nsplit = gemm_tn_splits(c->nproj, (int)nsys, 2 * c->npw);
+  const int nsplit = gemm_tn_splits(c->nproj, (int)nsys, 2 * c->npw, 4);  // the tuner's largest target
   bool bad = false;
   bad |= c->dvg_in.ensure(sizeof(double2) * ld_in * mb + 16) != 0;
   bad |= c->dng_out.ensure(sizeof(double2) * ld_out * mb + 16) != 0;
@@ -249,17 +253,126 @@ int ensure_workspace(wb_ctx* c, int mb, long ld_in, long ld_out) {
 }
 
 // T = (H - e + alpha Pv) X on columns cols[0..n) (pairs in items), K = 2 npw.
+// ---------------------------------------------------------------------------
+// autotuner: launch shapes timed on the first batch of each form
+// ---------------------------------------------------------------------------
+template <class F>
+float time_ms(wb_ctx* c, F fn) {
+  fn();  // warm-up
+  float best = 3.4e38f;
+  for (int r = 0; r < 3; ++r) {
+    cudaEventRecord(c->tev0, c->stream);
+    fn();
+    cudaEventRecord(c->tev1, c->stream);
+    cudaEventSynchronize(c->tev1);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->tev0, c->tev1) == cudaSuccess) best = std::min(best, ms);
+  }
+  return best;
+}
+
+// FP64 form: split-K target of the DMMA bra-ket (1, 2 or 4 CTAs per SM) and
+// the one-pass fused or two-pass plane kernel, timed on this batch's still
+// unused buffers (X zeroed; sticks, part and the active list are rewritten
+// by the batch afterwards).
+int autotune64(wb_ctx* c, int nsys) {
+  if (!c->tune.on || c->tune.done64) return WB_OK;
+  c->tune.done64 = 1;
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t s = c->stream;
+  const int K = 2 * c->npw;
+  const long ld = c->npw;
+  const int M = c->kinetic_only ? c->nocc : c->nproj;
+  const double* W = c->W.as<double>() + (c->kinetic_only ? (size_t)c->nkb * K : 0);
+  WB_CU(cudaMemsetAsync(c->X.p, 0, sizeof(double2) * ld * nsys, s));
+  cg_reset(c->conv.as<unsigned char>(), nsys, s);
+  cg_compact(c->conv.as<unsigned char>(), nsys, c->act.as<int>(), c->items.as<int2>(), c->nact.as<int>(), nullptr, s);
+  float best = 3.4e38f;
+  for (int ctas : {1, 2, 4}) {
+    const int ns = gemm_tn_splits(M, nsys, K, ctas);
+    const float ms = time_ms(c, [&] {
+      gemm_tn(W, K, M, (const double*)c->X.p, 2 * ld, c->act.as<int>(), nsys, K, ns, c->part.as<double>(), s);
+    });
+    if (ms < best) { best = ms; c->tune.dmma_ctas = ctas; }
+  }
+  if (!c->kinetic_only && fft_fusable(c->nr, c->st)) {
+    FftArgs fa = c->fa;
+    const int nit = (nsys + 1) / 2;
+    fa.unfused = 0;
+    const float tf = time_ms(c, [&] { fft_plane_vloc(fa, c->sticks.as<double2>(), nit, c->vs.as<double>()); });
+    fa.unfused = 1;
+    const float tu = time_ms(c, [&] { fft_plane_vloc(fa, c->sticks.as<double2>(), nit, c->vs.as<double>()); });
+    c->tune.unfused64 = tu < tf ? 1 : 0;
+  }
+  WB_CU(cudaGetLastError());
+  c->tune.ms += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return WB_OK;
+}
+
+// Mixed form: split-K target of the tcgen05 bra-ket (1..3 CTAs per SM), systems
+// per CTA of the tcgen05 update (64 or 128) and the FP32 plane kernel variant,
+// on the FP32 buffers before the inner solves use them.
+int autotune32(wb_ctx* c, int nsys) {
+  if (!c->tune.on || c->tune.done32) return WB_OK;
+  c->tune.done32 = 1;
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t s = c->stream;
+  const int K = 2 * c->npw;
+  const long ld = c->npw;
+  WB_CU(cudaMemsetAsync(c->P32.p, 0, sizeof(float2) * ld * nsys, s));
+  WB_CU(cudaMemsetAsync(c->C32.p, 0, sizeof(float) * (size_t)nsys * c->umma_M, s));
+  cg_reset(c->conv_in.as<unsigned char>(), nsys, s);
+  cg_compact(c->conv_in.as<unsigned char>(), nsys, c->act_in.as<int>(), c->items_in.as<int2>(),
+             c->nact_in.as<int>(), nullptr, s);
+  if (c->umma) {
+    float best = 3.4e38f;
+    for (int ctas = 1; ctas <= kUmmaMaxCtas; ++ctas) {
+      const float ms = time_ms(c, [&] {
+        umma_braket(c->umma_braket_w.p, c->umma_M, (const float*)c->P32.p, 2 * ld, c->act_in.as<int>(), nsys, K,
+                    c->part32.as<float>(), c->umma_err.as<int>(), s, nullptr, ctas);
+      });
+      if (ms < best) { best = ms; c->tune.umma_ctas = ctas; }
+    }
+    best = 3.4e38f;
+    const int nrb = (umma_np(c->umma_M) + 63) / 64;
+    for (int nj : {64, 128}) {
+      if (nj == 128 && nrb > 2) continue;
+      const float ms = time_ms(c, [&] {
+        umma_update(c->umma_update_w.p, c->umma_M, c->C32.as<float>(), (float*)c->T32.p, 2 * ld, c->act_in.as<int>(),
+                    nsys, K, c->umma_err.as<int>(), s, nullptr, nj);
+      });
+      if (ms < best) { best = ms; c->tune.update_nj = nj; }
+    }
+  }
+  if (!c->kinetic_only && fft_fusable(c->nr, c->st)) {
+    FftArgs32 fa = c->fa32;
+    const int nit = (nsys + 1) / 2;
+    fa.unfused = 0;
+    const float tf = time_ms(c, [&] { fft_plane_vloc32(fa, c->sticks32.as<float2>(), nit, c->vs32.as<float>()); });
+    fa.unfused = 1;
+    const float tu = time_ms(c, [&] { fft_plane_vloc32(fa, c->sticks32.as<float2>(), nit, c->vs32.as<float>()); });
+    c->tune.unfused32 = tu < tf ? 1 : 0;
+  }
+  WB_CU(cudaGetLastError());
+  c->tune.ms += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return WB_OK;
+}
+
+// dn: device count of the listed columns (graph replays; n is then the maximum).
 void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const int2* items, int n, int nsys,
-             int nsplit) {
+             int nsplit, const int* dn = nullptr) {
   const long ld = c->npw;
   const int K = 2 * c->npw;
   cudaStream_t s = c->stream;
+  FftArgs fa = c->fa;
+  fa.dcount = dn;
+  fa.unfused = c->tune.unfused64;
   const double* W = c->W.as<double>();
   int M = c->nproj, nkb = c->nkb;
   const double* Wsub = W;
   if (c->kinetic_only) {
     Stage g(c, WB_STAGE_VLOC_ZFWD, 1, n);
-    kinetic_hpsi(Xv, Tv, c->g2kin.as<double>(), c->ecol.as<double>(), cols, n, c->npw, ld, s);
+    kinetic_hpsi(Xv, Tv, c->g2kin.as<double>(), c->ecol.as<double>(), cols, n, c->npw, ld, s, dn);
     Wsub = W + (size_t)c->nkb * K;  // alpha Pv only
     M = c->nocc;
     nkb = 0;
@@ -267,31 +380,31 @@ void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const i
     const int nit = (n + 1) / 2;
     {
       Stage g(c, WB_STAGE_VLOC_ZINV, 1, nit);
-      fft_zinv(c->fa, Xv, ld, items, nit, c->sticks.as<double2>());
+      fft_zinv(fa, Xv, ld, items, nit, c->sticks.as<double2>());
     }
     {
       Stage g(c, WB_STAGE_VLOC_PLANE, 1, nit);
-      fft_plane_vloc(c->fa, c->sticks.as<double2>(), nit, c->vs.as<double>());
+      fft_plane_vloc(fa, c->sticks.as<double2>(), nit, c->vs.as<double>());
     }
     {
       Stage g(c, WB_STAGE_VLOC_ZFWD, 1, nit);
-      fft_zfwd_hpsi(c->fa, c->sticks.as<double2>(), items, nit, Xv, Tv, ld, c->g2kin.as<double>(),
+      fft_zfwd_hpsi(fa, c->sticks.as<double2>(), items, nit, Xv, Tv, ld, c->g2kin.as<double>(),
                     c->ecol.as<double>());
     }
     c->stats.fft_boxes += 2 * nit;
   }
   {
     Stage g(c, WB_STAGE_GEMM_TN, 1, n);
-    gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s);
+    gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s, dn);
   }
   {
     Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
     gamma_reduce(c->part.as<double>(), nsplit, M, n, Wsub, K, (const double*)Xv, 2 * ld, cols, c->D.as<double>(),
-                 nkb, c->alpha, c->C.as<double>(), s);
+                 nkb, c->alpha, c->C.as<double>(), s, dn);
   }
   {
     Stage g(c, WB_STAGE_GEMM_NN, 1, n);
-    gemm_nn(Wsub, K, M, c->C.as<double>(), (double*)Tv, 2 * ld, cols, n, K, 1.0, s);
+    gemm_nn(Wsub, K, M, c->C.as<double>(), (double*)Tv, 2 * ld, cols, n, K, 1.0, s, dn);
   }
   (void)nsys;
 }
@@ -352,15 +465,19 @@ int ensure_fp32(wb_ctx* c, int nsys, int nitems) {
 }
 
 // FP32 T = (H - e + alpha Pv) P on the listed columns.
-void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const int2* items, int n, int nsplit) {
+void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const int2* items, int n, int nsplit,
+               const int* dn = nullptr) {
   const long ld = c->npw;
   const int K = 2 * c->npw;
   cudaStream_t s = c->stream;
+  FftArgs32 fa = c->fa32;
+  fa.dcount = dn;
+  fa.unfused = c->tune.unfused32;
   const float* W = c->W32.as<float>();
   int M = c->nproj, nkb = c->nkb;
   if (c->kinetic_only) {
     Stage g(c, WB_STAGE_VLOC_ZFWD, 1, n);
-    kinetic_hpsi32(Pv, Tv, c->g2kin32.as<float>(), c->ecol32.as<float>(), cols, n, c->npw, ld, s);
+    kinetic_hpsi32(Pv, Tv, c->g2kin32.as<float>(), c->ecol32.as<float>(), cols, n, c->npw, ld, s, dn);
     W += (size_t)c->nkb * K;
     M = c->nocc;
     nkb = 0;
@@ -368,15 +485,15 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
     const int nit = (n + 1) / 2;
     {
       Stage g(c, WB_STAGE_VLOC_ZINV, 1, nit);
-      fft_zinv32(c->fa32, Pv, ld, items, nit, c->sticks32.as<float2>());
+      fft_zinv32(fa, Pv, ld, items, nit, c->sticks32.as<float2>());
     }
     {
       Stage g(c, WB_STAGE_VLOC_PLANE, 1, nit);
-      fft_plane_vloc32(c->fa32, c->sticks32.as<float2>(), nit, c->vs32.as<float>());
+      fft_plane_vloc32(fa, c->sticks32.as<float2>(), nit, c->vs32.as<float>());
     }
     {
       Stage g(c, WB_STAGE_VLOC_ZFWD, 1, nit);
-      fft_zfwd_hpsi32(c->fa32, c->sticks32.as<float2>(), items, nit, Pv, Tv, ld, c->g2kin32.as<float>(),
+      fft_zfwd_hpsi32(fa, c->sticks32.as<float2>(), items, nit, Pv, Tv, ld, c->g2kin32.as<float>(),
                       c->ecol32.as<float>());
     }
     c->stats.fft_boxes += 2 * nit;
@@ -385,22 +502,82 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
     Stage g(c, WB_STAGE_GEMM_TN, 1, n);
     if (c->umma)
       nsplit = umma_braket(c->umma_braket_w.p, M, (const float*)Pv, 2 * ld, cols, n, K, c->part32.as<float>(),
-                           c->umma_err.as<int>(), s);
+                           c->umma_err.as<int>(), s, dn, c->tune.umma_ctas);
     else
-      gemm_tn32(W, K, M, (const float*)Pv, 2 * ld, cols, n, K, nsplit, c->part32.as<float>(), s);
+      gemm_tn32(W, K, M, (const float*)Pv, 2 * ld, cols, n, K, nsplit, c->part32.as<float>(), s, dn);
   }
   {
     Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
     gamma_reduce32(c->part32.as<float>(), nsplit, M, n, W, K, (const float*)Pv, 2 * ld, cols, c->D32.as<float>(), nkb,
-                   (float)c->alpha, c->C32.as<float>(), s);
+                   (float)c->alpha, c->C32.as<float>(), s, dn);
   }
   {
     Stage g(c, WB_STAGE_GEMM_NN, 1, n);
     if (c->umma)
-      umma_update(c->umma_update_w.p, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, c->umma_err.as<int>(), s);
+      umma_update(c->umma_update_w.p, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, c->umma_err.as<int>(), s,
+                  dn, c->tune.update_nj);
     else
-      gemm_nn32_acc(W, K, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, s);
+      gemm_nn32_acc(W, K, M, c->C32.as<float>(), (float*)Tv, 2 * ld, cols, n, K, s, dn);
   }
+}
+
+// ---------------------------------------------------------------------------
+// CUDA graphs of the PCG loops
+// ---------------------------------------------------------------------------
+// One masked PCG pass (prec/rho, compaction, operator, update, loop control)
+// is captured into the body of a conditional WHILE node, so the whole loop runs
+// from one graph launch with its convergence test on the device.  The kernels
+// take the active count from device memory and size their grids for the
+// workspace capacity; the graph is rebuilt when a buffer, the capacity or tr2
+// changes.  Stage profiling needs host-side events and runs the loop eagerly.
+bool graph_mode(const wb_ctx* c) { return c->use_graphs && c->prof == 0; }
+
+template <class Body>
+int capture_loop(wb_ctx* c, wb_ctx::LoopGraph& lg, std::vector<const void*> key, double tr2, Body body) {
+  if (lg.exec && lg.key == key && lg.tr2 == tr2) return WB_OK;
+  lg.release();
+  cudaGraph_t g = nullptr;
+  WB_CU(cudaGraphCreate(&g, 0));
+  lg.graph = g;
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(c->stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    lg.release();
+    return fail(WB_ERR_CUDA, std::string("graph setup of the PCG loop: ") + cudaGetErrorString(e));
+  }
+  const wb_stats saved = c->stats;
+  body(h);
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(c->stream, &captured);
+  c->stats = saved;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&lg.exec, g, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    lg.release();
+    return fail(WB_ERR_CUDA, std::string("capture of the PCG loop: ") + cudaGetErrorString(e));
+  }
+  lg.key = std::move(key);
+  lg.tr2 = tr2;
+  return WB_OK;
+}
+
+// Adds the device loop counters of a finished graph run to the call's stats.
+void loop_stats(wb_ctx* c, int passes, int launches_per_pass) {
+  const long long act = *reinterpret_cast<const long long*>(c->loop_host + 4);
+  const long long boxes = *reinterpret_cast<const long long*>(c->loop_host + 6);
+  c->stats.cg_active_sum += act;
+  c->stats.fft_boxes += c->kinetic_only ? 0 : boxes;
+  c->stats.launches += (long long)passes * launches_per_pass + 2;
 }
 
 // Solves (H - e_v + alpha Pv) x_v = b_v for all systems of the batch by FP64
@@ -412,9 +589,35 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
   cudaStream_t s = c->stream;
   const int npw = c->npw, nocc = c->nocc, nsys = mb * nocc;
   const long ld = npw;
-  int rc = ensure_fp32(c, nsys, std::max((nsys + 1) / 2, 1));
+  const int cap = std::max(c->cap_nsys, nsys);
+  int rc = ensure_fp32(c, cap, std::max((cap + 1) / 2, 1));
   if (rc) return rc;
-  const int nsplit32 = gemm_tn_splits32(c->nproj, nsys, 2 * npw);
+  rc = autotune32(c, nsys);
+  if (rc) return rc;
+  const bool graph = graph_mode(c);
+  const int nsplit32 = gemm_tn_splits32(c->nproj, graph ? cap : nsys, 2 * npw);
+  int* st = c->loopst.as<int>();
+  if (graph) {
+    // inner PCG pass on device counts, for every refinement
+    std::vector<const void*> key = {c->g32.p,   c->P32.p,    c->T32.p,   c->d32.p,    c->sticks32.p, c->act_in.p,
+                                    c->items_in.p, c->nact_in.p, c->conv_in.p, c->rho_in.p, c->rho0.p,
+                                    c->part32.p, c->C32.p,    c->ecol32.p, st,          (const void*)(intptr_t)cap};
+    const int* dn = c->nact_in.as<int>();
+    rc = capture_loop(c, c->loop32, key, tr2, [&](cudaGraphConditionalHandle h) {
+      cg_prec_rho32(c->act_in.as<int>(), cap, c->g32.as<float2>(), c->P32.as<float2>(), c->iprec.as<double>(), nocc,
+                    c->rho_in.as<double>(), c->conv_in.as<unsigned char>(), 0, kInnerRhoReduction,
+                    c->rho0.as<double>(), tr2, npw, ld, s, dn, st + 1);
+      cg_compact(c->conv_in.as<unsigned char>(), cap, c->act_in.as<int>(), c->items_in.as<int2>(),
+                 c->nact_in.as<int>(), nullptr, s, st);
+      apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), c->act_in.as<int>(), c->items_in.as<int2>(), cap,
+                nsplit32, dn);
+      cg_update32(c->act_in.as<int>(), cap, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(),
+                  c->T32.as<float2>(), npw, ld, s, dn);
+      loop_ctl(h, dn, st, c->maxiter, true, s);
+    });
+    if (rc) return rc;
+    loop_init(st, nsys, true, s);
+  }
   double2 *B = c->B.as<double2>(), *X = c->X.as<double2>(), *T = c->T.as<double2>();
   unsigned char* conv = c->conv.as<unsigned char>();
   int* act = c->act.as<int>();
@@ -434,16 +637,22 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
                       c->g32.as<float2>(), c->d32.as<float2>(), npw, ld, s);
       cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
     }
+    if (graph) WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
     WB_CU(cudaStreamSynchronize(s));
     nact = *c->nact_host;
+    if (graph) inner_total = c->loop_host[3];
     if (nact == 0 || outer == kMaxRefinements - 1) break;
     c->stats.refinements += 1;
     WB_CU(cudaMemcpyAsync(cin, conv, nsys, cudaMemcpyDeviceToDevice, s));
-    cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
+    cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), graph ? nullptr : c->nact_host, s);
     int nin = nact;
     // each refinement restarts the FP32 PCG from d = 0 on the FP64 residual;
     // the refinements share the n_dfpt_maxiter budget
-    for (int it = 1; inner_total < c->maxiter; ++it) {
+    if (graph && inner_total < c->maxiter) {
+      loop_init(st, nsys, false, s);
+      WB_CU(cudaGraphLaunch(c->loop32.exec, s));
+    }
+    for (int it = 1; !graph && inner_total < c->maxiter; ++it) {
       {
         Stage g(c, WB_STAGE_CG, 2, nin);
         // stop at rho < max(1e-10 rho_outer, tr2): the first correction from x0 is the
@@ -472,6 +681,12 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
   {
     Stage g(c, WB_STAGE_CG, 1, mb);
     count_unconverged(conv, nocc, mb, c->unconv.as<int>(), s);
+  }
+  if (graph) {
+    WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaStreamSynchronize(s));
+    inner_total = c->loop_host[3];
+    loop_stats(c, inner_total, c->kinetic_only ? 7 : 10);
   }
   *iters_out = inner_total;
   if (c->umma) {  // a bounded wait of a tensor-core GEMM that ran out leaves its code here
@@ -525,7 +740,9 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
   c->stats.fft_boxes += mp + (long long)mb * npv;
   // 4. dvpsi <- -Pc dvpsi = -dvpsi + evc (evc^T dvpsi)  (dfpt_module.f90:346)
   const double* Wevc = c->W.as<double>() + (size_t)c->nkb * K;
-  const int nsplit = gemm_tn_splits(c->nproj, nsys, K);
+  int rc0 = autotune64(c, nsys);
+  if (rc0) return rc0;
+  const int nsplit = gemm_tn_splits(c->nproj, nsys, K, c->tune.dmma_ctas);
   {
     Stage g(c, WB_STAGE_OTHER, 4, nsys);
     gemm_tn(Wevc, K, nocc, (const double*)B, 2 * ld, nullptr, nsys, K, nsplit, c->part.as<double>(), s);
@@ -555,7 +772,31 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
       sub_into(T, B, G, npw, nsys, ld, s);                       // :130-138
     }
     int nact = nsys;
-    for (int it = 1; it <= c->maxiter; ++it) {                   // :146
+    const bool graph = graph_mode(c) && c->maxiter > 0;
+    if (graph) {                                                 // :146-330 as one graph launch
+      const int cap = c->cap_nsys;
+      const int nsplit_cap = gemm_tn_splits(c->nproj, cap, K, c->tune.dmma_ctas);
+      int* st = c->loopst.as<int>();
+      const int* dn = c->nact.as<int>();
+      std::vector<const void*> key = {B, X, G, T, c->sticks.p, act, items, dn, conv, c->rho.p, c->part.p, c->C.p,
+                                      c->ecol.p, st, (const void*)(intptr_t)cap};
+      int rc = capture_loop(c, c->loop64, key, tr2, [&](cudaGraphConditionalHandle h) {
+        cg_prec_rho(act, cap, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, 0, tr2, npw, ld, s, dn,
+                    st + 1);
+        cg_compact(conv, cap, act, items, c->nact.as<int>(), nullptr, s, st);
+        apply_A(c, B, T, act, items, cap, cap, nsplit_cap, dn);
+        cg_update(act, cap, X, G, B, T, npw, ld, s, dn);
+        loop_ctl(h, dn, st, c->maxiter, false, s);
+      });
+      if (rc) return rc;
+      loop_init(st, nsys, true, s);
+      WB_CU(cudaGraphLaunch(c->loop64.exec, s));
+      WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      WB_CU(cudaStreamSynchronize(s));
+      iters = c->loop_host[2];
+      loop_stats(c, iters, c->kinetic_only ? 7 : 10);
+    }
+    for (int it = 1; !graph && it <= c->maxiter; ++it) {        // :146
       {
         Stage g(c, WB_STAGE_CG, 2, nact);
         cg_prec_rho(act, nact, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, it, tr2, npw, ld, s);
@@ -688,7 +929,9 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
   if (cudaSetDevice(device) != cudaSuccess) return bail(fail(WB_ERR_CUDA, "cudaSetDevice failed"));
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaMallocHost(&c->nact_host, sizeof(int) * 4) != cudaSuccess)
+      cudaMallocHost(&c->nact_host, sizeof(int) * 4) != cudaSuccess ||
+      cudaMallocHost(&c->loop_host, sizeof(int) * 8) != cudaSuccess || c->loopst.ensure(sizeof(int) * 8) != 0 ||
+      cudaEventCreate(&c->tev0) != cudaSuccess || cudaEventCreate(&c->tev1) != cudaSuccess)
     return bail(fail(WB_ERR_CUDA, "stream/event creation failed"));
   c->npw = s->npw;
   c->nr = s->nr1;
@@ -772,10 +1015,16 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->vs32, &c->tw32, &c->g32, &c->P32, &c->T32, &c->d32, &c->sticks32, &c->part32, &c->C32,
                   &c->ecol32, &c->rho0, &c->rho_in, &c->conv_in, &c->act_in, &c->items_in, &c->nact_in,
                   &c->umma_braket_w, &c->umma_update_w, &c->umma_err};
+  c->loop64.release();
+  c->loop32.release();
   for (DBuf* b : bufs) b->release();
+  c->loopst.release();
   if (c->nact_host) cudaFreeHost(c->nact_host);
+  if (c->loop_host) cudaFreeHost(c->loop_host);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->tev0) cudaEventDestroy(c->tev0);
+  if (c->tev1) cudaEventDestroy(c->tev1);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -809,6 +1058,57 @@ int wb_set_profiling(wb_ctx* c, int stage_mask) {
   if (!c) return fail(WB_ERR_ARG, "null context");
   if (stage_mask < 0 || stage_mask > WB_PROFILE_ALL) return fail(WB_ERR_ARG, "profiling mask out of range");
   c->prof = stage_mask;
+  return WB_OK;
+}
+
+int wb_apply_operator_multi(int nctx, wb_ctx* const* ctx, const int* m, const double* const* dvg, const int* ld_dvg,
+                            double* const* dng, const int* ld_dng, double tr2, int iq, int* const* unconverged,
+                            int on_device) {
+  g_err.clear();
+  if (nctx < 0 || (nctx > 0 && (!ctx || !m || !dvg || !ld_dvg || !dng || !ld_dng)))
+    return fail(WB_ERR_ARG, "null argument");
+  for (int i = 0; i < nctx; ++i)
+    for (int j = 0; j < i; ++j)
+      if (ctx[i] == ctx[j]) return fail(WB_ERR_ARG, "a context appears twice");
+  std::vector<int> rc(nctx, WB_OK);
+  std::vector<std::string> msg(nctx);
+  std::vector<std::thread> th;
+  th.reserve(nctx);
+  for (int i = 0; i < nctx; ++i)
+    th.emplace_back([&, i] {
+      rc[i] = apply_impl(ctx[i], m[i], dvg[i], ld_dvg[i], dng[i], ld_dng[i], tr2, iq,
+                         unconverged ? unconverged[i] : nullptr, on_device != 0);
+      msg[i] = g_err;
+    });
+  for (auto& t : th) t.join();
+  for (int i = 0; i < nctx; ++i)
+    if (rc[i] != WB_OK) return fail(rc[i], "system " + std::to_string(i) + ": " + msg[i]);
+  return WB_OK;
+}
+
+int wb_get_tuning(const wb_ctx* c, wb_tuning* out) {
+  if (!c || !out) return fail(WB_ERR_ARG, "null argument");
+  out->autotune = c->tune.on;
+  out->tuned_fp64 = c->tune.done64;
+  out->tuned_mixed = c->tune.done32;
+  out->dmma_ctas_per_sm = c->tune.dmma_ctas;
+  out->tc_braket_ctas_per_sm = c->tune.umma_ctas;
+  out->tc_update_systems = c->tune.update_nj;
+  out->plane_fused_fp64 = fft_fusable(c->nr, c->st) && !c->tune.unfused64;
+  out->plane_fused_mixed = fft_fusable(c->nr, c->st) && !c->tune.unfused32;
+  out->tuning_ms = c->tune.ms;
+  return WB_OK;
+}
+
+int wb_set_autotune(wb_ctx* c, int enable) {
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  c->tune.on = enable ? 1 : 0;
+  return WB_OK;
+}
+
+int wb_set_graphs(wb_ctx* c, int enable) {
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  c->use_graphs = enable ? 1 : 0;
   return WB_OK;
 }
 

@@ -40,6 +40,16 @@ WB_DEV C ctw(C a, C w) {
   return mkc<C>(fma(a.x, w.x, a.y * w.y), fma(a.y, w.x, -a.x * w.y));
 }
 
+// Work units of a launch: the host count, or, when dn is given (launches
+// replayed from a CUDA graph), the count an earlier kernel left in device
+// memory; PAIRS rounds half of it up (two bands per Gamma FFT).
+template <bool PAIRS = false>
+WB_DEV int dev_count(const int* dn, int host) {
+  if (!dn) return host;
+  const int n = *dn;
+  return PAIRS ? (n + 1) / 2 : n;
+}
+
 // Block-wide sum of one double per thread; result valid in every thread.
 template <int NT>
 WB_DEV double block_sum(double v, double* red /* >= NT/32 doubles */) {

@@ -76,6 +76,33 @@ struct wb_ctx {
   wb::FftArgs32 fa32{};
   DBuf W32, D32, g2kin32, vs32, tw32, g32, P32, T32, d32, sticks32, part32, C32, ecol32, rho0, rho_in, conv_in,
       act_in, items_in, nact_in;
+  // CUDA graphs of the PCG loops: one conditional WHILE node whose body is one
+  // masked PCG pass; rebuilt when a buffer, the batch or tr2 changes
+  struct LoopGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> key;
+    double tr2 = 0.0;
+    void release() {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      exec = nullptr;
+      graph = nullptr;
+      key.clear();
+    }
+  };
+  LoopGraph loop64, loop32;
+  int use_graphs = 1;
+  int cap_nsys = 0;          // systems the per-call workspace is sized for (grow-only)
+  // autotuned launch shapes (set on the first batch of each form, then fixed)
+  struct Tune {
+    int on = 1, done64 = 0, done32 = 0;
+    int dmma_ctas = 2, umma_ctas = 2, update_nj = 0, unfused64 = 0, unfused32 = 0;
+    float ms = 0.f;
+  } tune;
+  cudaEvent_t tev0 = nullptr, tev1 = nullptr;
+  DBuf loopst;               // int[8] loop state (wb_la.cu loop_init / loop_ctl)
+  int* loop_host = nullptr;  // pinned copy of it
   // tensor-core GEMMs of the mixed form: W split into bf16 hi/lo tiles, and the
   // error word their bounded waits write
   int umma = 0, umma_M = 0;

@@ -19,6 +19,9 @@
 // sticks of pair q; stick 1 (mirror slot of (0,0)) is a dummy that is never
 // scattered.  g_qz of a stored G is (2q + side, z), side = which of the two
 // sticks of the pair holds it.
+#include <algorithm>
+#include <type_traits>
+
 #include "wb_fft.cuh"
 #include "wb_internal.h"
 
@@ -41,19 +44,13 @@ WB_DEV void load_tw(C* tw, const C* twg) {
 // ---------------------------------------------------------------------------
 // z pass, inverse: sphere coefficients of a pair of columns -> sticks
 // ---------------------------------------------------------------------------
+// One unit = stick pairs [16 qg, 16 qg + 16) of band-pair item `item`.
 template <int N, bool PR, class C>
-__global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld,
-                                              const int2* __restrict__ items, StickTab st,
-                                              C* __restrict__ out,
-                                              const C* __restrict__ twg) {
+WB_DEV void zinv_unit(const C* __restrict__ src, long ld, const int2* __restrict__ items, const StickTab& st,
+                      C* __restrict__ out, const C* tw, C* zb, int qg, int item) {
   constexpr int LS = LinePad<N>::LEN | 1;  // odd line stride: conflict-free transposes
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  C* zb = tw + 2 * N;
-  const int item = blockIdx.y;
-  const int q0 = blockIdx.x * ZSG;
+  const int q0 = qg * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
-  load_tw<N>(tw, twg);
   for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = mkc<C>(0, 0);  // pads too
   __syncthreads();
   const int2 it = items[item];
@@ -89,22 +86,50 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld
   }
 }
 
+template <int N, bool PR, class C>
+__global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld,
+                                              const int2* __restrict__ items, StickTab st,
+                                              C* __restrict__ out,
+                                              const C* __restrict__ twg) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  load_tw<N>(tw, twg);
+  zinv_unit<N, PR, C>(src, ld, items, st, out, tw, tw + 2 * N, blockIdx.x, blockIdx.y);
+}
+
+// Graph replays: a fixed grid of resident CTAs strides over the units of a
+// device-side item count; the unit body is a call so that nothing is hoisted
+// across units (register pressure stays that of one unit).
+template <int N, bool PR, class C>
+__device__ __noinline__ void zinv_unit_call(const C* src, long ld, const int2* items, StickTab st, C* out,
+                                            const C* tw, C* zb, int qg, int item) {
+  zinv_unit<N, PR, C>(src, ld, items, st, out, tw, zb, qg, item);
+}
+template <int N, bool PR, class C>
+__global__ void __launch_bounds__(ZNT) k_zinv_loop(const C* __restrict__ src, long ld,
+                                                   const int2* __restrict__ items, StickTab st,
+                                                   C* __restrict__ out, const C* __restrict__ twg, const int* dn) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  load_tw<N>(tw, twg);
+  const int ngx = (st.nsp + ZSG - 1) / ZSG;
+  const int units = dev_count<true>(dn, 0) * ngx;
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    zinv_unit_call<N, PR, C>(src, ld, items, st, out, tw, tw + 2 * N, u % ngx, u / ngx);
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // z pass, forward: sticks -> sphere with the Gamma unpack, then an epilogue
 // ---------------------------------------------------------------------------
 template <int N, bool PR, class C, class Epi>
-__global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
-                                              const int2* __restrict__ items, StickTab st,
-                                              const C* __restrict__ twg, Epi epi) {
+WB_DEV void zfwd_unit(const C* __restrict__ sticks, const int2* __restrict__ items, const StickTab& st,
+                      const C* tw, C* zb, const Epi& epi, int qg, int item) {
   constexpr int LS = LinePad<N>::LEN | 1;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  C* zb = tw + 2 * N;
-  const int item = blockIdx.y;
-  const int q0 = blockIdx.x * ZSG;
+  const int q0 = qg * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
   const int ns = 2 * nq;
-  load_tw<N>(tw, twg);
   const C* s0 = sticks + (long)item * N * st.nst + 2 * q0;
   for (int e = threadIdx.x; e < ns * N; e += ZNT) {
     const int s = e % ns, z = e / ns;
@@ -131,6 +156,36 @@ __global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
     const C fp = mkc<C>(T(0.5) * (ap.x + am.x), T(0.5) * (ap.y + am.y));
     const C fm = mkc<C>(T(0.5) * (ap.x - am.x), T(0.5) * (ap.y - am.y));
     epi(g, it, mkc<C>(fp.x, fm.y), mkc<C>(fp.y, -fm.x));
+  }
+}
+
+template <int N, bool PR, class C, class Epi>
+__global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
+                                              const int2* __restrict__ items, StickTab st,
+                                              const C* __restrict__ twg, Epi epi) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  load_tw<N>(tw, twg);
+  zfwd_unit<N, PR, C, Epi>(sticks, items, st, tw, tw + 2 * N, epi, blockIdx.x, blockIdx.y);
+}
+
+template <int N, bool PR, class C, class Epi>
+__device__ __noinline__ void zfwd_unit_call(const C* sticks, const int2* items, StickTab st, const C* tw, C* zb,
+                                            Epi epi, int qg, int item) {
+  zfwd_unit<N, PR, C, Epi>(sticks, items, st, tw, zb, epi, qg, item);
+}
+template <int N, bool PR, class C, class Epi>
+__global__ void __launch_bounds__(ZNT) k_zfwd_loop(const C* __restrict__ sticks,
+                                                   const int2* __restrict__ items, StickTab st,
+                                                   const C* __restrict__ twg, Epi epi, const int* dn) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  load_tw<N>(tw, twg);
+  const int ngx = (st.nsp + ZSG - 1) / ZSG;
+  const int units = dev_count<true>(dn, 0) * ngx;
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    __syncthreads();  // twiddles, and the previous unit's reads of zb
+    zfwd_unit_call<N, PR, C, Epi>(sticks, items, st, tw, tw + 2 * N, epi, u % ngx, u / ngx);
   }
 }
 
@@ -232,17 +287,12 @@ WB_DEV void plane_fft_rows(C* pl, const C* tw) {
   fft_lines<N, DIR, PNT, false, true, P>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
 }
 
-// psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma)
+// psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma);
+// one unit = plane z of item `item`
 template <int N, bool PR, class C>
-__global__ void __launch_bounds__(PNT) k_plane_vloc(C* __restrict__ sticks, StickTab st,
-                                                    const real_t<C>* __restrict__ vs,
-                                                    const C* __restrict__ twg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  C* pl = tw + 2 * N;
-  const int z = blockIdx.x, item = blockIdx.y;
+WB_DEV void plane_vloc_unit(C* __restrict__ sticks, const StickTab& st, const real_t<C>* __restrict__ vs,
+                            const C* tw, C* pl, int z, int item) {
   C* sz = sticks + ((long)item * N + z) * st.nst;
-  load_tw<N>(tw, twg);
   plane_zero<N, PR>(pl, st);
   __syncthreads();
   plane_scatter<N>(pl, sz, st.st_pos, st.nst);
@@ -258,6 +308,35 @@ __global__ void __launch_bounds__(PNT) k_plane_vloc(C* __restrict__ sticks, Stic
   plane_fft_rows<N, -1, PR>(pl, tw);
   plane_fft_cols<N, -1, PR>(pl, st, tw);
   plane_gather<N>(pl, sz, st.st_pos, st.nst);
+}
+
+template <int N, bool PR, class C>
+__global__ void __launch_bounds__(PNT) k_plane_vloc(C* __restrict__ sticks, StickTab st,
+                                                    const real_t<C>* __restrict__ vs,
+                                                    const C* __restrict__ twg) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  load_tw<N>(tw, twg);
+  plane_vloc_unit<N, PR, C>(sticks, st, vs, tw, tw + 2 * N, blockIdx.x, blockIdx.y);
+}
+
+template <int N, bool PR, class C>
+__device__ __noinline__ void plane_vloc_unit_call(C* sticks, StickTab st, const real_t<C>* vs, const C* tw, C* pl,
+                                                  int z, int item) {
+  plane_vloc_unit<N, PR, C>(sticks, st, vs, tw, pl, z, item);
+}
+template <int N, bool PR, class C>
+__global__ void __launch_bounds__(PNT) k_plane_vloc_loop(C* __restrict__ sticks, StickTab st,
+                                                         const real_t<C>* __restrict__ vs,
+                                                         const C* __restrict__ twg, const int* dn) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  load_tw<N>(tw, twg);
+  const int units = dev_count<true>(dn, 0) * N;
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    plane_vloc_unit_call<N, PR, C>(sticks, st, vs, tw, tw + 2 * N, u % N, u / N);
+    __syncthreads();
+  }
 }
 
 // sticks -> full real-space box (complex: two real functions), no scaling
@@ -373,10 +452,10 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
 // registers before the zero fill so their latency overlaps it.
 constexpr int kFusedMaxSticksPerThread = 4;
 
-template <int N, class C>
-__global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sticks, StickTab st,
-                                                             const real_t<C>* __restrict__ vs,
-                                                             const C* __restrict__ twg) {
+// LOAD_TW: load the twiddles into tw after the stick loads are issued (one-unit kernels)
+template <int N, class C, bool LOAD_TW = false>
+WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, const real_t<C>* __restrict__ vs,
+                                  C* tw, C* pl, int z, int item, const C* __restrict__ twg = nullptr) {
   using T = real_t<C>;
   constexpr int R = FftSplit<N>::N1;
   static_assert(FftSplit<N>::N1 == FftSplit<N>::N2, "fused rows need N1 == N2");
@@ -384,10 +463,7 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
   constexpr int NCH = (N + LPC - 1) / LPC;
   constexpr int MS = kFusedMaxSticksPerThread;
   using LP = LinePad<N>;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  C* pl = tw + 2 * N;
-  const int z = blockIdx.x, item = blockIdx.y, tid = threadIdx.x;
+  const int tid = threadIdx.x;
   C* sz = sticks + ((long)item * N + z) * st.nst;
   C sv[MS];
   int sp[MS];
@@ -400,7 +476,7 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
   const int k1 = tid % R;
   const bool rowthr = tid < LPC * R;
   const T* vz = vs + (long)z * N * N;
-  load_tw<N>(tw, twg);
+  if constexpr (LOAD_TW) load_tw<N>(tw, twg);
   plane_zero<N, true>(pl, st);
   __syncthreads();
 #pragma unroll
@@ -441,13 +517,41 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
   plane_gather<N>(pl, sz, st.st_pos, st.nst);
 }
 
+template <int N, class C>
+__global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sticks, StickTab st,
+                                                             const real_t<C>* __restrict__ vs,
+                                                             const C* __restrict__ twg) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  plane_vloc_fused_unit<N, C, true>(sticks, st, vs, tw, tw + 2 * N, blockIdx.x, blockIdx.y, twg);
+}
+
+template <int N, class C>
+__device__ __noinline__ void plane_vloc_fused_unit_call(C* sticks, StickTab st, const real_t<C>* vs, C* tw,
+                                                        C* pl, int z, int item) {
+  plane_vloc_fused_unit<N, C>(sticks, st, vs, tw, pl, z, item);
+}
+template <int N, class C>
+__global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused_loop(C* __restrict__ sticks, StickTab st,
+                                                                  const real_t<C>* __restrict__ vs,
+                                                                  const C* __restrict__ twg, const int* dn) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tw = reinterpret_cast<C*>(smraw);
+  load_tw<N>(tw, twg);
+  const int units = dev_count<true>(dn, 0) * N;
+  for (int u = blockIdx.x; u < units; u += gridDim.x) {
+    plane_vloc_fused_unit_call<N, C>(sticks, st, vs, tw, tw + 2 * N, u % N, u / N);
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
 template <int N, class C = double2>
-static size_t zsmem() { return sizeof(C) * (2 * N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
+static constexpr size_t zsmem() { return sizeof(C) * (2 * N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
 template <int N, class C = double2>
-static size_t psmem() { return sizeof(C) * (2 * N + Plane<N>::SIZE); }
+static constexpr size_t psmem() { return sizeof(C) * (2 * N + Plane<N>::SIZE); }
 
 template <int N>
 struct FftN {
@@ -463,6 +567,27 @@ struct FftN {
     cudaFuncSetAttribute(k_plane_rhs<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
     cudaFuncSetAttribute(k_plane_drho<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
   }
+  // CTAs of one full wave of a loop kernel (graph replays stride over the units)
+  template <class K>
+  static int wave(K k, int threads, size_t smem) {
+    int per = 0, dev = 0, sms = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem);
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, per) * std::max(1, sms);
+  }
+  // [precision: 0 FP64, 1 FP32][prune]
+  static inline int w_zinv[2][2], w_zfwd[2][2], w_plane[2][2], w_fused[2];
+  template <bool PR, class C, class EpiH>
+  static void setup_loops(int pi) {
+    constexpr size_t zs = zsmem<N, C>(), ps = psmem<N, C>();
+    cudaFuncSetAttribute(k_zinv_loop<N, PR, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
+    cudaFuncSetAttribute(k_zfwd_loop<N, PR, C, EpiH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
+    cudaFuncSetAttribute(k_plane_vloc_loop<N, PR, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps);
+    w_zinv[pi][PR] = wave(k_zinv_loop<N, PR, C>, ZNT, zs);
+    w_zfwd[pi][PR] = wave(k_zfwd_loop<N, PR, C, EpiH>, ZNT, zs);
+    w_plane[pi][PR] = wave(k_plane_vloc_loop<N, PR, C>, PNT, ps);
+  }
   static void setup() {
     setup_pr<false>();
     setup_pr<true>();
@@ -470,6 +595,12 @@ struct FftN {
       cudaFuncSetAttribute(k_plane_vloc_fused<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
       cudaFuncSetAttribute(k_plane_vloc_fused<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)psmem<N, float2>());
+      cudaFuncSetAttribute(k_plane_vloc_fused_loop<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)psmem<N>());
+      cudaFuncSetAttribute(k_plane_vloc_fused_loop<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)psmem<N, float2>());
+      w_fused[0] = wave(k_plane_vloc_fused_loop<N, double2>, PNT, psmem<N>());
+      w_fused[1] = wave(k_plane_vloc_fused_loop<N, float2>, PNT, psmem<N, float2>());
     }
     for (int pr = 0; pr < 2; ++pr) {
       auto zi = pr ? k_zinv<N, true, float2> : k_zinv<N, false, float2>;
@@ -479,65 +610,101 @@ struct FftN {
       cudaFuncSetAttribute(zf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, float2>());
       cudaFuncSetAttribute(pv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N, float2>());
     }
+    setup_loops<false, double2, EpiHpsi>(0);
+    setup_loops<true, double2, EpiHpsi>(0);
+    setup_loops<false, float2, EpiHpsi32>(1);
+    setup_loops<true, float2, EpiHpsi32>(1);
   }
-  // FP32 local potential of the mixed-precision inner PCG
-  static void zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks) {
+  static dim3 zgrid(const StickTab& st, int nitems) { return dim3((st.nsp + ZSG - 1) / ZSG, nitems); }
+  static bool fused(const StickTab& st) {
+    if constexpr (FUSABLE) return st.prune && st.nst <= kFusedMaxSticksPerThread * PNT;
+    return false;
+  }
+  template <class F>
+  static bool use_fused(const F& f) { return !f.unfused && fused(f.st); }
+  // Local-potential transforms of the PCG operator, FP64 (C = double2) or the
+  // FP32 inner solves (C = float2).  A host count launches one CTA per unit; a
+  // device count (graph replays) launches one wave of the loop kernels.
+  template <class C, class F>
+  static void zinv_t(const F& f, const C* src, long ld, const int2* items, int nitems, C* sticks) {
     if (nitems <= 0) return;
+    constexpr int pi = sizeof(C) == 8 ? 1 : 0;
+    constexpr size_t zs = zsmem<N, C>();
+    if (f.dcount) {
+      if (f.st.prune)
+        k_zinv_loop<N, true, C><<<w_zinv[pi][1], ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw, f.dcount);
+      else
+        k_zinv_loop<N, false, C><<<w_zinv[pi][0], ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw, f.dcount);
+      return;
+    }
     if (f.st.prune)
-      k_zinv<N, true, float2><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(src, ld, items, f.st,
-                                                                                         sticks, f.tw);
+      k_zinv<N, true, C><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw);
     else
-      k_zinv<N, false, float2><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(src, ld, items, f.st,
-                                                                                          sticks, f.tw);
+      k_zinv<N, false, C><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw);
   }
-  static void vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs) {
+  template <class C, class F>
+  static void vloc_t(const F& f, C* sticks, int nitems, const real_t<C>* vs) {
     if (nitems <= 0) return;
+    constexpr int pi = sizeof(C) == 8 ? 1 : 0;
+    constexpr size_t ps = psmem<N, C>();
     const dim3 g(N, nitems);
     if constexpr (FUSABLE) {
-      if (f.st.prune && f.st.nst <= kFusedMaxSticksPerThread * PNT) {
-        k_plane_vloc_fused<N, float2><<<g, PNT, psmem<N, float2>(), f.stream>>>(sticks, f.st, vs, f.tw);
+      if (use_fused(f)) {
+        if (f.dcount)
+          k_plane_vloc_fused_loop<N, C><<<w_fused[pi], PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+        else
+          k_plane_vloc_fused<N, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw);
         return;
       }
     }
-    if (f.st.prune) k_plane_vloc<N, true, float2><<<g, PNT, psmem<N, float2>(), f.stream>>>(sticks, f.st, vs, f.tw);
-    else k_plane_vloc<N, false, float2><<<g, PNT, psmem<N, float2>(), f.stream>>>(sticks, f.st, vs, f.tw);
+    if (f.dcount) {
+      if (f.st.prune)
+        k_plane_vloc_loop<N, true, C><<<w_plane[pi][1], PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+      else
+        k_plane_vloc_loop<N, false, C><<<w_plane[pi][0], PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+      return;
+    }
+    if (f.st.prune) k_plane_vloc<N, true, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw);
+    else k_plane_vloc<N, false, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw);
+  }
+  template <class C, class F, class Epi>
+  static void zfwd_t(const F& f, const C* sticks, const int2* items, int nitems, Epi epi) {
+    if (nitems <= 0) return;
+    constexpr int pi = sizeof(C) == 8 ? 1 : 0;
+    constexpr size_t zs = zsmem<N, C>();
+    if constexpr (std::is_same<Epi, EpiHpsi>::value || std::is_same<Epi, EpiHpsi32>::value) {
+      if (f.dcount) {
+        if (f.st.prune)
+          k_zfwd_loop<N, true, C, Epi><<<w_zfwd[pi][1], ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi, f.dcount);
+        else
+          k_zfwd_loop<N, false, C, Epi><<<w_zfwd[pi][0], ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi,
+                                                                             f.dcount);
+        return;
+      }
+    }
+    if (f.st.prune)
+      k_zfwd<N, true, C, Epi><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi);
+    else
+      k_zfwd<N, false, C, Epi><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi);
+  }
+  static void zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks) {
+    zinv_t<float2>(f, src, ld, items, nitems, sticks);
+  }
+  static void vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs) {
+    vloc_t<float2>(f, sticks, nitems, vs);
   }
   static void zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, EpiHpsi32 epi) {
-    if (nitems <= 0) return;
-    if (f.st.prune)
-      k_zfwd<N, true, float2, EpiHpsi32><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(
-          sticks, items, f.st, f.tw, epi);
-    else
-      k_zfwd<N, false, float2, EpiHpsi32><<<zgrid(f.st, nitems), ZNT, zsmem<N, float2>(), f.stream>>>(
-          sticks, items, f.st, f.tw, epi);
+    zfwd_t<float2>(f, sticks, items, nitems, epi);
   }
-  static dim3 zgrid(const StickTab& st, int nitems) { return dim3((st.nsp + ZSG - 1) / ZSG, nitems); }
   static void zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks) {
-    if (nitems <= 0) return;
-    if (f.st.prune)
-      k_zinv<N, true, double2><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
-    else
-      k_zinv<N, false, double2><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+    zinv_t<double2>(f, src, ld, items, nitems, sticks);
   }
   template <class Epi>
   static void zfwd(const FftArgs& f, const double2* sticks, const int2* items, int nitems, Epi epi) {
-    if (nitems <= 0) return;
-    if (f.st.prune)
-      k_zfwd<N, true, double2, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
-    else
-      k_zfwd<N, false, double2, Epi><<<zgrid(f.st, nitems), ZNT, zsmem<N>(), f.stream>>>(sticks, items, f.st, f.tw, epi);
+    zfwd_t<double2>(f, sticks, items, nitems, epi);
   }
   static void vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs) {
-    if (nitems <= 0) return;
-    const dim3 g(N, nitems);
-    if constexpr (FUSABLE) {
-      if (f.st.prune && f.st.nst <= kFusedMaxSticksPerThread * PNT) {
-        k_plane_vloc_fused<N, double2><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
-        return;
-      }
-    }
-    if (f.st.prune) k_plane_vloc<N, true, double2><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
-    else k_plane_vloc<N, false, double2><<<g, PNT, psmem<N>(), f.stream>>>(sticks, f.st, vs, f.tw);
+    vloc_t<double2>(f, sticks, nitems, vs);
   }
   static void inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box) {
     if (nitems <= 0) return;
@@ -567,6 +734,15 @@ struct FftN {
 };
 
 #define WB_FOR_EACH_N(X) X(16) X(20) X(24) X(32) X(36) X(40) X(48) X(60) X(64) X(72) X(80) X(96) X(100) X(108)
+
+bool fft_fusable(int n, const StickTab& st) {
+  switch (n) {
+#define X(n) case n: return FftN<n>::fused(st);
+    WB_FOR_EACH_N(X)
+#undef X
+    default: return false;
+  }
+}
 
 bool fft_supported(int n) {
   switch (n) {

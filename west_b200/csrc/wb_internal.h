@@ -16,11 +16,16 @@ struct StickTab {
   int prune;             // 1 if every |Miller index| < N/4 (sphere inside the outer quarters)
 };
 
+// Launches that take a device count (dcount != nullptr, CUDA-graph replays)
+// size their grid for the host count as a maximum and read the number of
+// systems from *dcount; items are pairs of systems.
 struct FftArgs {
   int n;                 // box edge
   StickTab st;
   const double2* tw;     // [n] exp(+2 pi i j / n)
   cudaStream_t stream;
+  const int* dcount = nullptr;
+  int unfused = 0;       // 1: the two-pass plane kernel even where the fused one applies
 };
 
 // FP32 twin of FftArgs for the mixed-precision inner solves.
@@ -29,9 +34,13 @@ struct FftArgs32 {
   StickTab st;
   const float2* tw;
   cudaStream_t stream;
+  const int* dcount = nullptr;
+  int unfused = 0;
 };
 
 bool fft_supported(int n);
+// the fused one-pass plane kernel applies to this box and stick table
+bool fft_fusable(int n, const StickTab& st);
 void fft_zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks);
 void fft_plane_vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs);
 void fft_zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, const float2* P,
@@ -51,16 +60,18 @@ void fft_plane_drho(const FftArgs& f, const double2* dsticks, const double2* evc
 
 // ---- dense kernels (wb_la.cu) ----
 // part[s][j][r] = sum_{k in split s} W[r*ldw + k] * X[col(j)*ldx + k]
-int gemm_tn_splits(int M, int ncol, int K);
+// split count of the DMMA bra-ket: about 2 * 148 * ctas_per_sm CTAs (4 warps each)
+int gemm_tn_splits(int M, int ncol, int K, int ctas_per_sm = 2);
 void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
-             int nsplit, double* part, cudaStream_t s);
+             int nsplit, double* part, cudaStream_t s, const int* dn = nullptr);
 // S = 2 sum_s part - W0 X0 (Gamma bra-ket, glbrak.f90:39-40), then
 // C[j][r] = sum_{r'<nkb} D[r][r'] S[j][r'] for r < nkb, alpha S[j][r] otherwise
 void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double* W, long ldw, const double* X,
-                  long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s);
+                  long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s,
+                  const int* dn = nullptr);
 // Y[col(j)] = beta Y[col(j)] + W C[j]  over K real rows
 void gemm_nn(const double* W, long ldw, int M, const double* C, double* Y, long ldy, const int* cols, int ncol,
-             int K, double beta, cudaStream_t s);
+             int K, double beta, cudaStream_t s, const int* dn = nullptr);
 
 void permute_scale(const double2* dvg, long ld_in, const int* perm, const double* sqvc, int npw, int m,
                    double2* aux, long ld_out, cudaStream_t s);
@@ -71,54 +82,63 @@ void precondition(const double2* f, double2* pf, const double* iprec, int nocc, 
                   cudaStream_t s);
 void sub_into(const double2* a, const double2* b, double2* out, int npw, int ncol, long ld, cudaStream_t s);
 void kinetic_hpsi(const double2* P, double2* T, const double* g2kin, const double* ecol, const int* cols, int ncol,
-                  int npw, long ld, cudaStream_t s);
+                  int npw, long ld, cudaStream_t s, const int* dn = nullptr);
 void set_eprec(const double2* evc, const double* g2kin, int npw, int nocc, double* eprec, cudaStream_t s);
 void fill_columns(const double* per_band, int nocc, int nsys, double* out, cudaStream_t s);
 void cg_reset(unsigned char* conv, int nsys, cudaStream_t s);
 void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* iprec, int nocc,
-                 double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s);
+                 double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s,
+                 const int* dn = nullptr, const int* iter_dev = nullptr);
+// nact_host may be null (no host copy); nsys_dev, if given, overrides nsys
 void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int* nact_dev, int* nact_host,
-                cudaStream_t s);
+                cudaStream_t s, const int* nsys_dev = nullptr);
 void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
-               long ld, cudaStream_t s);
+               long ld, cudaStream_t s, const int* dn = nullptr);
 void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cudaStream_t s);
+// loop state of the graph-captured PCG loops: int st[8] (wb_la.cu)
+void loop_init(int* st, int nsys, bool reset_totals, cudaStream_t s);
+void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool shared_budget, cudaStream_t s);
 
 // ---- mixed form: FP32 inner PCG and FP64 refinement (wb_la.cu) ----
 // inner test: rho < max(eta * rel[j], floor)
 void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* iprec, int nocc,
                    double* rho_prev, unsigned char* conv, int iter, double eta, const double* rel, double floor,
-                   int npw, long ld, cudaStream_t s);
+                   int npw, long ld, cudaStream_t s, const int* dn = nullptr, const int* iter_dev = nullptr);
 void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
-                 cudaStream_t s);
+                 cudaStream_t s, const int* dn = nullptr);
 void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* iprec, int nocc,
                      double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32, int npw, long ld,
                      cudaStream_t s);
 void refine_accumulate(const int* act, int nact, double2* X, const float2* d32, int npw, long ld, cudaStream_t s);
 void kinetic_hpsi32(const float2* P, float2* T, const float* g2kin, const float* ecol, const int* cols, int ncol,
-                    int npw, long ld, cudaStream_t s);
+                    int npw, long ld, cudaStream_t s, const int* dn = nullptr);
 void to_float(const double* a, float* b, long n, cudaStream_t s);
 int gemm_tn_splits32(int M, int ncol, int K);
 void gemm_tn32(const float* W, long ldw, int M, const float* X, long ldx, const int* cols, int ncol, int K, int nsplit,
-               float* part, cudaStream_t s);
+               float* part, cudaStream_t s, const int* dn = nullptr);
 void gamma_reduce32(const float* part, int nsplit, int M, int ncol, const float* W, long ldw, const float* X, long ldx,
-                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s);
+                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s,
+                    const int* dn = nullptr);
 void gemm_nn32_acc(const float* W, long ldw, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
-                   cudaStream_t s);
+                   cudaStream_t s, const int* dn = nullptr);
 
 // split-BF16x3 tcgen05 GEMMs of the FP32 inner solve (wb_umma.cu)
 bool umma_supported(int M);
 int umma_np(int M);
 void umma_setup();
-void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split);
+void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split, int ctas_per_sm = 2);
+// part floats for any batch up to nsys and any ctas_per_sm up to kUmmaMaxCtas
+constexpr int kUmmaMaxCtas = 3;
 size_t umma_part_floats(int M, int nsys, int K);
 size_t umma_braket_bytes(int M, int K);
 size_t umma_update_bytes(int M, int K);
 void umma_presplit(const double* W, long ldw, int M, int K, void* braket_tiles, void* update_tiles, cudaStream_t s);
 // part[s][j][r] = sum over split s of W[r][k] X[cols[j]][k]; returns the number of splits
 int umma_braket(const void* tiles, int M, const float* X, long ldx, const int* cols, int ncol, int K, float* part,
-                int* err, cudaStream_t s);
+                int* err, cudaStream_t s, const int* dn = nullptr, int ctas_per_sm = 2);
 // Y[cols[j]][k] += sum_r W[r][k] C[j][r]
+// nj: systems per CTA (64 or 128; 0 = by projector count)
 void umma_update(const void* tiles, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
-                 int* err, cudaStream_t s);
+                 int* err, cudaStream_t s, const int* dn = nullptr, int nj = 0);
 
 }  // namespace wb

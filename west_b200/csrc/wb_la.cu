@@ -28,12 +28,14 @@ constexpr int TN_W = 4;
 
 __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict__ W, long ldw, int M,
                                                        const double* __restrict__ X, long ldx,
-                                                       const int* __restrict__ cols, int ncol, int K, int kchunk,
-                                                       double* __restrict__ part) {
+                                                       const int* __restrict__ cols, int ncol_host, const int* dn,
+                                                       int K, int kchunk, double* __restrict__ part) {
   __shared__ double red[TN_W][TN_T * TN_T];
+  const int ncol = dev_count(dn, ncol_host);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lr = lane >> 2, lk = lane & 3;
   const int r0 = blockIdx.x * TN_T, j0 = blockIdx.y * TN_T, split = blockIdx.z;
+  if (j0 >= ncol) return;
   const int kb = split * kchunk, ke = min(K, kb + kchunk);
   const double* arow[4];
   bool aok[4];
@@ -85,9 +87,9 @@ __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict_
   }
 }
 
-int gemm_tn_splits(int M, int ncol, int K) {
+int gemm_tn_splits(int M, int ncol, int K, int ctas_per_sm) {
   const int tiles = ((M + TN_T - 1) / TN_T) * ((ncol + TN_T - 1) / TN_T);
-  int ns = (2 * 148 * 2 + tiles - 1) / tiles;
+  int ns = (2 * 148 * ctas_per_sm + tiles - 1) / tiles;
   const int maxs = (K + 511) / 512;
   if (ns > maxs) ns = maxs;
   if (ns < 1) ns = 1;
@@ -95,21 +97,23 @@ int gemm_tn_splits(int M, int ncol, int K) {
 }
 
 void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
-             int nsplit, double* part, cudaStream_t s) {
+             int nsplit, double* part, cudaStream_t s, const int* dn) {
   if (ncol <= 0 || M <= 0) return;
   int kchunk = (K + nsplit - 1) / nsplit;
   kchunk = (kchunk + 15) / 16 * 16;
   dim3 grid((M + TN_T - 1) / TN_T, (ncol + TN_T - 1) / TN_T, nsplit);
-  k_gemm_tn<<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, K, kchunk, part);
+  k_gemm_tn<<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, dn, K, kchunk, part);
 }
 
-__global__ void __launch_bounds__(256) k_gamma_reduce(const double* __restrict__ part, int nsplit, int M, int ncol,
-                                                      const double* __restrict__ W, long ldw,
-                                                      const double* __restrict__ X, long ldx,
+__global__ void __launch_bounds__(256) k_gamma_reduce(const double* __restrict__ part, int nsplit, int M,
+                                                      int ncol_host, const int* dn, const double* __restrict__ W,
+                                                      long ldw, const double* __restrict__ X, long ldx,
                                                       const int* __restrict__ cols, const double* __restrict__ D,
                                                       int nkb, double alpha, double* __restrict__ C) {
   extern __shared__ double S[];
+  const int ncol = dev_count(dn, ncol_host);
   const int j = blockIdx.x;
+  if (j >= ncol) return;
   const int col = cols ? cols[j] : j;
   const double x0 = X[(long)col * ldx];
   for (int r = threadIdx.x; r < M; r += blockDim.x) {
@@ -131,10 +135,11 @@ __global__ void __launch_bounds__(256) k_gamma_reduce(const double* __restrict__
 }
 
 void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double* W, long ldw, const double* X,
-                  long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s) {
+                  long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s,
+                  const int* dn) {
   if (ncol <= 0 || M <= 0) return;
-  k_gamma_reduce<<<ncol, 256, sizeof(double) * M, s>>>(part, nsplit, M, ncol, W, ldw, X, ldx, cols, D, nkb, alpha,
-                                                        C);
+  k_gamma_reduce<<<ncol, 256, sizeof(double) * M, s>>>(part, nsplit, M, ncol, dn, W, ldw, X, ldx, cols, D, nkb,
+                                                        alpha, C);
 }
 
 // ---------------------------------------------------------------------------
@@ -143,10 +148,13 @@ void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double*
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_gemm_nn(const double* __restrict__ W, long ldw, int M,
                                                  const double* __restrict__ C, double* __restrict__ Y, long ldy,
-                                                 const int* __restrict__ cols, int ncol, int K, double beta) {
+                                                 const int* __restrict__ cols, int ncol_host, const int* dn, int K,
+                                                 double beta) {
+  const int ncol = dev_count(dn, ncol_host);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lr = lane >> 2, lk = lane & 3;
   const int k0 = blockIdx.x * 128 + warp * 32, j0 = blockIdx.y * 32;
+  if (j0 >= ncol) return;
   bool kok[4], jok[4];
   const double* crow[4];
 #pragma unroll
@@ -194,10 +202,10 @@ __global__ void __launch_bounds__(128) k_gemm_nn(const double* __restrict__ W, l
 }
 
 void gemm_nn(const double* W, long ldw, int M, const double* C, double* Y, long ldy, const int* cols, int ncol,
-             int K, double beta, cudaStream_t s) {
+             int K, double beta, cudaStream_t s, const int* dn) {
   if (ncol <= 0 || M <= 0) return;
   dim3 grid((K + 127) / 128, (ncol + 31) / 32);
-  k_gemm_nn<<<grid, 128, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, K, beta);
+  k_gemm_nn<<<grid, 128, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, dn, K, beta);
 }
 
 // ---------------------------------------------------------------------------
@@ -260,7 +268,8 @@ void sub_into(const double2* a, const double2* b, double2* out, int npw, int nco
 // apply_sternheimerop_to_m_wfcs.f90)
 __global__ void k_kinetic_hpsi(const double2* __restrict__ P, double2* __restrict__ T,
                                const double* __restrict__ g2kin, const double* __restrict__ ecol,
-                               const int* __restrict__ cols, int npw, long ld) {
+                               const int* __restrict__ cols, const int* dn, int npw, long ld) {
+  if ((int)blockIdx.y >= dev_count(dn, gridDim.y)) return;
   const int c = cols ? cols[blockIdx.y] : blockIdx.y;
   const double e = ecol[c];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
@@ -271,9 +280,9 @@ __global__ void k_kinetic_hpsi(const double2* __restrict__ P, double2* __restric
   }
 }
 void kinetic_hpsi(const double2* P, double2* T, const double* g2kin, const double* ecol, const int* cols, int ncol,
-                  int npw, long ld, cudaStream_t s) {
+                  int npw, long ld, cudaStream_t s, const int* dn) {
   if (ncol <= 0) return;
-  k_kinetic_hpsi<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(P, T, g2kin, ecol, cols, npw, ld);
+  k_kinetic_hpsi<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(P, T, g2kin, ecol, cols, dn, npw, ld);
 }
 
 // eprec_v = 1.35 sum_G |psi_v(G)|^2 g2kin(G)       (set_eprec.f90:40-53)
@@ -315,66 +324,77 @@ void cg_reset(unsigned char* conv, int nsys, cudaStream_t s) {
 // P = -h + (rho / rho_prev) P  (P = -h at the first iteration).  C is the
 // vector type (double2, or float2 in the mixed form); scalars are FP64.
 template <class C>
-__global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act, const C* __restrict__ g,
+__global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act, const int* dn, const C* __restrict__ g,
                                                      C* __restrict__ P, const double* __restrict__ iprec, int nocc,
-                                                     double* rho_prev,
-                                                     unsigned char* conv, int iter, double tr2,
-                                                     const double* __restrict__ rel, double floor, int npw, long ld) {
+                                                     double* rho_prev, unsigned char* conv, int iter_host,
+                                                     const int* iter_dev, double tr2, const double* __restrict__ rel,
+                                                     double floor, int npw, long ld) {
   using T = real_t<C>;
   __shared__ double red[16];
-  const int j = act[blockIdx.x];
-  const C* gj = g + (long)j * ld;
-  C* pj = P + (long)j * ld;
-  const double* ip = iprec + (long)(j % nocc) * npw;
-  double t = 0.0, t0 = 0.0;
-  for (int i = threadIdx.x; i < npw; i += 256) {
-    const double w = ip[i];
-    const C gv = gj[i];
-    const double hx = (double)gv.x * w, hy = (double)gv.y * w;
-    t = fma(hx, (double)gv.x, fma(hy, (double)gv.y, t));
-    if (i == 0) t0 = hx * (double)gv.x;
-  }
-  const double2 s = block_sum2<256>(t, t0, red);
-  const double rho = 2.0 * s.x - s.y;
-  const double thr = rel ? fmax(tr2 * rel[j], floor) : tr2;
-  const bool c = rho < thr;
-  if (c) {
-    if (threadIdx.x == 0) conv[j] = 1;
-    return;
-  }
-  const double beta = (iter == 1) ? 0.0 : rho / rho_prev[j];
-  __syncthreads();
-  if (threadIdx.x == 0) rho_prev[j] = rho;
-  for (int i = threadIdx.x; i < npw; i += 256) {
-    const double w = ip[i];
-    const C gv = gj[i];
-    const double hx = (double)gv.x * w, hy = (double)gv.y * w;
-    if (iter == 1) {
-      pj[i] = mkc<C>(T(-hx), T(-hy));
-    } else {
-      const C pv = pj[i];
-      pj[i] = mkc<C>(T(fma(beta, (double)pv.x, -hx)), T(fma(beta, (double)pv.y, -hy)));
+  const int n = dev_count(dn, gridDim.x);
+  const int iter = iter_dev ? *iter_dev : iter_host;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const int j = act[b];
+    const C* gj = g + (long)j * ld;
+    C* pj = P + (long)j * ld;
+    const double* ip = iprec + (long)(j % nocc) * npw;
+    double t = 0.0, t0 = 0.0;
+    for (int i = threadIdx.x; i < npw; i += 256) {
+      const double w = ip[i];
+      const C gv = gj[i];
+      const double hx = (double)gv.x * w, hy = (double)gv.y * w;
+      t = fma(hx, (double)gv.x, fma(hy, (double)gv.y, t));
+      if (i == 0) t0 = hx * (double)gv.x;
+    }
+    const double2 s = block_sum2<256>(t, t0, red);
+    const double rho = 2.0 * s.x - s.y;
+    const double thr = rel ? fmax(tr2 * rel[j], floor) : tr2;
+    if (rho < thr) {  // block-uniform
+      if (threadIdx.x == 0) conv[j] = 1;
+      continue;
+    }
+    const double beta = (iter == 1) ? 0.0 : rho / rho_prev[j];
+    __syncthreads();
+    if (threadIdx.x == 0) rho_prev[j] = rho;
+    for (int i = threadIdx.x; i < npw; i += 256) {
+      const double w = ip[i];
+      const C gv = gj[i];
+      const double hx = (double)gv.x * w, hy = (double)gv.y * w;
+      if (iter == 1) {
+        pj[i] = mkc<C>(T(-hx), T(-hy));
+      } else {
+        const C pv = pj[i];
+        pj[i] = mkc<C>(T(fma(beta, (double)pv.x, -hx)), T(fma(beta, (double)pv.y, -hy)));
+      }
     }
   }
 }
+
+// Grid of a per-system launch: one CTA per system, or, with a device count,
+// a fixed grid that strides over the systems.
+static int sys_grid(int nmax, const int* dn) { return dn ? std::min(nmax, 4 * 148) : nmax; }
+
 void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* iprec, int nocc,
-                 double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s) {
+                 double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s,
+                 const int* dn, const int* iter_dev) {
   if (nact <= 0) return;
-  k_cg_prec_rho<double2><<<nact, 256, 0, s>>>(act, g, P, iprec, nocc, rho_prev, conv, iter, tr2, nullptr, 0.0, npw,
-                                              ld);
+  k_cg_prec_rho<double2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, g, P, iprec, nocc, rho_prev, conv, iter, iter_dev,
+                                                           tr2, nullptr, 0.0, npw, ld);
 }
 void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* iprec, int nocc,
                    double* rho_prev, unsigned char* conv, int iter, double eta, const double* rel, double floor,
-                   int npw, long ld, cudaStream_t s) {
+                   int npw, long ld, cudaStream_t s, const int* dn, const int* iter_dev) {
   if (nact <= 0) return;
-  k_cg_prec_rho<float2><<<nact, 256, 0, s>>>(act, g, P, iprec, nocc, rho_prev, conv, iter, eta, rel, floor, npw, ld);
+  k_cg_prec_rho<float2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, g, P, iprec, nocc, rho_prev, conv, iter, iter_dev,
+                                                          eta, rel, floor, npw, ld);
 }
 
 // Active list in increasing system order (map_lbnd2ibnd, :356-382) and the
 // Gamma FFT pairs (act[2k], act[2k+1]).
-__global__ void __launch_bounds__(1024) k_cg_compact(const unsigned char* __restrict__ conv, int nsys,
-                                                     int* __restrict__ act, int2* __restrict__ items,
-                                                     int* __restrict__ nact_out) {
+__global__ void __launch_bounds__(1024) k_cg_compact(const unsigned char* __restrict__ conv, int nsys_host,
+                                                     const int* nsys_dev, int* __restrict__ act,
+                                                     int2* __restrict__ items, int* __restrict__ nact_out) {
+  const int nsys = dev_count(nsys_dev, nsys_host);
   __shared__ int wsum[32];
   __shared__ int base;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -409,51 +429,54 @@ __global__ void __launch_bounds__(1024) k_cg_compact(const unsigned char* __rest
   if (tid == 0) *nact_out = n;
 }
 void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int* nact_dev, int* nact_host,
-                cudaStream_t s) {
-  k_cg_compact<<<1, 1024, 0, s>>>(conv, nsys, act, items, nact_dev);
-  cudaMemcpyAsync(nact_host, nact_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+                cudaStream_t s, const int* nsys_dev) {
+  k_cg_compact<<<1, 1024, 0, s>>>(conv, nsys, nsys_dev, act, items, nact_dev);
+  if (nact_host) cudaMemcpyAsync(nact_host, nact_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
 }
 
 // a = <P|g>, c = <P|T> (Gamma); x -= (a/c) P ; g -= (a/c) T     (:253-322)
 template <class C>
-__global__ void __launch_bounds__(256) k_cg_update(const int* __restrict__ act, C* __restrict__ x,
+__global__ void __launch_bounds__(256) k_cg_update(const int* __restrict__ act, const int* dn, C* __restrict__ x,
                                                    C* __restrict__ g, const C* __restrict__ P,
                                                    const C* __restrict__ T, int npw, long ld) {
   using R = real_t<C>;
   __shared__ double red[16];
-  const int j = act[blockIdx.x];
-  const C* pj = P + (long)j * ld;
-  const C* tj = T + (long)j * ld;
-  C* gj = g + (long)j * ld;
-  C* xj = x + (long)j * ld;
-  double a = 0.0, c = 0.0;
-  for (int i = threadIdx.x; i < npw; i += 256) {
-    const C p = pj[i], gv = gj[i], t = tj[i];
-    double da = fma((double)p.x, (double)gv.x, (double)p.y * (double)gv.y);
-    double dc = fma((double)p.x, (double)t.x, (double)p.y * (double)t.y);
-    if (i == 0) { da -= 0.5 * (double)p.x * (double)gv.x; dc -= 0.5 * (double)p.x * (double)t.x; }
-    a += da;
-    c += dc;
-  }
-  const double2 s = block_sum2<256>(a, c, red);
-  const double rd = (2.0 * s.x) / (2.0 * s.y);
-  const R r = R(rd);
-  for (int i = threadIdx.x; i < npw; i += 256) {
-    const C p = pj[i], t = tj[i];
-    C xv = xj[i], gv = gj[i];
-    xj[i] = mkc<C>(fma(-r, p.x, xv.x), fma(-r, p.y, xv.y));
-    gj[i] = mkc<C>(fma(-r, t.x, gv.x), fma(-r, t.y, gv.y));
+  const int n = dev_count(dn, gridDim.x);
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const int j = act[b];
+    const C* pj = P + (long)j * ld;
+    const C* tj = T + (long)j * ld;
+    C* gj = g + (long)j * ld;
+    C* xj = x + (long)j * ld;
+    double a = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < npw; i += 256) {
+      const C p = pj[i], gv = gj[i], t = tj[i];
+      double da = fma((double)p.x, (double)gv.x, (double)p.y * (double)gv.y);
+      double dc = fma((double)p.x, (double)t.x, (double)p.y * (double)t.y);
+      if (i == 0) { da -= 0.5 * (double)p.x * (double)gv.x; dc -= 0.5 * (double)p.x * (double)t.x; }
+      a += da;
+      c += dc;
+    }
+    const double2 s = block_sum2<256>(a, c, red);
+    const double rd = (2.0 * s.x) / (2.0 * s.y);
+    const R r = R(rd);
+    for (int i = threadIdx.x; i < npw; i += 256) {
+      const C p = pj[i], t = tj[i];
+      C xv = xj[i], gv = gj[i];
+      xj[i] = mkc<C>(fma(-r, p.x, xv.x), fma(-r, p.y, xv.y));
+      gj[i] = mkc<C>(fma(-r, t.x, gv.x), fma(-r, t.y, gv.y));
+    }
   }
 }
 void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
-               long ld, cudaStream_t s) {
+               long ld, cudaStream_t s, const int* dn) {
   if (nact <= 0) return;
-  k_cg_update<double2><<<nact, 256, 0, s>>>(act, x, g, P, T, npw, ld);
+  k_cg_update<double2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, x, g, P, T, npw, ld);
 }
 void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
-                 cudaStream_t s) {
+                 cudaStream_t s, const int* dn) {
   if (nact <= 0) return;
-  k_cg_update<float2><<<nact, 256, 0, s>>>(act, x, g, P, T, npw, ld);
+  k_cg_update<float2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, x, g, P, T, npw, ld);
 }
 
 // ---------------------------------------------------------------------------
@@ -517,7 +540,9 @@ void refine_accumulate(const int* act, int nact, double2* X, const float2* d32, 
 
 // FP32 T = g2kin P (Im at G=0 zeroed) - e P for the kinetic-only operator
 __global__ void k_kinetic_hpsi32(const float2* __restrict__ P, float2* __restrict__ T, const float* __restrict__ g2kin,
-                                 const float* __restrict__ ecol, const int* __restrict__ cols, int npw, long ld) {
+                                 const float* __restrict__ ecol, const int* __restrict__ cols, const int* dn, int npw,
+                                 long ld) {
+  if ((int)blockIdx.y >= dev_count(dn, gridDim.y)) return;
   const int c = cols ? cols[blockIdx.y] : blockIdx.y;
   const float e = ecol[c];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npw; i += gridDim.x * blockDim.x) {
@@ -528,9 +553,9 @@ __global__ void k_kinetic_hpsi32(const float2* __restrict__ P, float2* __restric
   }
 }
 void kinetic_hpsi32(const float2* P, float2* T, const float* g2kin, const float* ecol, const int* cols, int ncol,
-                    int npw, long ld, cudaStream_t s) {
+                    int npw, long ld, cudaStream_t s, const int* dn) {
   if (ncol <= 0) return;
-  k_kinetic_hpsi32<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(P, T, g2kin, ecol, cols, npw, ld);
+  k_kinetic_hpsi32<<<dim3((npw + 255) / 256, ncol), 256, 0, s>>>(P, T, g2kin, ecol, cols, dn, npw, ld);
 }
 
 __global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, long n) {
@@ -547,12 +572,14 @@ void to_float(const double* a, float* b, long n, cudaStream_t s) {
 // part[s][j][r] = sum_{k in split s} W[r][k] X[col j][k]; tile 64 r x 64 j, k step 16
 __global__ void __launch_bounds__(256) k_gemm_tn_f32(const float* __restrict__ W, long ldw, int M,
                                                      const float* __restrict__ X, long ldx,
-                                                     const int* __restrict__ cols, int ncol, int K, int kchunk,
-                                                     float* __restrict__ part) {
+                                                     const int* __restrict__ cols, int ncol_host, const int* dn,
+                                                     int K, int kchunk, float* __restrict__ part) {
   __shared__ float Ws[16][64 + 4];
   __shared__ float Xs[16][64 + 4];
+  const int ncol = dev_count(dn, ncol_host);
   const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
   const int r0 = blockIdx.x * 64, j0 = blockIdx.y * 64, split = blockIdx.z;
+  if (j0 >= ncol) return;
   const int kb = split * kchunk, ke = min(K, kb + kchunk);
   float acc[4][4] = {};
   // loader: 64 rows x 8 float2 per operand, two per thread
@@ -612,21 +639,24 @@ int gemm_tn_splits32(int M, int ncol, int K) {
 }
 
 void gemm_tn32(const float* W, long ldw, int M, const float* X, long ldx, const int* cols, int ncol, int K, int nsplit,
-               float* part, cudaStream_t s) {
+               float* part, cudaStream_t s, const int* dn) {
   if (ncol <= 0 || M <= 0) return;
   int kchunk = (K + nsplit - 1) / nsplit;
   kchunk = (kchunk + 15) / 16 * 16;
   dim3 grid((M + 63) / 64, (ncol + 63) / 64, nsplit);
-  k_gemm_tn_f32<<<grid, 256, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, K, kchunk, part);
+  k_gemm_tn_f32<<<grid, 256, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, dn, K, kchunk, part);
 }
 
-__global__ void __launch_bounds__(256) k_gamma_reduce32(const float* __restrict__ part, int nsplit, int M, int ncol,
+__global__ void __launch_bounds__(256) k_gamma_reduce32(const float* __restrict__ part, int nsplit, int M,
+                                                        int ncol_host, const int* dn,
                                                         const float* __restrict__ W, long ldw,
                                                         const float* __restrict__ X, long ldx,
                                                         const int* __restrict__ cols, const float* __restrict__ D,
                                                         int nkb, float alpha, float* __restrict__ C) {
   extern __shared__ float Sf[];
+  const int ncol = dev_count(dn, ncol_host);
   const int j = blockIdx.x;
+  if (j >= ncol) return;
   const int col = cols ? cols[j] : j;
   const float x0 = X[(long)col * ldx];
   for (int r = threadIdx.x; r < M; r += blockDim.x) {
@@ -647,19 +677,23 @@ __global__ void __launch_bounds__(256) k_gamma_reduce32(const float* __restrict_
   }
 }
 void gamma_reduce32(const float* part, int nsplit, int M, int ncol, const float* W, long ldw, const float* X, long ldx,
-                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s) {
+                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s, const int* dn) {
   if (ncol <= 0 || M <= 0) return;
-  k_gamma_reduce32<<<ncol, 256, sizeof(float) * M, s>>>(part, nsplit, M, ncol, W, ldw, X, ldx, cols, D, nkb, alpha, C);
+  k_gamma_reduce32<<<ncol, 256, sizeof(float) * M, s>>>(part, nsplit, M, ncol, dn, W, ldw, X, ldx, cols, D, nkb, alpha,
+                                                        C);
 }
 
 // Y[col j][k] += sum_r W[r][k] C[j][r]; tile 128 k x 32 j, r step 16
 __global__ void __launch_bounds__(256) k_gemm_nn_f32(const float* __restrict__ W, long ldw, int M,
                                                      const float* __restrict__ C, float* __restrict__ Y, long ldy,
-                                                     const int* __restrict__ cols, int ncol, int K) {
+                                                     const int* __restrict__ cols, int ncol_host, const int* dn,
+                                                     int K) {
   __shared__ float Ws[16][128 + 4];
   __shared__ float Cs[16][32 + 1];
+  const int ncol = dev_count(dn, ncol_host);
   const int tid = threadIdx.x, tx = tid % 32, ty = tid / 32;
   const int k0 = blockIdx.x * 128, j0 = blockIdx.y * 32;
+  if (j0 >= ncol) return;
   float acc[4][4] = {};  // [k i][j q]: k = k0 + tx*4 + i, j = j0 + ty*4 + q
   for (int rb = 0; rb < M; rb += 16) {
     for (int e = tid; e < 16 * 64; e += 256) {           // W tile: 16 r x 64 float2
@@ -701,10 +735,58 @@ __global__ void __launch_bounds__(256) k_gemm_nn_f32(const float* __restrict__ W
   }
 }
 void gemm_nn32_acc(const float* W, long ldw, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
-                   cudaStream_t s) {
+                   cudaStream_t s, const int* dn) {
   if (ncol <= 0 || M <= 0) return;
   dim3 grid((K + 127) / 128, (ncol + 31) / 32);
-  k_gemm_nn_f32<<<grid, 256, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, K);
+  k_gemm_nn_f32<<<grid, 256, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, dn, K);
+}
+
+// ---------------------------------------------------------------------------
+// device-side loop control of the graph-captured PCG loops
+// ---------------------------------------------------------------------------
+// st[0] systems of the batch, st[1] iteration of the next pass, st[2] last
+// iteration run, st[3] inner iterations run over all refinements (mixed form);
+// st[4..5] active system-iterations and st[6..7] FFT boxes (64-bit counters).
+__global__ void k_loop_init(int* st, int nsys, int reset_totals) {
+  st[0] = nsys;
+  st[1] = 1;
+  st[2] = 0;
+  if (reset_totals) {
+    st[3] = 0;
+    *reinterpret_cast<long long*>(st + 4) = 0;
+    *reinterpret_cast<long long*>(st + 6) = 0;
+  }
+}
+void loop_init(int* st, int nsys, bool reset_totals, cudaStream_t s) {
+  k_loop_init<<<1, 1, 0, s>>>(st, nsys, reset_totals ? 1 : 0);
+}
+
+// End of one PCG pass.  FP64 form (shared_budget = 0): linsolve's loop over
+// iter = 1..n_dfpt_maxiter, leaving when no system is active
+// (linsolve_sternheimer_m_wfcts.f90:146,222).  Mixed form: the inner passes of
+// all refinements share n_dfpt_maxiter.  Sets the WHILE condition of the graph.
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, int shared_budget) {
+  const int n = *nact, it = st[1];
+  long long* sum = reinterpret_cast<long long*>(st + 4);
+  long long* boxes = reinterpret_cast<long long*>(st + 6);
+  bool more;
+  if (n > 0) {
+    *sum += n;
+    *boxes += 2 * ((n + 1) / 2);
+  }
+  if (!shared_budget) {
+    st[2] = it;
+    more = n > 0 && it < maxiter;
+  } else {
+    if (n > 0) st[3] += 1;
+    more = n > 0 && st[3] < maxiter;
+  }
+  if (more) st[1] = it + 1;
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool shared_budget,
+              cudaStream_t s) {
+  k_loop_ctl<<<1, 1, 0, s>>>(h, nact, st, maxiter, shared_budget ? 1 : 0);
 }
 
 __global__ void k_count_unconverged(const unsigned char* __restrict__ conv, int nocc, int mb, int* __restrict__ out) {

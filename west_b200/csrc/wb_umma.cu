@@ -224,6 +224,7 @@ struct BraketArgs {
   int NP, M, kb_per_split, nkb;
   float* part;
   int* err;
+  const int* dn;  // device count of columns (graph replays) or null
 };
 
 __host__ __device__ constexpr int braket_stage_bytes(int NP) { return 2 * kTile + NP * 256; }
@@ -238,8 +239,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_braket_umma(BraketArgs a) {
   uint32_t* slot = reinterpret_cast<uint32_t*>(mdone + 2);
   volatile int* abort_f = reinterpret_cast<volatile int*>(slot + 1);
 
+  const int ncol = a.dn ? *a.dn : a.ncol;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int j0 = blockIdx.x * kRows;
+  if (j0 >= ncol) return;  // before any TMEM or barrier state
   const int kb0 = blockIdx.y * a.kb_per_split;
   const int nk = min(a.nkb, kb0 + a.kb_per_split) - kb0;
   const uint32_t ncols = tmem_cols(a.NP);
@@ -263,7 +266,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_braket_umma(BraketArgs a) {
 #pragma unroll
   for (int p = 0; p < 4; ++p) {
     const int j = j0 + p * 32 + (tid >> 3);
-    xr[p] = j < a.ncol ? a.X + (long)(a.cols ? a.cols[j] : j) * a.ldx : nullptr;
+    xr[p] = j < ncol ? a.X + (long)(a.cols ? a.cols[j] : j) * a.ldx : nullptr;
   }
   float v[4][8];
   auto load = [&](int kb) {
@@ -341,11 +344,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_braket_umma(BraketArgs a) {
   tc_fence_after();
   if (ok && warp < 4) {
     const int j = j0 + warp * 32 + lane;
-    float* dst = a.part + ((long)blockIdx.y * a.ncol + j) * a.M;
+    float* dst = a.part + ((long)blockIdx.y * ncol + j) * a.M;
     for (int c0 = 0; c0 < a.NP; c0 += 16) {
       float d[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, d);
-      if (j < a.ncol) {
+      if (j < ncol) {
 #pragma unroll
         for (int i = 0; i < 16; ++i)
           if (c0 + i < a.M) dst[c0 + i] = d[i];
@@ -373,6 +376,7 @@ struct UpdateArgs {
   const int* cols;
   int ncol, K, NJ;
   int* err;
+  const int* dn;
 };
 
 __host__ __device__ constexpr int update_smem_bytes(int nrb, int NJ) { return nrb * 2 * kTile + nrb * NJ * 256 + 64 + 1024; }
@@ -388,8 +392,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_update_umma(UpdateArgs a) {
   uint64_t* done = afull + 1;
   uint32_t* slot = reinterpret_cast<uint32_t*>(done + 1);
 
+  const int ncol = a.dn ? *a.dn : a.ncol;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int k0 = blockIdx.x * kRows, jt0 = blockIdx.y * NJ;
+  if (jt0 >= ncol) return;  // before any TMEM or barrier state
   const uint32_t ncols = tmem_cols(NJ);
   if (warp == 0) tmem_alloc(slot, ncols);
   if (tid == 0) {
@@ -412,7 +418,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_update_umma(UpdateArgs a) {
     const int j = jt0 + row, r0 = rb * 64 + ch * 8;
     float x[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) x[i] = (j < a.ncol && r0 + i < a.M) ? __ldg(a.C + (long)j * a.M + r0 + i) : 0.f;
+    for (int i = 0; i < 8; ++i) x[i] = (j < ncol && r0 + i < a.M) ? __ldg(a.C + (long)j * a.M + r0 + i) : 0.f;
     uint4 hi, lo;
     split8(x, hi, lo);
     unsigned char* b = Bt + rb * NJ * 256;
@@ -455,7 +461,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_update_umma(UpdateArgs a) {
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int j = jt0 + c0 + i;
-      ycol[i] = (j < a.ncol && k < a.K) ? (a.cols ? __ldg(a.cols + j) : j) : -1;
+      ycol[i] = (j < ncol && k < a.K) ? (a.cols ? a.cols[j] : j) : -1;
     }
 #pragma unroll
     for (int i = 0; i < 16; ++i) yv[i] = ycol[i] >= 0 ? a.Y[(long)ycol[i] * a.ldy + k] : 0.f;
@@ -495,10 +501,10 @@ bool umma_supported(int M) { return M >= 1 && M <= 256; }
 
 int umma_np(int M) { return (M + 15) / 16 * 16; }
 
-void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split) {
+void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split, int ctas_per_sm) {
   const int nkb = (K + 63) / 64;
   const int tiles = std::max(1, (ncol + kRows - 1) / kRows);
-  const int target = std::max(1, (2 * 148 + tiles - 1) / tiles);
+  const int target = std::max(1, (ctas_per_sm * 148 + tiles - 1) / tiles);
   int per = std::max(2, (nkb + target - 1) / target);
   per = std::min(per, nkb);
   *kb_per_split = per;
@@ -509,9 +515,11 @@ size_t umma_part_floats(int M, int nsys, int K) {
   size_t best = 0;
   for (int t = 1; t <= (nsys + kRows - 1) / kRows; ++t) {
     const int n = std::min(nsys, t * kRows);
-    int ns, per;
-    umma_braket_plan(n, K, &ns, &per);
-    best = std::max(best, (size_t)ns * n * M);
+    for (int c = 1; c <= kUmmaMaxCtas; ++c) {
+      int ns, per;
+      umma_braket_plan(n, K, &ns, &per, c);
+      best = std::max(best, (size_t)ns * n * M);
+    }
   }
   return best;
 }
@@ -536,7 +544,7 @@ void umma_setup() {
 }
 
 int umma_braket(const void* tiles, int M, const float* X, long ldx, const int* cols, int ncol, int K, float* part,
-                int* err, cudaStream_t s) {
+                int* err, cudaStream_t s, const int* dn, int ctas_per_sm) {
   if (ncol <= 0) return 1;
   BraketArgs a{};
   a.X = X;
@@ -549,16 +557,17 @@ int umma_braket(const void* tiles, int M, const float* X, long ldx, const int* c
   a.M = M;
   a.nkb = (K + 63) / 64;
   int nsplit;
-  umma_braket_plan(ncol, K, &nsplit, &a.kb_per_split);
+  umma_braket_plan(ncol, K, &nsplit, &a.kb_per_split, std::min(std::max(ctas_per_sm, 1), kUmmaMaxCtas));
   a.part = part;
   a.err = err;
+  a.dn = dn;
   const dim3 grid((ncol + kRows - 1) / kRows, nsplit);
   k_braket_umma<<<grid, kThreads, braket_smem(a.NP), s>>>(a);
   return nsplit;
 }
 
 void umma_update(const void* tiles, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
-                 int* err, cudaStream_t s) {
+                 int* err, cudaStream_t s, const int* dn, int nj) {
   if (ncol <= 0) return;
   UpdateArgs a{};
   a.Wt = static_cast<const unsigned char*>(tiles);
@@ -571,8 +580,9 @@ void umma_update(const void* tiles, int M, const float* C, float* Y, long ldy, c
   a.cols = cols;
   a.ncol = ncol;
   a.K = K;
-  a.NJ = update_nj(a.nrb);
+  a.NJ = (nj == 64 || (nj == 128 && a.nrb <= 2)) ? nj : update_nj(a.nrb);
   a.err = err;
+  a.dn = dn;
   const dim3 grid((K + kRows - 1) / kRows, (ncol + a.NJ - 1) / a.NJ);
   k_update_umma<<<grid, kThreads, update_smem_bytes(a.nrb, a.NJ), s>>>(a);
 }

@@ -24,7 +24,9 @@ WB_NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 EXPORTS = (
     "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
     "wb_apply_operator_device_noalloc",
-    "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling", "wb_davidson", "wb_pdep_db_write",
+    "wb_apply_operator_multi", "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling",
+    "wb_set_graphs", "wb_get_tuning", "wb_set_autotune", "wb_davidson",
+    "wb_pdep_db_write",
     "wb_pdep_db_read", "wb_last_error", "wb_version",
 )
 NSTAGES = 10
@@ -63,6 +65,12 @@ class WbDavidsonInfo(ctypes.Structure):
                 ("perturbations", ctypes.c_longlong), ("seconds", _d)]
 
 
+class WbTuning(ctypes.Structure):
+    _fields_ = [("autotune", _i), ("tuned_fp64", _i), ("tuned_mixed", _i), ("dmma_ctas_per_sm", _i),
+                ("tc_braket_ctas_per_sm", _i), ("tc_update_systems", _i), ("plane_fused_fp64", _i),
+                ("plane_fused_mixed", _i), ("tuning_ms", ctypes.c_float)]
+
+
 class WestB200Error(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"west_b200 error {code}: {msg}")
@@ -87,6 +95,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.wb_set_precision.argtypes = [_p, _i]
     lib.wb_set_batch.argtypes = [_p, _i]
     lib.wb_set_profiling.argtypes = [_p, _i]
+    lib.wb_set_graphs.argtypes = [_p, _i]
+    lib.wb_get_tuning.argtypes = [_p, ctypes.POINTER(WbTuning)]
+    lib.wb_set_autotune.argtypes = [_p, _i]
+    lib.wb_apply_operator_multi.argtypes = [_i, _p, _p, _p, _p, _p, _p, _d, _i, _p, _i]
     lib.wb_get_stats.argtypes = [_p, ctypes.POINTER(WbStats)]
     lib.wb_davidson.argtypes = [_p, ctypes.POINTER(WbDavidsonParams), _p, _i, _p, _p, _p, _i,
                                 ctypes.POINTER(WbDavidsonInfo)]

@@ -98,6 +98,20 @@ class ResponseOperator:
                 mask |= 1 << _lib.STAGES.index(name)
         _lib.check(self._lib.wb_set_profiling(self._ctx, mask))
 
+    def set_graphs(self, enable: bool = True):
+        """Run each batch's PCG loop from one CUDA graph launch (default) or eagerly."""
+        _lib.check(self._lib.wb_set_graphs(self._ctx, int(bool(enable))))
+
+    def set_autotune(self, enable: bool = True):
+        """Tune launch shapes on the first batch of each form (default) or keep the built-in ones."""
+        _lib.check(self._lib.wb_set_autotune(self._ctx, int(bool(enable))))
+
+    def tuning(self) -> dict:
+        """Launch shapes the autotuner chose (wb_get_tuning)."""
+        t = _lib.WbTuning()
+        _lib.check(self._lib.wb_get_tuning(self._ctx, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
     def stats(self) -> dict:
         st = _lib.WbStats()
         _lib.check(self._lib.wb_get_stats(self._ctx, ctypes.byref(st)))
@@ -148,6 +162,41 @@ class ResponseOperator:
         if self.verbose and not info.converged:
             sys.stdout.write(f"     WARNING : {info.notcnv:5d} eigenvalues not converged in chidiago\n")
         return ev, conv.astype(bool), vec, {k: getattr(info, k) for k, _ in info._fields_}
+
+
+def apply_operator_multi(ops, dvgs, dngs, tr2, iq=1):
+    """Several ground states in one call (wb_apply_operator_multi): ops[i] maps
+    dvgs[i] [npwqx_i, m_i] to dngs[i]; the systems run concurrently on one GPU.
+    All arrays are host numpy (Fortran complex128) or all torch CUDA tensors
+    ([m_i, npwqx_i]).  Returns the list of ierr arrays."""
+    n = len(ops)
+    if not (len(dvgs) == len(dngs) == n):
+        raise ValueError("ops, dvgs and dngs must have the same length")
+    lib = ops[0]._lib
+    on_device = n > 0 and _is_torch_cuda(dvgs[0])
+    keep, ierrs = [], []
+    ms, lds_in, lds_out, pin, pout = [], [], [], [], []
+    for op, dvg, dng in zip(ops, dvgs, dngs):
+        if on_device:
+            m = int(dvg.shape[0])
+            ms.append(m); lds_in.append(int(dvg.shape[1])); lds_out.append(int(dng.shape[1]))
+            pin.append(dvg.data_ptr()); pout.append(dng.data_ptr())
+        else:
+            if not (isinstance(dng, np.ndarray) and dng.dtype == np.complex128 and dng.flags.f_contiguous):
+                raise TypeError("dng must be a Fortran-ordered complex128 array")
+            d = np.asfortranarray(dvg, dtype=np.complex128)
+            keep.append(d)
+            ms.append(int(d.shape[1])); lds_in.append(d.shape[0]); lds_out.append(dng.shape[0])
+            pin.append(_ptr(d)); pout.append(_ptr(dng))
+        ierrs.append(np.zeros(max(ms[-1], 1), dtype=np.int32))
+    P = ctypes.c_void_p * max(n, 1)
+    I = ctypes.c_int * max(n, 1)
+    ctxs = P(*[op._ctx.value for op in ops])
+    perr = P(*[_ptr(e) for e in ierrs])
+    rc = lib.wb_apply_operator_multi(n, ctxs, I(*ms), P(*pin), I(*lds_in), P(*pout), I(*lds_out), float(tr2), int(iq),
+                                     perr, int(on_device))
+    _lib.check(rc)
+    return [e[:m] for e, m in zip(ierrs, ms)]
 
 
 def _is_torch_cuda(x) -> bool:
