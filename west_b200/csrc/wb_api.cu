@@ -236,7 +236,8 @@ int ensure_workspace(wb_ctx* c, int mb, long ld_in, long ld_out) {
   bad |= c->sticks.ensure(stk1 * nitems) != 0;
   bad |= c->sticks2.ensure(stk1 * mp) != 0;
   bad |= c->acc.ensure(sizeof(double2) * (size_t)c->nnr * mp) != 0;
-  bad |= c->part.ensure(sizeof(double) * (size_t)nsplit * nsys * c->nproj) != 0;
+  bad |= c->part.ensure(sizeof(double) * std::max((size_t)nsplit * nsys * c->nproj,
+                                                   gemm_tn_part_doubles(c->nproj, (int)nsys, 2 * c->npw, 4))) != 0;
   bad |= c->C.ensure(sizeof(double) * nsys * c->nproj) != 0;
   bad |= c->rho.ensure(sizeof(double) * nsys) != 0;
   bad |= c->conv.ensure(nsys + 16) != 0;
@@ -395,12 +396,13 @@ void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const i
   }
   {
     Stage g(c, WB_STAGE_GEMM_TN, 1, n);
-    gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s, dn);
+    gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s, dn,
+            c->tune.dmma_ctas);
   }
   {
     Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
     gamma_reduce(c->part.as<double>(), nsplit, M, n, Wsub, K, (const double*)Xv, 2 * ld, cols, c->D.as<double>(),
-                 nkb, c->alpha, c->C.as<double>(), s, dn);
+                 nkb, c->alpha, c->C.as<double>(), s, dn, K, c->tune.dmma_ctas);
   }
   {
     Stage g(c, WB_STAGE_GEMM_NN, 1, n);
@@ -509,7 +511,7 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
   {
     Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
     gamma_reduce32(c->part32.as<float>(), nsplit, M, n, W, K, (const float*)Pv, 2 * ld, cols, c->D32.as<float>(), nkb,
-                   (float)c->alpha, c->C32.as<float>(), s, dn);
+                   (float)c->alpha, c->C32.as<float>(), s, dn, K, c->umma ? c->tune.umma_ctas : 0);
   }
   {
     Stage g(c, WB_STAGE_GEMM_NN, 1, n);
@@ -532,36 +534,80 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
 // changes.  Stage profiling needs host-side events and runs the loop eagerly.
 bool graph_mode(const wb_ctx* c) { return c->use_graphs && c->prof == 0; }
 
-template <class Body>
-int capture_loop(wb_ctx* c, wb_ctx::LoopGraph& lg, std::vector<const void*> key, double tr2, Body body) {
+// The graph: WHILE { k_loop_bucket -> SWITCH(bucket) { one PCG pass sized for
+// up to kMinBucketItems << k band-pair items } -> k_loop_ctl }.  Each branch
+// launches the same kernels as the eager loop with grids for its bucket; the
+// CTAs beyond the device count return at once, so at most half a grid idles.
+constexpr int kMinBucketItems = 16;
+
+template <class Pass>
+int capture_loop(wb_ctx* c, wb_ctx::LoopGraph& lg, std::vector<const void*> key, double tr2, int cap, const int* dn,
+                 int* st, bool shared_budget, Pass pass) {
   if (lg.exec && lg.key == key && lg.tr2 == tr2) return WB_OK;
   lg.release();
-  cudaGraph_t g = nullptr;
-  WB_CU(cudaGraphCreate(&g, 0));
-  lg.graph = g;
-  cudaGraphConditionalHandle h;
-  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
-  cudaGraphNodeParams np = {};
-  np.type = cudaGraphNodeTypeConditional;
-  np.conditional.handle = h;
-  np.conditional.type = cudaGraphCondTypeWhile;
-  np.conditional.size = 1;
-  cudaGraphNode_t node;
-  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
-  if (e == cudaSuccess)
-    e = cudaStreamBeginCaptureToGraph(c->stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                      cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) {
-    lg.release();
-    return fail(WB_ERR_CUDA, std::string("graph setup of the PCG loop: ") + cudaGetErrorString(e));
-  }
+  const int cap_items = (cap + 1) / 2;
+  int nb = 1;
+  while ((kMinBucketItems << (nb - 1)) < cap_items) ++nb;
+  cudaStream_t s = c->stream;
   const wb_stats saved = c->stats;
-  body(h);
-  cudaGraph_t captured = nullptr;
-  e = cudaStreamEndCapture(c->stream, &captured);
+  cudaError_t e = cudaGraphCreate(&lg.graph, 0);
+  cudaGraphConditionalHandle hw, hs;
+  cudaGraphNodeParams wp = {};
+  cudaGraphNode_t wnode, bnode, snode;
+  cudaGraph_t body = nullptr;
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hw, lg.graph, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) {
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    e = cudaGraphAddNode(&wnode, lg.graph, nullptr, 0, &wp);
+  }
+  if (e == cudaSuccess) {
+    body = wp.conditional.phGraph_out[0];
+    e = cudaGraphConditionalHandleCreate(&hs, body, 0, 0);
+  }
+  // 1. the bucket of this pass
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    loop_bucket(hs, dn, kMinBucketItems, nb, s);
+    cudaGraph_t g1 = nullptr;
+    e = cudaStreamEndCapture(s, &g1);
+  }
+  size_t nn = 1;
+  if (e == cudaSuccess) e = cudaGraphGetNodes(body, &bnode, &nn);
+  // 2. SWITCH over the buckets, one PCG pass per branch
+  cudaGraphNodeParams sp = {};
+  if (e == cudaSuccess) {
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = hs;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = (unsigned)nb;
+    e = cudaGraphAddNode(&snode, body, &bnode, 1, &sp);
+  }
+  for (int k = 0; k < nb && e == cudaSuccess; ++k) {
+    e = cudaStreamBeginCaptureToGraph(s, sp.conditional.phGraph_out[k], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) break;
+    pass(std::min(cap, 2 * (kMinBucketItems << k)));
+    cudaGraph_t gk = nullptr;
+    e = cudaStreamEndCapture(s, &gk);
+  }
+  // 3. loop control after the pass
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, body, &snode, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    loop_ctl(hw, dn, st, c->maxiter, shared_budget, s);
+    cudaGraph_t g3 = nullptr;
+    e = cudaStreamEndCapture(s, &g3);
+  }
   c->stats = saved;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&lg.exec, g, 0);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&lg.exec, lg.graph, 0);
   if (e != cudaSuccess) {
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(s, &junk);
+    }
     cudaGetLastError();
     lg.release();
     return fail(WB_ERR_CUDA, std::string("capture of the PCG loop: ") + cudaGetErrorString(e));
@@ -603,17 +649,16 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
                                     c->items_in.p, c->nact_in.p, c->conv_in.p, c->rho_in.p, c->rho0.p,
                                     c->part32.p, c->C32.p,    c->ecol32.p, st,          (const void*)(intptr_t)cap};
     const int* dn = c->nact_in.as<int>();
-    rc = capture_loop(c, c->loop32, key, tr2, [&](cudaGraphConditionalHandle h) {
-      cg_prec_rho32(c->act_in.as<int>(), cap, c->g32.as<float2>(), c->P32.as<float2>(), c->iprec.as<double>(), nocc,
+    rc = capture_loop(c, c->loop32, key, tr2, cap, dn, st, true, [&](int nmax) {
+      cg_prec_rho32(c->act_in.as<int>(), nmax, c->g32.as<float2>(), c->P32.as<float2>(), c->iprec.as<double>(), nocc,
                     c->rho_in.as<double>(), c->conv_in.as<unsigned char>(), 0, kInnerRhoReduction,
                     c->rho0.as<double>(), tr2, npw, ld, s, dn, st + 1);
       cg_compact(c->conv_in.as<unsigned char>(), cap, c->act_in.as<int>(), c->items_in.as<int2>(),
                  c->nact_in.as<int>(), nullptr, s, st);
-      apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), c->act_in.as<int>(), c->items_in.as<int2>(), cap,
+      apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), c->act_in.as<int>(), c->items_in.as<int2>(), nmax,
                 nsplit32, dn);
-      cg_update32(c->act_in.as<int>(), cap, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(),
+      cg_update32(c->act_in.as<int>(), nmax, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(),
                   c->T32.as<float2>(), npw, ld, s, dn);
-      loop_ctl(h, dn, st, c->maxiter, true, s);
     });
     if (rc) return rc;
     loop_init(st, nsys, true, s);
@@ -780,13 +825,12 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
       const int* dn = c->nact.as<int>();
       std::vector<const void*> key = {B, X, G, T, c->sticks.p, act, items, dn, conv, c->rho.p, c->part.p, c->C.p,
                                       c->ecol.p, st, (const void*)(intptr_t)cap};
-      int rc = capture_loop(c, c->loop64, key, tr2, [&](cudaGraphConditionalHandle h) {
-        cg_prec_rho(act, cap, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, 0, tr2, npw, ld, s, dn,
+      int rc = capture_loop(c, c->loop64, key, tr2, cap, dn, st, false, [&](int nmax) {
+        cg_prec_rho(act, nmax, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, 0, tr2, npw, ld, s, dn,
                     st + 1);
         cg_compact(conv, cap, act, items, c->nact.as<int>(), nullptr, s, st);
-        apply_A(c, B, T, act, items, cap, cap, nsplit_cap, dn);
-        cg_update(act, cap, X, G, B, T, npw, ld, s, dn);
-        loop_ctl(h, dn, st, c->maxiter, false, s);
+        apply_A(c, B, T, act, items, nmax, cap, nsplit_cap, dn);
+        cg_update(act, nmax, X, G, B, T, npw, ld, s, dn);
       });
       if (rc) return rc;
       loop_init(st, nsys, true, s);

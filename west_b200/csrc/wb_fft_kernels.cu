@@ -45,10 +45,21 @@ WB_DEV void load_tw(C* tw, const C* twg) {
 // z pass, inverse: sphere coefficients of a pair of columns -> sticks
 // ---------------------------------------------------------------------------
 // One unit = stick pairs [16 qg, 16 qg + 16) of band-pair item `item`.
+// Shared memory of every unit: the twiddles (2N), then the work area.  A unit
+// takes its pointers from the dynamic shared array itself so that a unit body
+// compiled as a separate function still addresses shared memory directly.
+template <class C>
+WB_DEV C* smem_tw() {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  return reinterpret_cast<C*>(smraw);
+}
+
 template <int N, bool PR, class C>
 WB_DEV void zinv_unit(const C* __restrict__ src, long ld, const int2* __restrict__ items, const StickTab& st,
-                      C* __restrict__ out, const C* tw, C* zb, int qg, int item) {
+                      C* __restrict__ out, int qg, int item) {
   constexpr int LS = LinePad<N>::LEN | 1;  // odd line stride: conflict-free transposes
+  const C* tw = smem_tw<C>();
+  C* zb = smem_tw<C>() + 2 * N;
   const int q0 = qg * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
   for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = mkc<C>(0, 0);  // pads too
@@ -90,34 +101,10 @@ template <int N, bool PR, class C>
 __global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld,
                                               const int2* __restrict__ items, StickTab st,
                                               C* __restrict__ out,
-                                              const C* __restrict__ twg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  load_tw<N>(tw, twg);
-  zinv_unit<N, PR, C>(src, ld, items, st, out, tw, tw + 2 * N, blockIdx.x, blockIdx.y);
-}
-
-// Graph replays: a fixed grid of resident CTAs strides over the units of a
-// device-side item count; the unit body is a call so that nothing is hoisted
-// across units (register pressure stays that of one unit).
-template <int N, bool PR, class C>
-__device__ __noinline__ void zinv_unit_call(const C* src, long ld, const int2* items, StickTab st, C* out,
-                                            const C* tw, C* zb, int qg, int item) {
-  zinv_unit<N, PR, C>(src, ld, items, st, out, tw, zb, qg, item);
-}
-template <int N, bool PR, class C>
-__global__ void __launch_bounds__(ZNT) k_zinv_loop(const C* __restrict__ src, long ld,
-                                                   const int2* __restrict__ items, StickTab st,
-                                                   C* __restrict__ out, const C* __restrict__ twg, const int* dn) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  load_tw<N>(tw, twg);
-  const int ngx = (st.nsp + ZSG - 1) / ZSG;
-  const int units = dev_count<true>(dn, 0) * ngx;
-  for (int u = blockIdx.x; u < units; u += gridDim.x) {
-    zinv_unit_call<N, PR, C>(src, ld, items, st, out, tw, tw + 2 * N, u % ngx, u / ngx);
-    __syncthreads();
-  }
+                                              const C* __restrict__ twg, const int* dn) {
+  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;  // beyond the device item count
+  load_tw<N>(smem_tw<C>(), twg);
+  zinv_unit<N, PR, C>(src, ld, items, st, out, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -125,8 +112,10 @@ __global__ void __launch_bounds__(ZNT) k_zinv_loop(const C* __restrict__ src, lo
 // ---------------------------------------------------------------------------
 template <int N, bool PR, class C, class Epi>
 WB_DEV void zfwd_unit(const C* __restrict__ sticks, const int2* __restrict__ items, const StickTab& st,
-                      const C* tw, C* zb, const Epi& epi, int qg, int item) {
+                      const Epi& epi, int qg, int item) {
   constexpr int LS = LinePad<N>::LEN | 1;
+  const C* tw = smem_tw<C>();
+  C* zb = smem_tw<C>() + 2 * N;
   const int q0 = qg * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
   const int ns = 2 * nq;
@@ -162,31 +151,10 @@ WB_DEV void zfwd_unit(const C* __restrict__ sticks, const int2* __restrict__ ite
 template <int N, bool PR, class C, class Epi>
 __global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
                                               const int2* __restrict__ items, StickTab st,
-                                              const C* __restrict__ twg, Epi epi) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  load_tw<N>(tw, twg);
-  zfwd_unit<N, PR, C, Epi>(sticks, items, st, tw, tw + 2 * N, epi, blockIdx.x, blockIdx.y);
-}
-
-template <int N, bool PR, class C, class Epi>
-__device__ __noinline__ void zfwd_unit_call(const C* sticks, const int2* items, StickTab st, const C* tw, C* zb,
-                                            Epi epi, int qg, int item) {
-  zfwd_unit<N, PR, C, Epi>(sticks, items, st, tw, zb, epi, qg, item);
-}
-template <int N, bool PR, class C, class Epi>
-__global__ void __launch_bounds__(ZNT) k_zfwd_loop(const C* __restrict__ sticks,
-                                                   const int2* __restrict__ items, StickTab st,
-                                                   const C* __restrict__ twg, Epi epi, const int* dn) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  load_tw<N>(tw, twg);
-  const int ngx = (st.nsp + ZSG - 1) / ZSG;
-  const int units = dev_count<true>(dn, 0) * ngx;
-  for (int u = blockIdx.x; u < units; u += gridDim.x) {
-    __syncthreads();  // twiddles, and the previous unit's reads of zb
-    zfwd_unit_call<N, PR, C, Epi>(sticks, items, st, tw, tw + 2 * N, epi, u % ngx, u / ngx);
-  }
+                                              const C* __restrict__ twg, Epi epi, const int* dn) {
+  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;
+  load_tw<N>(smem_tw<C>(), twg);
+  zfwd_unit<N, PR, C, Epi>(sticks, items, st, epi, blockIdx.x, blockIdx.y);
 }
 
 struct EpiStore {
@@ -290,8 +258,10 @@ WB_DEV void plane_fft_rows(C* pl, const C* tw) {
 // psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma);
 // one unit = plane z of item `item`
 template <int N, bool PR, class C>
-WB_DEV void plane_vloc_unit(C* __restrict__ sticks, const StickTab& st, const real_t<C>* __restrict__ vs,
-                            const C* tw, C* pl, int z, int item) {
+WB_DEV void plane_vloc_unit(C* __restrict__ sticks, const StickTab& st, const real_t<C>* __restrict__ vs, int z,
+                            int item) {
+  const C* tw = smem_tw<C>();
+  C* pl = smem_tw<C>() + 2 * N;
   C* sz = sticks + ((long)item * N + z) * st.nst;
   plane_zero<N, PR>(pl, st);
   __syncthreads();
@@ -313,30 +283,10 @@ WB_DEV void plane_vloc_unit(C* __restrict__ sticks, const StickTab& st, const re
 template <int N, bool PR, class C>
 __global__ void __launch_bounds__(PNT) k_plane_vloc(C* __restrict__ sticks, StickTab st,
                                                     const real_t<C>* __restrict__ vs,
-                                                    const C* __restrict__ twg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  load_tw<N>(tw, twg);
-  plane_vloc_unit<N, PR, C>(sticks, st, vs, tw, tw + 2 * N, blockIdx.x, blockIdx.y);
-}
-
-template <int N, bool PR, class C>
-__device__ __noinline__ void plane_vloc_unit_call(C* sticks, StickTab st, const real_t<C>* vs, const C* tw, C* pl,
-                                                  int z, int item) {
-  plane_vloc_unit<N, PR, C>(sticks, st, vs, tw, pl, z, item);
-}
-template <int N, bool PR, class C>
-__global__ void __launch_bounds__(PNT) k_plane_vloc_loop(C* __restrict__ sticks, StickTab st,
-                                                         const real_t<C>* __restrict__ vs,
-                                                         const C* __restrict__ twg, const int* dn) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  load_tw<N>(tw, twg);
-  const int units = dev_count<true>(dn, 0) * N;
-  for (int u = blockIdx.x; u < units; u += gridDim.x) {
-    plane_vloc_unit_call<N, PR, C>(sticks, st, vs, tw, tw + 2 * N, u % N, u / N);
-    __syncthreads();
-  }
+                                                    const C* __restrict__ twg, const int* dn) {
+  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;
+  load_tw<N>(smem_tw<C>(), twg);
+  plane_vloc_unit<N, PR, C>(sticks, st, vs, blockIdx.x, blockIdx.y);
 }
 
 // sticks -> full real-space box (complex: two real functions), no scaling
@@ -452,10 +402,14 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
 // registers before the zero fill so their latency overlaps it.
 constexpr int kFusedMaxSticksPerThread = 4;
 
-// LOAD_TW: load the twiddles into tw after the stick loads are issued (one-unit kernels)
-template <int N, class C, bool LOAD_TW = false>
-WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, const real_t<C>* __restrict__ vs,
-                                  C* tw, C* pl, int z, int item, const C* __restrict__ twg = nullptr) {
+// LOAD_TW: load the twiddles into tw after the stick loads are issued (one-unit kernels);
+// PRELOAD: issue the stick loads into registers before zeroing the plane (one-unit
+// kernels; a unit called in a loop scatters straight from global memory)
+template <int N, class C, bool LOAD_TW = false, bool PRELOAD = true>
+WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, const real_t<C>* __restrict__ vs, int z,
+                                  int item, const C* __restrict__ twg = nullptr) {
+  C* tw = smem_tw<C>();
+  C* pl = smem_tw<C>() + 2 * N;
   using T = real_t<C>;
   constexpr int R = FftSplit<N>::N1;
   static_assert(FftSplit<N>::N1 == FftSplit<N>::N2, "fused rows need N1 == N2");
@@ -467,11 +421,13 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
   C* sz = sticks + ((long)item * N + z) * st.nst;
   C sv[MS];
   int sp[MS];
+  if constexpr (PRELOAD) {
 #pragma unroll
-  for (int i = 0; i < MS; ++i) {
-    const int s = tid + i * PNT;
-    sp[i] = -1;
-    if (s < st.nst) { sp[i] = st.st_pos[s]; sv[i] = sz[s]; }
+    for (int i = 0; i < MS; ++i) {
+      const int s = tid + i * PNT;
+      sp[i] = -1;
+      if (s < st.nst) { sp[i] = st.st_pos[s]; sv[i] = sz[s]; }
+    }
   }
   const int k1 = tid % R;
   const bool rowthr = tid < LPC * R;
@@ -479,9 +435,13 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
   if constexpr (LOAD_TW) load_tw<N>(tw, twg);
   plane_zero<N, true>(pl, st);
   __syncthreads();
+  if constexpr (PRELOAD) {
 #pragma unroll
-  for (int i = 0; i < MS; ++i)
-    if (sp[i] >= 0) pl[Plane<N>::at_lin(sp[i])] = sv[i];
+    for (int i = 0; i < MS; ++i)
+      if (sp[i] >= 0) pl[Plane<N>::at_lin(sp[i])] = sv[i];
+  } else {
+    plane_scatter<N>(pl, sz, st.st_pos, st.nst);
+  }
   __syncthreads();
   plane_fft_cols<N, +1, true>(pl, st, tw);
   fft_step1<N, +1, PNT, false, true, PRUNE_IN>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
@@ -520,29 +480,9 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
 template <int N, class C>
 __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sticks, StickTab st,
                                                              const real_t<C>* __restrict__ vs,
-                                                             const C* __restrict__ twg) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  plane_vloc_fused_unit<N, C, true>(sticks, st, vs, tw, tw + 2 * N, blockIdx.x, blockIdx.y, twg);
-}
-
-template <int N, class C>
-__device__ __noinline__ void plane_vloc_fused_unit_call(C* sticks, StickTab st, const real_t<C>* vs, C* tw,
-                                                        C* pl, int z, int item) {
-  plane_vloc_fused_unit<N, C>(sticks, st, vs, tw, pl, z, item);
-}
-template <int N, class C>
-__global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused_loop(C* __restrict__ sticks, StickTab st,
-                                                                  const real_t<C>* __restrict__ vs,
-                                                                  const C* __restrict__ twg, const int* dn) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C* tw = reinterpret_cast<C*>(smraw);
-  load_tw<N>(tw, twg);
-  const int units = dev_count<true>(dn, 0) * N;
-  for (int u = blockIdx.x; u < units; u += gridDim.x) {
-    plane_vloc_fused_unit_call<N, C>(sticks, st, vs, tw, tw + 2 * N, u % N, u / N);
-    __syncthreads();
-  }
+                                                             const C* __restrict__ twg, const int* dn) {
+  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;
+  plane_vloc_fused_unit<N, C, true>(sticks, st, vs, blockIdx.x, blockIdx.y, twg);
 }
 
 // ---------------------------------------------------------------------------
@@ -567,27 +507,6 @@ struct FftN {
     cudaFuncSetAttribute(k_plane_rhs<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
     cudaFuncSetAttribute(k_plane_drho<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
   }
-  // CTAs of one full wave of a loop kernel (graph replays stride over the units)
-  template <class K>
-  static int wave(K k, int threads, size_t smem) {
-    int per = 0, dev = 0, sms = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, smem);
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return std::max(1, per) * std::max(1, sms);
-  }
-  // [precision: 0 FP64, 1 FP32][prune]
-  static inline int w_zinv[2][2], w_zfwd[2][2], w_plane[2][2], w_fused[2];
-  template <bool PR, class C, class EpiH>
-  static void setup_loops(int pi) {
-    constexpr size_t zs = zsmem<N, C>(), ps = psmem<N, C>();
-    cudaFuncSetAttribute(k_zinv_loop<N, PR, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
-    cudaFuncSetAttribute(k_zfwd_loop<N, PR, C, EpiH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zs);
-    cudaFuncSetAttribute(k_plane_vloc_loop<N, PR, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ps);
-    w_zinv[pi][PR] = wave(k_zinv_loop<N, PR, C>, ZNT, zs);
-    w_zfwd[pi][PR] = wave(k_zfwd_loop<N, PR, C, EpiH>, ZNT, zs);
-    w_plane[pi][PR] = wave(k_plane_vloc_loop<N, PR, C>, PNT, ps);
-  }
   static void setup() {
     setup_pr<false>();
     setup_pr<true>();
@@ -595,12 +514,6 @@ struct FftN {
       cudaFuncSetAttribute(k_plane_vloc_fused<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
       cudaFuncSetAttribute(k_plane_vloc_fused<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)psmem<N, float2>());
-      cudaFuncSetAttribute(k_plane_vloc_fused_loop<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)psmem<N>());
-      cudaFuncSetAttribute(k_plane_vloc_fused_loop<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)psmem<N, float2>());
-      w_fused[0] = wave(k_plane_vloc_fused_loop<N, double2>, PNT, psmem<N>());
-      w_fused[1] = wave(k_plane_vloc_fused_loop<N, float2>, PNT, psmem<N, float2>());
     }
     for (int pr = 0; pr < 2; ++pr) {
       auto zi = pr ? k_zinv<N, true, float2> : k_zinv<N, false, float2>;
@@ -610,10 +523,6 @@ struct FftN {
       cudaFuncSetAttribute(zf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zsmem<N, float2>());
       cudaFuncSetAttribute(pv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N, float2>());
     }
-    setup_loops<false, double2, EpiHpsi>(0);
-    setup_loops<true, double2, EpiHpsi>(0);
-    setup_loops<false, float2, EpiHpsi32>(1);
-    setup_loops<true, float2, EpiHpsi32>(1);
   }
   static dim3 zgrid(const StickTab& st, int nitems) { return dim3((st.nsp + ZSG - 1) / ZSG, nitems); }
   static bool fused(const StickTab& st) {
@@ -623,69 +532,40 @@ struct FftN {
   template <class F>
   static bool use_fused(const F& f) { return !f.unfused && fused(f.st); }
   // Local-potential transforms of the PCG operator, FP64 (C = double2) or the
-  // FP32 inner solves (C = float2).  A host count launches one CTA per unit; a
-  // device count (graph replays) launches one wave of the loop kernels.
+  // FP32 inner solves (C = float2): one CTA per (stick group or plane, item);
+  // with a device count (graph replays) nitems is the bound the grid is sized
+  // for and the CTAs beyond the device count return at once.
   template <class C, class F>
   static void zinv_t(const F& f, const C* src, long ld, const int2* items, int nitems, C* sticks) {
     if (nitems <= 0) return;
-    constexpr int pi = sizeof(C) == 8 ? 1 : 0;
     constexpr size_t zs = zsmem<N, C>();
-    if (f.dcount) {
-      if (f.st.prune)
-        k_zinv_loop<N, true, C><<<w_zinv[pi][1], ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw, f.dcount);
-      else
-        k_zinv_loop<N, false, C><<<w_zinv[pi][0], ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw, f.dcount);
-      return;
-    }
     if (f.st.prune)
-      k_zinv<N, true, C><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+      k_zinv<N, true, C><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw, f.dcount);
     else
-      k_zinv<N, false, C><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw);
+      k_zinv<N, false, C><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(src, ld, items, f.st, sticks, f.tw, f.dcount);
   }
   template <class C, class F>
   static void vloc_t(const F& f, C* sticks, int nitems, const real_t<C>* vs) {
     if (nitems <= 0) return;
-    constexpr int pi = sizeof(C) == 8 ? 1 : 0;
     constexpr size_t ps = psmem<N, C>();
     const dim3 g(N, nitems);
     if constexpr (FUSABLE) {
       if (use_fused(f)) {
-        if (f.dcount)
-          k_plane_vloc_fused_loop<N, C><<<w_fused[pi], PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
-        else
-          k_plane_vloc_fused<N, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw);
+        k_plane_vloc_fused<N, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
         return;
       }
     }
-    if (f.dcount) {
-      if (f.st.prune)
-        k_plane_vloc_loop<N, true, C><<<w_plane[pi][1], PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
-      else
-        k_plane_vloc_loop<N, false, C><<<w_plane[pi][0], PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
-      return;
-    }
-    if (f.st.prune) k_plane_vloc<N, true, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw);
-    else k_plane_vloc<N, false, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw);
+    if (f.st.prune) k_plane_vloc<N, true, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+    else k_plane_vloc<N, false, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
   }
   template <class C, class F, class Epi>
   static void zfwd_t(const F& f, const C* sticks, const int2* items, int nitems, Epi epi) {
     if (nitems <= 0) return;
-    constexpr int pi = sizeof(C) == 8 ? 1 : 0;
     constexpr size_t zs = zsmem<N, C>();
-    if constexpr (std::is_same<Epi, EpiHpsi>::value || std::is_same<Epi, EpiHpsi32>::value) {
-      if (f.dcount) {
-        if (f.st.prune)
-          k_zfwd_loop<N, true, C, Epi><<<w_zfwd[pi][1], ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi, f.dcount);
-        else
-          k_zfwd_loop<N, false, C, Epi><<<w_zfwd[pi][0], ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi,
-                                                                             f.dcount);
-        return;
-      }
-    }
     if (f.st.prune)
-      k_zfwd<N, true, C, Epi><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi);
+      k_zfwd<N, true, C, Epi><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi, f.dcount);
     else
-      k_zfwd<N, false, C, Epi><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi);
+      k_zfwd<N, false, C, Epi><<<zgrid(f.st, nitems), ZNT, zs, f.stream>>>(sticks, items, f.st, f.tw, epi, f.dcount);
   }
   static void zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks) {
     zinv_t<float2>(f, src, ld, items, nitems, sticks);

@@ -60,15 +60,29 @@ void fft_plane_drho(const FftArgs& f, const double2* dsticks, const double2* evc
 
 // ---- dense kernels (wb_la.cu) ----
 // part[s][j][r] = sum_{k in split s} W[r*ldw + k] * X[col(j)*ldx + k]
+// Split-K plans of the bra-ket GEMMs, host and device: a graph replay sizes its
+// split grid for the largest plan and every CTA derives the plan of the device
+// column count itself, so both paths split the same count the same way.
+constexpr int kDmmaTile = 32;  // DMMA bra-ket CTA tile (rows and columns)
 // split count of the DMMA bra-ket: about 2 * 148 * ctas_per_sm CTAs (4 warps each)
-int gemm_tn_splits(int M, int ncol, int K, int ctas_per_sm = 2);
+__host__ __device__ inline int gemm_tn_splits(int M, int ncol, int K, int ctas_per_sm = 2) {
+  const int tiles = ((M + kDmmaTile - 1) / kDmmaTile) * ((ncol + kDmmaTile - 1) / kDmmaTile);
+  int ns = (2 * 148 * ctas_per_sm + tiles - 1) / (tiles > 0 ? tiles : 1);
+  const int maxs = (K + 511) / 512;
+  if (ns > maxs) ns = maxs;
+  if (ns < 1) ns = 1;
+  return ns;
+}
+// part doubles for any column count up to nsys and any target up to ctas_max
+size_t gemm_tn_part_doubles(int M, int nsys, int K, int ctas_max);
+// with dn, ctas selects the device plan (nsplit is then ignored)
 void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
-             int nsplit, double* part, cudaStream_t s, const int* dn = nullptr);
+             int nsplit, double* part, cudaStream_t s, const int* dn = nullptr, int ctas = 2);
 // S = 2 sum_s part - W0 X0 (Gamma bra-ket, glbrak.f90:39-40), then
 // C[j][r] = sum_{r'<nkb} D[r][r'] S[j][r'] for r < nkb, alpha S[j][r] otherwise
 void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double* W, long ldw, const double* X,
                   long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s,
-                  const int* dn = nullptr);
+                  const int* dn = nullptr, int K = 0, int ctas = 0);
 // Y[col(j)] = beta Y[col(j)] + W C[j]  over K real rows
 void gemm_nn(const double* W, long ldw, int M, const double* C, double* Y, long ldy, const int* cols, int ncol,
              int K, double beta, cudaStream_t s, const int* dn = nullptr);
@@ -98,6 +112,7 @@ void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cu
 // loop state of the graph-captured PCG loops: int st[8] (wb_la.cu)
 void loop_init(int* st, int nsys, bool reset_totals, cudaStream_t s);
 void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool shared_budget, cudaStream_t s);
+void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int min_items, int nbuckets, cudaStream_t s);
 
 // ---- mixed form: FP32 inner PCG and FP64 refinement (wb_la.cu) ----
 // inner test: rho < max(eta * rel[j], floor)
@@ -118,7 +133,7 @@ void gemm_tn32(const float* W, long ldw, int M, const float* X, long ldx, const 
                float* part, cudaStream_t s, const int* dn = nullptr);
 void gamma_reduce32(const float* part, int nsplit, int M, int ncol, const float* W, long ldw, const float* X, long ldx,
                     const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s,
-                    const int* dn = nullptr);
+                    const int* dn = nullptr, int K = 0, int umma_ctas = 0);
 void gemm_nn32_acc(const float* W, long ldw, int M, const float* C, float* Y, long ldy, const int* cols, int ncol, int K,
                    cudaStream_t s, const int* dn = nullptr);
 
@@ -126,7 +141,19 @@ void gemm_nn32_acc(const float* W, long ldw, int M, const float* C, float* Y, lo
 bool umma_supported(int M);
 int umma_np(int M);
 void umma_setup();
-void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split, int ctas_per_sm = 2);
+__host__ __device__ inline void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split,
+                                                 int ctas_per_sm = 2) {
+  const int nkb = (K + 63) / 64;
+  int tiles = (ncol + 127) / 128;
+  if (tiles < 1) tiles = 1;
+  int target = (ctas_per_sm * 148 + tiles - 1) / tiles;
+  if (target < 1) target = 1;
+  int per = (nkb + target - 1) / target;
+  if (per < 2) per = 2;
+  if (per > nkb) per = nkb;
+  *kb_per_split = per;
+  *nsplit = (nkb + per - 1) / per;
+}
 // part floats for any batch up to nsys and any ctas_per_sm up to kUmmaMaxCtas
 constexpr int kUmmaMaxCtas = 3;
 size_t umma_part_floats(int M, int nsys, int K);

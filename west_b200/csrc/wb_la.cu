@@ -29,13 +29,18 @@ constexpr int TN_W = 4;
 __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict__ W, long ldw, int M,
                                                        const double* __restrict__ X, long ldx,
                                                        const int* __restrict__ cols, int ncol_host, const int* dn,
-                                                       int K, int kchunk, double* __restrict__ part) {
+                                                       int K, int kchunk, int ctas, double* __restrict__ part) {
   __shared__ double red[TN_W][TN_T * TN_T];
   const int ncol = dev_count(dn, ncol_host);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lr = lane >> 2, lk = lane & 3;
   const int r0 = blockIdx.x * TN_T, j0 = blockIdx.y * TN_T, split = blockIdx.z;
   if (j0 >= ncol) return;
+  if (dn) {  // the split plan of this column count
+    const int ns = gemm_tn_splits(M, ncol, K, ctas);
+    if (split >= ns) return;
+    kchunk = ((K + ns - 1) / ns + 15) / 16 * 16;
+  }
   const int kb = split * kchunk, ke = min(K, kb + kchunk);
   const double* arow[4];
   bool aok[4];
@@ -87,33 +92,36 @@ __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict_
   }
 }
 
-int gemm_tn_splits(int M, int ncol, int K, int ctas_per_sm) {
-  const int tiles = ((M + TN_T - 1) / TN_T) * ((ncol + TN_T - 1) / TN_T);
-  int ns = (2 * 148 * ctas_per_sm + tiles - 1) / tiles;
-  const int maxs = (K + 511) / 512;
-  if (ns > maxs) ns = maxs;
-  if (ns < 1) ns = 1;
-  return ns;
+size_t gemm_tn_part_doubles(int M, int nsys, int K, int ctas_max) {
+  size_t best = 0;
+  for (int t = 1; t <= (nsys + TN_T - 1) / TN_T; ++t) {
+    const int n = std::min(nsys, t * TN_T);
+    for (int c = 1; c <= ctas_max; ++c) best = std::max(best, (size_t)gemm_tn_splits(M, n, K, c) * n * M);
+  }
+  return best;
 }
 
 void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
-             int nsplit, double* part, cudaStream_t s, const int* dn) {
+             int nsplit, double* part, cudaStream_t s, const int* dn, int ctas) {
   if (ncol <= 0 || M <= 0) return;
+  if (dn) nsplit = gemm_tn_splits(M, 1, K, ctas);  // grid for the largest plan
   int kchunk = (K + nsplit - 1) / nsplit;
   kchunk = (kchunk + 15) / 16 * 16;
   dim3 grid((M + TN_T - 1) / TN_T, (ncol + TN_T - 1) / TN_T, nsplit);
-  k_gemm_tn<<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, dn, K, kchunk, part);
+  k_gemm_tn<<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, dn, K, kchunk, ctas, part);
 }
 
 __global__ void __launch_bounds__(256) k_gamma_reduce(const double* __restrict__ part, int nsplit, int M,
                                                       int ncol_host, const int* dn, const double* __restrict__ W,
                                                       long ldw, const double* __restrict__ X, long ldx,
                                                       const int* __restrict__ cols, const double* __restrict__ D,
-                                                      int nkb, double alpha, double* __restrict__ C) {
+                                                      int nkb, double alpha, double* __restrict__ C, int K,
+                                                      int ctas) {
   extern __shared__ double S[];
   const int ncol = dev_count(dn, ncol_host);
   const int j = blockIdx.x;
   if (j >= ncol) return;
+  if (dn && ctas > 0) nsplit = gemm_tn_splits(M, ncol, K, ctas);
   const int col = cols ? cols[j] : j;
   const double x0 = X[(long)col * ldx];
   for (int r = threadIdx.x; r < M; r += blockDim.x) {
@@ -136,10 +144,10 @@ __global__ void __launch_bounds__(256) k_gamma_reduce(const double* __restrict__
 
 void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double* W, long ldw, const double* X,
                   long ldx, const int* cols, const double* D, int nkb, double alpha, double* C, cudaStream_t s,
-                  const int* dn) {
+                  const int* dn, int K, int ctas) {
   if (ncol <= 0 || M <= 0) return;
   k_gamma_reduce<<<ncol, 256, sizeof(double) * M, s>>>(part, nsplit, M, ncol, dn, W, ldw, X, ldx, cols, D, nkb,
-                                                        alpha, C);
+                                                        alpha, C, K, ctas);
 }
 
 // ---------------------------------------------------------------------------
@@ -370,9 +378,9 @@ __global__ void __launch_bounds__(256) k_cg_prec_rho(const int* __restrict__ act
   }
 }
 
-// Grid of a per-system launch: one CTA per system, or, with a device count,
-// a fixed grid that strides over the systems.
-static int sys_grid(int nmax, const int* dn) { return dn ? std::min(nmax, 4 * 148) : nmax; }
+// Grid of a per-system launch: one CTA per system; with a device count nmax
+// bounds it (the CTAs beyond the count return at once).
+static int sys_grid(int nmax, const int*) { return nmax; }
 
 void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* iprec, int nocc,
                  double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s,
@@ -652,11 +660,16 @@ __global__ void __launch_bounds__(256) k_gamma_reduce32(const float* __restrict_
                                                         const float* __restrict__ W, long ldw,
                                                         const float* __restrict__ X, long ldx,
                                                         const int* __restrict__ cols, const float* __restrict__ D,
-                                                        int nkb, float alpha, float* __restrict__ C) {
+                                                        int nkb, float alpha, float* __restrict__ C, int K,
+                                                        int umma_ctas) {
   extern __shared__ float Sf[];
   const int ncol = dev_count(dn, ncol_host);
   const int j = blockIdx.x;
   if (j >= ncol) return;
+  if (dn && umma_ctas > 0) {  // the split plan of the tcgen05 bra-ket for this column count
+    int per;
+    umma_braket_plan(ncol, K, &nsplit, &per, umma_ctas);
+  }
   const int col = cols ? cols[j] : j;
   const float x0 = X[(long)col * ldx];
   for (int r = threadIdx.x; r < M; r += blockDim.x) {
@@ -677,10 +690,11 @@ __global__ void __launch_bounds__(256) k_gamma_reduce32(const float* __restrict_
   }
 }
 void gamma_reduce32(const float* part, int nsplit, int M, int ncol, const float* W, long ldw, const float* X, long ldx,
-                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s, const int* dn) {
+                    const int* cols, const float* D, int nkb, float alpha, float* C, cudaStream_t s, const int* dn,
+                    int K, int umma_ctas) {
   if (ncol <= 0 || M <= 0) return;
   k_gamma_reduce32<<<ncol, 256, sizeof(float) * M, s>>>(part, nsplit, M, ncol, dn, W, ldw, X, ldx, cols, D, nkb, alpha,
-                                                        C);
+                                                        C, K, umma_ctas);
 }
 
 // Y[col j][k] += sum_r W[r][k] C[j][r]; tile 128 k x 32 j, r step 16
@@ -787,6 +801,18 @@ __global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* s
 void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool shared_budget,
               cudaStream_t s) {
   k_loop_ctl<<<1, 1, 0, s>>>(h, nact, st, maxiter, shared_budget ? 1 : 0);
+}
+
+// SWITCH value of a pass: the smallest bucket k with min_items << k >= the
+// active band-pair items (last bucket: the workspace capacity).
+__global__ void k_loop_bucket(cudaGraphConditionalHandle h, const int* nact, int min_items, int nbuckets) {
+  const int items = (*nact + 1) / 2;
+  int k = 0;
+  while (k < nbuckets - 1 && (min_items << k) < items) ++k;
+  cudaGraphSetConditional(h, (unsigned)k);
+}
+void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int min_items, int nbuckets, cudaStream_t s) {
+  k_loop_bucket<<<1, 1, 0, s>>>(h, nact, min_items, nbuckets);
 }
 
 __global__ void k_count_unconverged(const unsigned char* __restrict__ conv, int nocc, int mb, int* __restrict__ out) {

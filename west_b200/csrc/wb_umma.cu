@@ -225,6 +225,7 @@ struct BraketArgs {
   float* part;
   int* err;
   const int* dn;  // device count of columns (graph replays) or null
+  int ctas;       // split target of the device plan (with dn)
 };
 
 __host__ __device__ constexpr int braket_stage_bytes(int NP) { return 2 * kTile + NP * 256; }
@@ -243,6 +244,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_braket_umma(BraketArgs a) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int j0 = blockIdx.x * kRows;
   if (j0 >= ncol) return;  // before any TMEM or barrier state
+  if (a.dn) {              // the split plan of this column count
+    int ns;
+    umma_braket_plan(ncol, a.K, &ns, &a.kb_per_split, a.ctas);
+    if ((int)blockIdx.y >= ns) return;
+  }
   const int kb0 = blockIdx.y * a.kb_per_split;
   const int nk = min(a.nkb, kb0 + a.kb_per_split) - kb0;
   const uint32_t ncols = tmem_cols(a.NP);
@@ -501,16 +507,6 @@ bool umma_supported(int M) { return M >= 1 && M <= 256; }
 
 int umma_np(int M) { return (M + 15) / 16 * 16; }
 
-void umma_braket_plan(int ncol, int K, int* nsplit, int* kb_per_split, int ctas_per_sm) {
-  const int nkb = (K + 63) / 64;
-  const int tiles = std::max(1, (ncol + kRows - 1) / kRows);
-  const int target = std::max(1, (ctas_per_sm * 148 + tiles - 1) / tiles);
-  int per = std::max(2, (nkb + target - 1) / target);
-  per = std::min(per, nkb);
-  *kb_per_split = per;
-  *nsplit = (nkb + per - 1) / per;
-}
-
 size_t umma_part_floats(int M, int nsys, int K) {
   size_t best = 0;
   for (int t = 1; t <= (nsys + kRows - 1) / kRows; ++t) {
@@ -557,7 +553,9 @@ int umma_braket(const void* tiles, int M, const float* X, long ldx, const int* c
   a.M = M;
   a.nkb = (K + 63) / 64;
   int nsplit;
-  umma_braket_plan(ncol, K, &nsplit, &a.kb_per_split, std::min(std::max(ctas_per_sm, 1), kUmmaMaxCtas));
+  a.ctas = std::min(std::max(ctas_per_sm, 1), kUmmaMaxCtas);
+  // a device count launches the largest plan's split grid (one column)
+  umma_braket_plan(dn ? 1 : ncol, K, &nsplit, &a.kb_per_split, a.ctas);
   a.part = part;
   a.err = err;
   a.dn = dn;

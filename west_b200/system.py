@@ -194,24 +194,129 @@ def _dense_gamma_hamiltonian(sysd, device="cpu"):
     return H[keep][:, keep]
 
 
+# Real Gamma basis dimension above which the lowest bands come from the
+# iterative solver (the dense eigensolver needs (2 npw)^2 doubles and its
+# 64-bit cuSOLVER path rejects n > 32768).
+DENSE_MAX_DIM = 20000
+
+
+def _fix_signs(evc):
+    # only a sign is free (psi(r) stays real): make the largest real part positive
+    for b in range(evc.shape[1]):
+        k = np.argmax(np.abs(evc[:, b].real))
+        if evc[k, b].real < 0:
+            evc[:, b] *= -1.0
+    return evc
+
+
 def _ground_state(sysd, nbnd, device="cpu"):
     import torch
+    npw = sysd["mill"].shape[0]
+    if 2 * npw - 1 > DENSE_MAX_DIM:
+        return _ground_state_iterative(sysd, nbnd, device=device)
     H = _dense_gamma_hamiltonian(sysd, device=device)
     H = 0.5 * (H + H.T)
     w, v = torch.linalg.eigh(H)
     w = w[:nbnd].cpu().numpy()
     x = v[:, :nbnd].cpu().numpy()
-    npw = sysd["mill"].shape[0]
     evc = np.empty((npw, nbnd), dtype=np.complex128)
     evc[0] = x[0]
     s = 1.0 / math.sqrt(2.0)
     evc[1:] = (x[1:npw] + 1j * x[npw:]) * s
-    # only a sign is free (psi(r) stays real): make the largest real part positive
-    for b in range(nbnd):
-        k = np.argmax(np.abs(evc[:, b].real))
-        if evc[k, b].real < 0:
-            evc[:, b] *= -1.0
-    return w, evc
+    return w, _fix_signs(evc)
+
+
+class _GammaH:
+    """Matrix-free H on the Gamma half sphere (psi(-G) = conj psi(G)): kinetic,
+    local potential through the FFT box (QE invfft unscaled, fwfft with 1/N^3)
+    and Kleinman-Bylander projectors with the Gamma bra-ket 2 Re sum - G0."""
+
+    def __init__(self, sysd, device):
+        import torch
+        nr = sysd["nr"]
+        mill = sysd["mill"]
+        self.nr = nr
+        self.nl = torch.as_tensor(box_index(mill, nr), device=device)
+        self.nlm = torch.as_tensor(box_index(-mill, nr), device=device)
+        self.v = torch.as_tensor(sysd["vrs"].reshape(nr, nr, nr), device=device)
+        self.g2 = torch.as_tensor(sysd["g2kin"], device=device)
+        self.B = torch.as_tensor(sysd["vkb"], device=device)
+        self.D = torch.as_tensor(sysd["deeq"], device=device).to(self.B.dtype)
+        self.chunk = max(1, int(2e9 // (16 * nr ** 3)))   # vectors per FFT batch (about 2 GB of boxes)
+
+    def dot(self, a, b):
+        """Gamma Gram matrix <a_i|b_j> (real)."""
+        import torch
+        return 2.0 * (a.conj().T @ b).real - torch.outer(a[0].conj(), b[0]).real
+
+    def __call__(self, psi):
+        import torch
+        nr = self.nr
+        out = torch.empty_like(psi)
+        for c0 in range(0, psi.shape[1], self.chunk):
+            p = psi[:, c0:c0 + self.chunk]
+            k = p.shape[1]
+            box = torch.zeros((k, nr ** 3), dtype=torch.complex128, device=psi.device)
+            box[:, self.nlm] = p.T.conj()
+            box[:, self.nl] = p.T                       # G = 0: the +G store wins (psi(0) is real)
+            r = torch.fft.ifftn(box.view(k, nr, nr, nr), dim=(1, 2, 3), norm="forward") * self.v
+            g = torch.fft.fftn(r, dim=(1, 2, 3), norm="forward").reshape(k, -1)
+            out[:, c0:c0 + k] = g[:, self.nl].T
+        out += self.g2[:, None] * psi
+        becp = self.dot(self.B, psi)
+        out += self.B @ (self.D @ becp.to(self.B.dtype))
+        out[0].imag.zero_()                             # Im hpsi(G = 0) = 0
+        return out
+
+
+def _ground_state_iterative(sysd, nbnd, device="cpu", tol=1e-9, maxit=500, seed=7):
+    """Lowest nbnd eigenpairs by block LOBPCG on the Gamma half sphere: Rayleigh-Ritz
+    over [X, T R, P] orthonormalised in the Gamma metric, T = 1 / (1 + g2kin) the
+    kinetic preconditioner, stopped when every wanted residual is below tol."""
+    import torch
+    H = _GammaH(sysd, device)
+    npw = sysd["mill"].shape[0]
+    k = nbnd + max(4, nbnd // 8)                        # guard vectors
+    gen = torch.Generator().manual_seed(seed)
+    X = torch.complex(torch.randn(npw, k, generator=gen, dtype=torch.float64),
+                      torch.randn(npw, k, generator=gen, dtype=torch.float64)).to(device)
+    X = X / (1.0 + H.g2[:, None])
+    X[0].imag.zero_()
+    prec = 1.0 / (1.0 + H.g2)
+
+    def ortho(Y):
+        S = H.dot(Y, Y)
+        w, U = torch.linalg.eigh(0.5 * (S + S.T))
+        keep = w > w.max() * 1e-13
+        return Y @ (U[:, keep] / torch.sqrt(w[keep])).to(Y.dtype)
+
+    X = ortho(X)
+    HX = H(X)
+    P = None
+    th = None
+    for _ in range(maxit):
+        A = H.dot(X, HX)
+        th, C = torch.linalg.eigh(0.5 * (A + A.T))
+        C = C.to(X.dtype)
+        X, HX = X @ C, HX @ C
+        R = HX - X * th[None, :].to(X.dtype)
+        rn = torch.sqrt(torch.clamp(torch.diagonal(H.dot(R, R)), min=0.0))
+        if float(rn[:nbnd].max()) < tol:
+            break
+        W = R * prec[:, None]
+        W[0].imag.zero_()
+        Q = ortho(torch.cat([X, W] + ([P] if P is not None else []), 1))
+        HQ = H(Q)
+        A = H.dot(Q, HQ)
+        _, C = torch.linalg.eigh(0.5 * (A + A.T))
+        C = C[:, :k].to(Q.dtype)
+        Xn = Q @ C
+        P = Xn - X @ H.dot(X, Xn).to(X.dtype)
+        X, HX = Xn, HQ @ C
+    w = th[:nbnd].cpu().numpy()
+    evc = X[:, :nbnd].cpu().numpy().astype(np.complex128)
+    evc[0] = evc[0].real
+    return w, _fix_signs(evc)
 
 
 def build_system(spec: SystemSpec | str, device: Optional[str] = None) -> GammaSystem:
