@@ -628,8 +628,9 @@ void loop_stats(wb_ctx* c, int passes, int launches_per_pass) {
 
 // Solves (H - e_v + alpha Pv) x_v = b_v for all systems of the batch by FP64
 // iterative refinement: FP64 residual r = b - A x, the reference's test
-// <r|M^-1 r> < tr2, then an FP32 masked PCG for A d = r (restarted from d = 0)
-// and x += d in FP64.  X holds the initial guess on entry
+// <r|M^-1 r> < tr2, then an FP32 masked PCG for A d = r (restarted from d = 0,
+// at most n_dfpt_maxiter passes like the reference's PCG) and x += d in FP64;
+// at most kMaxRefinements residuals.  X holds the initial guess on entry
 // (dfpt_module.f90:348) and the solution on exit.
 int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
   cudaStream_t s = c->stream;
@@ -691,13 +692,12 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     WB_CU(cudaMemcpyAsync(cin, conv, nsys, cudaMemcpyDeviceToDevice, s));
     cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), graph ? nullptr : c->nact_host, s);
     int nin = nact;
-    // each refinement restarts the FP32 PCG from d = 0 on the FP64 residual;
-    // the refinements share the n_dfpt_maxiter budget
-    if (graph && inner_total < c->maxiter) {
+    // each refinement restarts the FP32 PCG from d = 0 on the FP64 residual
+    if (graph && c->maxiter > 0) {
       loop_init(st, nsys, false, s);
       WB_CU(cudaGraphLaunch(c->loop32.exec, s));
     }
-    for (int it = 1; !graph && inner_total < c->maxiter; ++it) {
+    for (int it = 1; !graph && it <= c->maxiter; ++it) {
       {
         Stage g(c, WB_STAGE_CG, 2, nin);
         // stop at rho < max(1e-10 rho_outer, tr2): the first correction from x0 is the

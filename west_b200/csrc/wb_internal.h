@@ -111,7 +111,7 @@ void cg_update(const int* act, int nact, double2* x, double2* g, const double2* 
 void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cudaStream_t s);
 // loop state of the graph-captured PCG loops: int st[8] (wb_la.cu)
 void loop_init(int* st, int nsys, bool reset_totals, cudaStream_t s);
-void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool shared_budget, cudaStream_t s);
+void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool inner, cudaStream_t s);
 void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int min_items, int nbuckets, cudaStream_t s);
 
 // ---- mixed form: FP32 inner PCG and FP64 refinement (wb_la.cu) ----

@@ -775,32 +775,27 @@ void loop_init(int* st, int nsys, bool reset_totals, cudaStream_t s) {
   k_loop_init<<<1, 1, 0, s>>>(st, nsys, reset_totals ? 1 : 0);
 }
 
-// End of one PCG pass.  FP64 form (shared_budget = 0): linsolve's loop over
-// iter = 1..n_dfpt_maxiter, leaving when no system is active
-// (linsolve_sternheimer_m_wfcts.f90:146,222).  Mixed form: the inner passes of
-// all refinements share n_dfpt_maxiter.  Sets the WHILE condition of the graph.
-__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, int shared_budget) {
+// End of one PCG pass: linsolve's loop over iter = 1..n_dfpt_maxiter, leaving
+// when no system is active (linsolve_sternheimer_m_wfcts.f90:146,222); every
+// FP32 correction solve of the mixed form is bounded the same way (inner = 1
+// also counts its passes over all refinements in st[3]).  Sets the WHILE
+// condition of the graph.
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, int inner) {
   const int n = *nact, it = st[1];
   long long* sum = reinterpret_cast<long long*>(st + 4);
   long long* boxes = reinterpret_cast<long long*>(st + 6);
-  bool more;
   if (n > 0) {
     *sum += n;
     *boxes += 2 * ((n + 1) / 2);
+    if (inner) st[3] += 1;
   }
-  if (!shared_budget) {
-    st[2] = it;
-    more = n > 0 && it < maxiter;
-  } else {
-    if (n > 0) st[3] += 1;
-    more = n > 0 && st[3] < maxiter;
-  }
+  if (!inner) st[2] = it;
+  const bool more = n > 0 && it < maxiter;
   if (more) st[1] = it + 1;
   cudaGraphSetConditional(h, more ? 1u : 0u);
 }
-void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool shared_budget,
-              cudaStream_t s) {
-  k_loop_ctl<<<1, 1, 0, s>>>(h, nact, st, maxiter, shared_budget ? 1 : 0);
+void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool inner, cudaStream_t s) {
+  k_loop_ctl<<<1, 1, 0, s>>>(h, nact, st, maxiter, inner ? 1 : 0);
 }
 
 // SWITCH value of a pass: the smallest bucket k with min_items << k >= the
