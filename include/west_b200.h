@@ -211,6 +211,7 @@ typedef struct wb_davidson_info {
   int apply_calls;          /* apply_operator calls                             */
   long long perturbations;  /* columns pushed through apply_operator            */
   double seconds;           /* wall time of the solve                           */
+  double seconds_apply;     /* of which inside apply_operator                   */
 } wb_davidson_info;
 
 /*

@@ -23,6 +23,28 @@ template <> WB_DEV float2 mkc<float2>(float x, float y) { return make_float2(x, 
 
 template <class C> WB_DEV C cadd(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
 template <class C> WB_DEV C csub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
+// FP32 complex add and subtract as one paired instruction (sm_100 f32x2; same
+// rounding as two scalar adds)
+WB_DEV unsigned long long f2_bits(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+WB_DEV float2 bits_f2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+template <> WB_DEV float2 cadd<float2>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(r);
+}
+template <> WB_DEV float2 csub<float2>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return bits_f2(r);
+}
 template <class C> WB_DEV C cmul(C a, C b) {
   return mkc<C>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }

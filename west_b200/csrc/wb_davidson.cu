@@ -223,11 +223,14 @@ struct Dav {
     WB_CU(cudaGetLastError());
     return WB_OK;
   }
+  double apply_s = 0.0;
   int apply(int col0, int n, double tr2) {
     unconv.assign(std::max(n, 1), 0);
+    const auto t0 = std::chrono::steady_clock::now();
     const int rc = wb_apply_operator_device(c, n, reinterpret_cast<const double*>(dvg + (long)col0 * ld), (int)ld,
                                             reinterpret_cast<double*>(dng + (long)col0 * ld), (int)ld, tr2, 1,
                                             unconv.data());
+    apply_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     ++apply_calls;
     applied += n;
     return rc;
@@ -384,6 +387,7 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
     info->apply_calls = d.apply_calls;
     info->perturbations = d.applied;
     info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    info->seconds_apply = d.apply_s;
   }
   return WB_OK;
 }

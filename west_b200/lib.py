@@ -62,7 +62,7 @@ class WbDavidsonParams(ctypes.Structure):
 
 class WbDavidsonInfo(ctypes.Structure):
     _fields_ = [("dav_iter", _i), ("notcnv", _i), ("converged", _i), ("apply_calls", _i),
-                ("perturbations", ctypes.c_longlong), ("seconds", _d)]
+                ("perturbations", ctypes.c_longlong), ("seconds", _d), ("seconds_apply", _d)]
 
 
 class WbTuning(ctypes.Structure):
