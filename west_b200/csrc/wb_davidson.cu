@@ -93,15 +93,25 @@ __global__ void k_mgs_axpy(double2* __restrict__ a, long ld, int npw, int k, int
 // Cyclic two-sided Jacobi on the upper triangle of hr[:n, :n] (what DSYEV 'U'
 // reads in matdiago_dsy, Tools/linear_algebra_kernel.f90:84), round-robin
 // ordering so each round rotates n/2 disjoint (p, q) planes in parallel.
-// One CTA; A and V row-major in global scratch.  Writes the nsel lowest
-// eigenvalues to w and their eigenvectors to vr(:, 0:nsel) (ld ldv).
+// One CTA; A and V row-major in shared memory when in_smem (n <= kJacobiSmemN),
+// else in global scratch.  Writes the nsel lowest eigenvalues to w and their
+// eigenvectors to vr(:, 0:nsel) (ld ldv).
+constexpr int kJacobiSmemN = 112;  // 2 n^2 doubles + pair tables within 227 KB
+
+__host__ __device__ inline size_t jacobi_pairs_bytes(int n) {
+  const int ne = n + (n & 1);
+  return ((size_t)(ne / 2) * (2 * sizeof(double) + 2 * sizeof(int)) + sizeof(int) * n + 15) / 16 * 16;
+}
+
 __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ hr, long ldh, int n,
-                                                 double* __restrict__ A, double* __restrict__ V,
+                                                 double* __restrict__ Ag, double* __restrict__ Vg,
                                                  int nsel, double* __restrict__ w, double* __restrict__ vr,
-                                                 long ldv, int* __restrict__ sweeps_out) {
-  extern __shared__ unsigned char shm[];
+                                                 long ldv, int* __restrict__ sweeps_out, int in_smem) {
+  extern __shared__ __align__(16) unsigned char shm[];
   const int ne = n + (n & 1);
   const int npairs = ne / 2;
+  double* A = in_smem ? reinterpret_cast<double*>(shm + jacobi_pairs_bytes(n)) : Ag;
+  double* V = in_smem ? A + (size_t)n * n : Vg;
   double* cs = reinterpret_cast<double*>(shm);           // [npairs] cos
   double* sn = cs + npairs;                                // [npairs] sin
   int* pp = reinterpret_cast<int*>(sn + npairs);           // [npairs]
@@ -212,10 +222,26 @@ struct Dav {
   long long applied = 0;
   std::vector<int> unconv;
 
-  int mgs(int start, int end) {  // do_mgs on columns [start, end)
-    for (int k = 0; k < end; ++k) {
-      if (k >= start) k_mgs_normalize<<<1, 256, 0, s>>>(dvg + (long)k * ld, npw);
-      const int j0 = std::max(k + 1, start);
+  // do_mgs on columns [start, end) (davidson_diago.f90:909): the columns before
+  // start are orthonormal, so the new block is first projected against all of
+  // them at once, twice (classical Gram-Schmidt with reorthogonalisation: the
+  // Gamma bra-ket GEMM and the update GEMM), then orthonormalised column by
+  // column inside the block.  Same result as the reference's column order up
+  // to rounding; two GEMM passes instead of two launches per old column.
+  int mgs(int start, int end) {
+    if (start > 0 && end > start) {
+      const int K = 2 * npw, nb = end - start;
+      const double* B = reinterpret_cast<const double*>(dvg);
+      double* X = reinterpret_cast<double*>(dvg + (long)start * ld);
+      for (int pass = 0; pass < 2; ++pass) {
+        gemm_tn(B, 2 * ld, start, X, 2 * ld, nullptr, nb, K, nsplit, part, s);
+        gamma_reduce(part, nsplit, start, nb, B, 2 * ld, X, 2 * ld, nullptr, nullptr, 0, -1.0, coef, s);
+        gemm_nn(B, 2 * ld, start, coef, X, 2 * ld, nullptr, nb, K, 1.0, s);
+      }
+    }
+    for (int k = start; k < end; ++k) {
+      k_mgs_normalize<<<1, 256, 0, s>>>(dvg + (long)k * ld, npw);
+      const int j0 = k + 1;
       if (j0 >= end) continue;
       k_mgs_dots<<<end - j0, 256, 0, s>>>(dvg, ld, npw, k, j0, dots);
       k_mgs_axpy<<<dim3((npw + 255) / 256, end - j0), 256, 0, s>>>(dvg, ld, npw, k, j0, dots);
@@ -245,9 +271,9 @@ struct Dav {
     return WB_OK;
   }
   int diagox(int nbase, std::vector<double>& ew_host) {  // lowest nvec eigenpairs of hr[:nbase, :nbase]
-    const int ne = nbase + (nbase & 1);
-    const size_t shm = (size_t)(ne / 2) * (2 * sizeof(double) + 2 * sizeof(int)) + sizeof(int) * nbase + 16;
-    k_jacobi<<<1, 1024, shm, s>>>(hr, nvecx, nbase, A, V, nvec, w, vr, nvecx, sweeps);
+    const int in_smem = nbase <= kJacobiSmemN ? 1 : 0;
+    const size_t shm = jacobi_pairs_bytes(nbase) + (in_smem ? 2 * sizeof(double) * nbase * nbase : 0);
+    k_jacobi<<<1, 1024, shm, s>>>(hr, nvecx, nbase, A, V, nvec, w, vr, nvecx, sweeps, in_smem);
     WB_CU(cudaGetLastError());
     WB_CU(cudaMemcpyAsync(ew_host.data(), w, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
     WB_CU(cudaStreamSynchronize(s));
@@ -278,6 +304,9 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
   if (ld_dvg0 < c->npw || (pdep && ld_pdep < c->npw)) return fail(WB_ERR_ARG, "leading dimension smaller than npw");
   const auto t0 = std::chrono::steady_clock::now();
   WB_CU(cudaSetDevice(c->device));
+  WB_CU(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(jacobi_pairs_bytes(kJacobiSmemN) +
+                                   2 * sizeof(double) * kJacobiSmemN * kJacobiSmemN)));
   Dav d;
   d.c = c;
   d.npw = c->npw;
