@@ -34,6 +34,68 @@ int fail(int code, const std::string& msg) {
 
 namespace {
 
+// Numbering of the stick pairs (pair 0 is (0,0)).  The plane kernels scatter
+// and gather stick s of a plane from thread s % 256 of the CTA, so the order
+// decides which plane offsets one warp instruction touches.  Pairs are taken
+// in (y, x) order, each time the first one whose two sticks land on shared-
+// memory bank slots not yet used by the current half-warp (8-byte elements,
+// offset mod 16) and quarter-warp (16-byte elements, offset mod 8); when none
+// fits, the next in order.
+std::vector<std::pair<int, int>> stick_pair_order(int N, int prune, const std::map<std::pair<int, int>, int>& pairs) {
+  const int nsp = (int)pairs.size();
+  wb::StickTab shape{};
+  shape.prune = prune;
+  shape.nst = 2 * nsp;
+  const bool fused = wb::fft_fusable(N, shape);
+  std::vector<std::pair<int, int>> rest;
+  for (auto& kv : pairs)
+    if (kv.first.first != 0 || kv.first.second != 0) rest.push_back(kv.first);
+  std::stable_sort(rest.begin(), rest.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+    return a.second != b.second ? a.second < b.second : a.first < b.first;
+  });
+  auto slots = [&](int x, int y, int& s16, int& s8) {
+    s16 = wb::fft_plane_offset(N, fused, 8, (x + N) % N, (y + N) % N) % 16;
+    s8 = wb::fft_plane_offset(N, fused, 16, (x + N) % N, (y + N) % N) % 8;
+  };
+  std::vector<std::pair<int, int>> order;
+  order.reserve(nsp);
+  order.push_back({0, 0});
+  unsigned used16 = 0, used8 = 0;
+  {
+    int a16, a8;
+    slots(0, 0, a16, a8);
+    used16 = 1u << a16;
+    used8 = 1u << a8;
+  }
+  std::vector<char> taken(rest.size(), 0);
+  size_t first = 0;
+  for (size_t n = 0; n < rest.size(); ++n) {
+    const int lane = 2 * (int)order.size();
+    if (lane % 16 == 0) used16 = 0;
+    if (lane % 8 == 0) used8 = 0;
+    while (taken[first]) ++first;
+    size_t pick = first;
+    int p16 = 0, p8 = 0, m16 = 0, m8 = 0;
+    for (size_t i = first; i < rest.size(); ++i) {
+      if (taken[i]) continue;
+      int a16, a8, b16, b8;
+      slots(rest[i].first, rest[i].second, a16, a8);
+      slots(-rest[i].first, -rest[i].second, b16, b8);
+      if (i == first) { p16 = a16; p8 = a8; m16 = b16; m8 = b8; }
+      if (a16 != b16 && a8 != b8 && !(used16 >> a16 & 1) && !(used16 >> b16 & 1) && !(used8 >> a8 & 1) &&
+          !(used8 >> b8 & 1)) {
+        pick = i; p16 = a16; p8 = a8; m16 = b16; m8 = b8;
+        break;
+      }
+    }
+    taken[pick] = 1;
+    used16 |= (1u << p16) | (1u << m16);
+    used8 |= (1u << p8) | (1u << m8);
+    order.push_back(rest[pick]);
+  }
+  return order;
+}
+
 int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
   const int N = s->nr1, npw = s->npw;
   struct GInfo { int mx, my, mz, ref; };
@@ -69,16 +131,12 @@ int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
     if (cx == 0 && cy == 0) continue;
     pairs.emplace(std::make_pair(cx, cy), 0);
   }
-  int q = 1;
-  std::vector<std::pair<int, int>> pair_xy(pairs.size());
-  pair_xy[0] = {0, 0};
-  for (auto& kv : pairs) {
-    if (kv.first.first == 0 && kv.first.second == 0) continue;
-    kv.second = q;
-    pair_xy[q] = kv.first;
-    ++q;
-  }
   const int nsp = (int)pairs.size();
+  int mmax = 0;
+  for (auto& g : gi) mmax = std::max({mmax, std::abs(g.mx), std::abs(g.my), std::abs(g.mz)});
+  const int prune = (4 * mmax < N && N % 4 == 0) ? 1 : 0;
+  std::vector<std::pair<int, int>> pair_xy = stick_pair_order(N, prune, pairs);
+  for (int p = 1; p < nsp; ++p) pairs[pair_xy[p]] = p;
   std::vector<int> gq(npw), gside(npw);
   int xmax = 0;
   for (int i = 0; i < npw; ++i) {
@@ -127,9 +185,7 @@ int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
   c->st.st_pos = c->stpos.as<int>();
   c->st.xhi = xmax;
   c->st.ncols = 2 * xmax + 1;
-  int mmax = 0;
-  for (auto& g : gi) mmax = std::max({mmax, std::abs(g.mx), std::abs(g.my), std::abs(g.mz)});
-  c->st.prune = (4 * mmax < N && N % 4 == 0) ? 1 : 0;
+  c->st.prune = prune;
   if (c->st.prune) {
     // pruned transforms read every x in the outer quarters, so those columns
     // are the active set (they are all zero-filled and transformed)

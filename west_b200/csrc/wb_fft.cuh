@@ -52,6 +52,20 @@ template <> struct Factor2<10> { static constexpr int A = 5, B = 2; };
 template <> struct Factor2<12> { static constexpr int A = 4, B = 3; };
 template <> struct Factor2<16> { static constexpr int A = 4, B = 4; };
 
+constexpr double kR2 = 0.70710678118654752440;   // sqrt(1/2)
+
+// a * exp(DIR 2 pi i j / 8) for j = 1, 2, 3 (the inner twiddles of the radix-8
+// DFT), from the exact forms (1 + i)/sqrt(2), i, (-1 + i)/sqrt(2)
+template <int DIR, class C>
+WB_DEV C tw8(C a, int j) {
+  using T = real_t<C>;
+  const T c = T(kR2);
+  if (j == 2) return cmul_i<DIR>(a);
+  const T s = a.x + a.y, d = a.x - a.y;
+  if (j == 1) return DIR > 0 ? mkc<C>(c * d, c * s) : mkc<C>(c * s, -c * d);
+  return DIR > 0 ? mkc<C>(-c * s, c * d) : mkc<C>(-c * d, -c * s);
+}
+
 // In-register DFT of size R: v[k] <- sum_n v[n] exp(DIR 2 pi i n k / R).
 // NT is the length of the shared twiddle table twN (R divides NT).  C is
 // double2 or float2.
@@ -103,7 +117,10 @@ WB_DEV void rdft(C* v, const C* twN) {
       rdft<A, DIR, NT>(z[b], twN);
 #pragma unroll
       for (int k1 = 1; k1 < A; ++k1)
-        if (b > 0) z[b][k1] = ctw<DIR>(z[b][k1], twN[((b * k1) * (NT / R)) % NT]);
+        if (b > 0) {
+          if constexpr (R == 8) z[b][k1] = tw8<DIR>(z[b][k1], k1);
+          else z[b][k1] = ctw<DIR>(z[b][k1], twN[((b * k1) * (NT / R)) % NT]);
+        }
     }
 #pragma unroll
     for (int k1 = 0; k1 < A; ++k1) {
@@ -120,13 +137,14 @@ WB_DEV void rdft(C* v, const C* twN) {
 // Element layout of one line in shared memory.  Element e = N2*a + b is stored
 // at (N2 + PAD)*a + b: with an odd block length, the N1 threads of step 2 (which
 // read elements N2*k1 + n2) hit distinct banks, as do the N2 threads of step 1.
+#define WB_HD __host__ __device__ __forceinline__
 template <int N>
 struct LinePad {
   static constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
   static constexpr int PAD = (N2 % 2 == 0) ? 1 : 0;
   static constexpr int LEN = N1 * (N2 + PAD);  // stored length of a line
-  WB_DEV static int off(int e) { return (e / N2) * (N2 + PAD) + (e % N2); }
-  WB_DEV static int off_blk(int a, int b) { return (N2 + PAD) * a + b; }
+  WB_HD static int off(int e) { return (e / N2) * (N2 + PAD) + (e % N2); }
+  WB_HD static int off_blk(int a, int b) { return (N2 + PAD) * a + b; }
 };
 
 // Pruning for lines whose nonzero inputs (inverse) or needed outputs
@@ -233,9 +251,32 @@ template <int N>
 struct Plane {
   static constexpr int RS = LinePad<N>::LEN;
   static constexpr int SIZE = N * RS;
-  WB_DEV static int at(int x, int y) { return y * RS + LinePad<N>::off(x); }
+  WB_HD static int row(int y) { return y * RS; }
+  WB_HD static int at(int x, int y) { return y * RS + LinePad<N>::off(x); }
   // plane offset of the e-th element in row-major (y*N + x) order
-  WB_DEV static int at_lin(int e) { return at(e % N, e / N); }
+  WB_HD static int at_lin(int e) { return at(e % N, e / N); }
+};
+
+// Plane of the fused local-potential kernel.  For N = 8 x 8 with 8-byte
+// elements (FP32 complex) every group of 8 rows is shifted by GP = 8 more
+// elements.  A half-warp of 8-byte accesses covers 16 bank slots (offset mod
+// 16); the row stride 72 puts rows y and y+1 eight slots apart, and the group
+// shift does the same for rows y and y+8, so the column passes can give each
+// half-warp one aligned block of 8 columns in two rows 1 or 8 apart without a
+// conflict (16-byte elements are served per quarter-warp, one row, and need
+// no shift).
+template <int N, class C>
+struct FPlane {
+  static constexpr int R = FftSplit<N>::N1;
+  static constexpr int RS = LinePad<N>::LEN;
+  static constexpr int GP = (sizeof(C) == 8 && R == 8 && FftSplit<N>::N2 == 8) ? 8 : 0;
+  static constexpr int GS = R * RS + GP;  // stride between groups of R rows
+  static constexpr int SIZE = N * RS + (N / R) * GP;
+  // row y = R * a + b with b in [0, R)
+  WB_HD static int row2(int a, int b) { return a * GS + b * RS; }
+  WB_HD static int row(int y) { return row2(y / R, y % R); }
+  WB_HD static int at(int x, int y) { return row(y) + LinePad<N>::off(x); }
+  WB_HD static int at_lin(int e) { return at(e % N, e / N); }
 };
 
 }  // namespace wb

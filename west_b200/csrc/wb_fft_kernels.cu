@@ -213,7 +213,7 @@ struct EpiDng {
 // Zero what the inverse transforms read: with pruning (PR) only the active
 // columns (which then are all x in [0, N/4) u [3N/4, N)) at live rows (y in
 // the same quarters), otherwise the whole plane.
-template <int N, bool PR, class C>
+template <int N, bool PR, class C, class PL = Plane<N>>
 WB_DEV void plane_zero(C* pl, const StickTab& st) {
   if constexpr (PR && Prune<N>::IN_OK) {
     constexpr int NL = 2 * (N / 4);
@@ -222,25 +222,25 @@ WB_DEV void plane_zero(C* pl, const StickTab& st) {
       const int l = e % nc, r = e / nc;
       const int x = l < nlow ? l : N - nc + l;
       const int y = r < N / 4 ? r : N - NL + r;
-      pl[Plane<N>::at(x, y)] = mkc<C>(0, 0);
+      pl[PL::at(x, y)] = mkc<C>(0, 0);
     }
   } else {
-    for (int e = threadIdx.x; e < Plane<N>::SIZE; e += PNT) pl[e] = mkc<C>(0, 0);
+    for (int e = threadIdx.x; e < PL::SIZE; e += PNT) pl[e] = mkc<C>(0, 0);
   }
 }
 // stick positions are y*N + x in row-major plane order
-template <int N, class C>
+template <int N, class C, class PL = Plane<N>>
 WB_DEV void plane_scatter(C* pl, const C* __restrict__ sz, const int* __restrict__ pos, int nst) {
   for (int s = threadIdx.x; s < nst; s += PNT) {
     const int p = pos[s];
-    if (p >= 0) pl[Plane<N>::at_lin(p)] = sz[s];
+    if (p >= 0) pl[PL::at_lin(p)] = sz[s];
   }
 }
-template <int N, class C>
+template <int N, class C, class PL = Plane<N>>
 WB_DEV void plane_gather(const C* pl, C* __restrict__ sz, const int* __restrict__ pos, int nst) {
   for (int s = threadIdx.x; s < nst; s += PNT) {
     const int p = pos[s];
-    sz[s] = p >= 0 ? pl[Plane<N>::at_lin(p)] : mkc<C>(0, 0);
+    sz[s] = p >= 0 ? pl[PL::at_lin(p)] : mkc<C>(0, 0);
   }
 }
 // inverse transforms prune inputs, forward transforms prune outputs
@@ -398,21 +398,70 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
 // V(r)/N^3 product and the forward-row first step run in registers of one
 // thread (the outputs X[k1 + R k2] of the inverse are exactly the inputs
 // x[R n1 + k1] of the forward step for n1 = k2), saving a shared-memory round
-// trip of the whole plane.  The plane's sticks and V values are loaded into
-// registers before the zero fill so their latency overlaps it.
+// trip of the whole plane.  The plane's sticks are loaded into registers
+// before the zero fill so their latency overlaps it.  The plane uses the
+// FPlane layout; the row threads keep their step-1 twiddles W^(q n2) in
+// registers (every row item of a thread has the same n2 = tid % R).
 constexpr int kFusedMaxSticksPerThread = 4;
 
-// LOAD_TW: load the twiddles into tw after the stick loads are issued (one-unit kernels);
-// PRELOAD: issue the stick loads into registers before zeroing the plane (one-unit
-// kernels; a unit called in a loop scatters straight from global memory)
-template <int N, class C, bool LOAD_TW = false, bool PRELOAD = true>
+template <int N, class C>
+struct OffFRows {
+  WB_DEV int operator()(int l) const { return FPlane<N, C>::row(l); }
+};
+
+// Column transforms of the fused plane.  For N = 64 (pruned: 32 active columns
+// in the four aligned blocks x in [0,16) u [48,64)) thread t takes column
+// 8 ((t / 16) % 4) + t % 8 of the active set and sub = 2 (t / 64) + (t / 8) % 2
+// as its n2 (step 1) and k1 (step 2): a half-warp then covers one block of 8
+// columns in two rows 1 (steps 1 and 2-out) or 8 (step 2-in) apart, which
+// FPlane puts in disjoint bank slots.
+template <int N, int DIR, int P, class C>
+WB_DEV void fused_cols(C* pl, const StickTab& st, const C* tw) {
+  using FP = FPlane<N, C>;
+  if constexpr (N == 64 && PNT == 256) {
+    constexpr int R = 8;
+    using PR = Prune<N>;
+    constexpr bool PIN = P == PRUNE_IN, POUT = P == PRUNE_OUT;
+    const int tid = threadIdx.x;
+    const int l = 8 * ((tid >> 4) & 3) + (tid & 7);
+    const int x = l < 16 ? l : 32 + l;
+    const int sub = 2 * (tid >> 6) + ((tid >> 3) & 1);
+    C* p = pl + LinePad<N>::off(x);
+    C v[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1)
+      v[n1] = (PIN && !PR::in_live(n1)) ? mkc<C>(0, 0) : p[FP::row2(n1, sub)];
+    rdft<R, DIR, N>(v, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) v[k1] = ctw<DIR>(v[k1], tw[N + k1 * R + sub]);
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) p[FP::row2(k1, sub)] = v[k1];
+    __syncthreads();
+#pragma unroll
+    for (int n2 = 0; n2 < R; ++n2) v[n2] = p[FP::row2(sub, n2)];
+    rdft<R, DIR, N>(v, tw);
+    __syncthreads();
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2)
+      if (!POUT || PR::out_live(k2)) p[FP::row2(k2, sub)] = v[k2];
+    __syncthreads();
+  } else {
+    static_assert(FP::GP == 0, "grouped plane rows need the N = 64 column mapping");
+    fft_lines<N, DIR, PNT, true, false, P>(pl, OffCols<N>{st.xhi + 1, st.ncols}, FP::RS, st.ncols, tw);
+  }
+}
+
+template <int N, class C, bool TWR>
 WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, const real_t<C>* __restrict__ vs, int z,
-                                  int item, const C* __restrict__ twg = nullptr) {
+                                  int item, const C* __restrict__ twg) {
   C* tw = smem_tw<C>();
   C* pl = smem_tw<C>() + 2 * N;
   using T = real_t<C>;
+  using FP = FPlane<N, C>;
+  using PR = Prune<N>;
   constexpr int R = FftSplit<N>::N1;
   static_assert(FftSplit<N>::N1 == FftSplit<N>::N2, "fused rows need N1 == N2");
+  static_assert(PNT % R == 0, "row threads keep one n2");
   constexpr int LPC = PNT / R;
   constexpr int NCH = (N + LPC - 1) / LPC;
   constexpr int MS = kFusedMaxSticksPerThread;
@@ -421,36 +470,47 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
   C* sz = sticks + ((long)item * N + z) * st.nst;
   C sv[MS];
   int sp[MS];
-  if constexpr (PRELOAD) {
 #pragma unroll
-    for (int i = 0; i < MS; ++i) {
-      const int s = tid + i * PNT;
-      sp[i] = -1;
-      if (s < st.nst) { sp[i] = st.st_pos[s]; sv[i] = sz[s]; }
-    }
+  for (int i = 0; i < MS; ++i) {
+    const int s = tid + i * PNT;
+    sp[i] = -1;
+    if (s < st.nst) { sp[i] = st.st_pos[s]; sv[i] = sz[s]; }
   }
   const int k1 = tid % R;
   const bool rowthr = tid < LPC * R;
   const T* vz = vs + (long)z * N * N;
-  if constexpr (LOAD_TW) load_tw<N>(tw, twg);
-  plane_zero<N, true>(pl, st);
+  load_tw<N>(tw, twg);
+  plane_zero<N, true, C, FP>(pl, st);
   __syncthreads();
-  if constexpr (PRELOAD) {
 #pragma unroll
-    for (int i = 0; i < MS; ++i)
-      if (sp[i] >= 0) pl[Plane<N>::at_lin(sp[i])] = sv[i];
-  } else {
-    plane_scatter<N>(pl, sz, st.st_pos, st.nst);
+  for (int i = 0; i < MS; ++i)
+    if (sp[i] >= 0) pl[FP::at_lin(sp[i])] = sv[i];
+  C wr[R];
+  if constexpr (TWR) {
+#pragma unroll
+    for (int q = 1; q < R; ++q) wr[q] = tw[N + q * R + k1];
   }
   __syncthreads();
-  plane_fft_cols<N, +1, true>(pl, st, tw);
-  fft_step1<N, +1, PNT, false, true, PRUNE_IN>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
+  fused_cols<N, +1, PRUNE_IN, C>(pl, st, tw);
+  // inverse rows, step 1 (pruned input): row y = it / R, n2 = it % R = k1
+  for (int it = tid; it < N * R; it += PNT) {
+    C* p = pl + FP::row(it / R);
+    C v[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1)
+      v[n1] = (PR::IN_OK && !PR::in_live(n1)) ? mkc<C>(0, 0) : p[LP::off_blk(n1, k1)];
+    rdft<R, +1, N>(v, tw);
+#pragma unroll
+    for (int q = 1; q < R; ++q) v[q] = ctw<+1>(v[q], TWR ? wr[q] : tw[N + q * R + k1]);
+#pragma unroll
+    for (int q = 0; q < R; ++q) p[LP::off_blk(q, k1)] = v[q];
+  }
   __syncthreads();
 #pragma unroll
   for (int c = 0; c < NCH; ++c) {
     const int y = c * LPC + tid / R;
     const bool act = rowthr && y < N;
-    C* p = pl + (act ? y : 0) * Plane<N>::RS;
+    C* p = pl + FP::row(act ? y : 0);
     C v[R];
     if (act) {
       T vr[R];                                      // V(r) of this row, loaded here to keep registers free
@@ -463,7 +523,7 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
       for (int k2 = 0; k2 < R; ++k2) v[k2] = cscale(v[k2], vr[k2]);
       rdft<R, -1, N>(v, tw);                        // forward step 1 over n1 = k2, thread n2 = k1
 #pragma unroll
-      for (int q = 1; q < R; ++q) v[q] = ctw<-1>(v[q], tw[N + q * R + k1]);
+      for (int q = 1; q < R; ++q) v[q] = ctw<-1>(v[q], TWR ? wr[q] : tw[N + q * R + k1]);
     }
     __syncthreads();
     if (act) {
@@ -472,9 +532,9 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
     }
   }
   __syncthreads();
-  fft_step2<N, -1, PNT, false, true, PRUNE_OUT>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
-  plane_fft_cols<N, -1, true>(pl, st, tw);
-  plane_gather<N>(pl, sz, st.st_pos, st.nst);
+  fft_step2<N, -1, PNT, false, true, PRUNE_OUT>(pl, OffFRows<N, C>{}, 1, N, tw);
+  fused_cols<N, -1, PRUNE_OUT, C>(pl, st, tw);
+  plane_gather<N, C, FP>(pl, sz, st.st_pos, st.nst);
 }
 
 template <int N, class C>
@@ -482,7 +542,7 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
                                                              const real_t<C>* __restrict__ vs,
                                                              const C* __restrict__ twg, const int* dn) {
   if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;
-  plane_vloc_fused_unit<N, C, true>(sticks, st, vs, blockIdx.x, blockIdx.y, twg);
+  plane_vloc_fused_unit<N, C, sizeof(C) == 8>(sticks, st, vs, blockIdx.x, blockIdx.y, twg);
 }
 
 // ---------------------------------------------------------------------------
@@ -492,6 +552,8 @@ template <int N, class C = double2>
 static constexpr size_t zsmem() { return sizeof(C) * (2 * N + 2 * ZSG * (LinePad<N>::LEN | 1)); }
 template <int N, class C = double2>
 static constexpr size_t psmem() { return sizeof(C) * (2 * N + Plane<N>::SIZE); }
+template <int N, class C>
+static constexpr size_t fsmem() { return sizeof(C) * (2 * N + FPlane<N, C>::SIZE); }
 
 template <int N>
 struct FftN {
@@ -511,9 +573,10 @@ struct FftN {
     setup_pr<false>();
     setup_pr<true>();
     if constexpr (FUSABLE) {
-      cudaFuncSetAttribute(k_plane_vloc_fused<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem<N>());
+      cudaFuncSetAttribute(k_plane_vloc_fused<N, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)fsmem<N, double2>());
       cudaFuncSetAttribute(k_plane_vloc_fused<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)psmem<N, float2>());
+                           (int)fsmem<N, float2>());
     }
     for (int pr = 0; pr < 2; ++pr) {
       auto zi = pr ? k_zinv<N, true, float2> : k_zinv<N, false, float2>;
@@ -551,7 +614,7 @@ struct FftN {
     const dim3 g(N, nitems);
     if constexpr (FUSABLE) {
       if (use_fused(f)) {
-        k_plane_vloc_fused<N, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+        k_plane_vloc_fused<N, C><<<g, PNT, fsmem<N, C>(), f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
         return;
       }
     }
@@ -621,6 +684,18 @@ bool fft_fusable(int n, const StickTab& st) {
     WB_FOR_EACH_N(X)
 #undef X
     default: return false;
+  }
+}
+
+int fft_plane_offset(int n, bool fused, int elem_bytes, int x, int y) {
+  switch (n) {
+#define X(n)                                                                                  \
+  case n:                                                                                     \
+    if (!fused) return Plane<n>::at(x, y);                                                    \
+    return elem_bytes == 8 ? FPlane<n, float2>::at(x, y) : FPlane<n, double2>::at(x, y);
+    WB_FOR_EACH_N(X)
+#undef X
+    default: return 0;
   }
 }
 

@@ -41,6 +41,10 @@ struct FftArgs32 {
 bool fft_supported(int n);
 // the fused one-pass plane kernel applies to this box and stick table
 bool fft_fusable(int n, const StickTab& st);
+// offset of plane element (x, y) in the shared-memory plane of the x-y pass
+// kernels: the fused local-potential layout (fused) or the padded-row one,
+// for elem_bytes 8 (FP32 complex) or 16 (FP64 complex)
+int fft_plane_offset(int n, bool fused, int elem_bytes, int x, int y);
 void fft_zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks);
 void fft_plane_vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs);
 void fft_zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, const float2* P,
