@@ -492,26 +492,28 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
   }
   __syncthreads();
   fused_cols<N, +1, PRUNE_IN, C>(pl, st, tw);
-  // inverse rows, step 1 (pruned input): row y = it / R, n2 = it % R = k1
-  for (int it = tid; it < N * R; it += PNT) {
-    C* p = pl + FP::row(it / R);
-    C v[R];
-#pragma unroll
-    for (int n1 = 0; n1 < R; ++n1)
-      v[n1] = (PR::IN_OK && !PR::in_live(n1)) ? mkc<C>(0, 0) : p[LP::off_blk(n1, k1)];
-    rdft<R, +1, N>(v, tw);
-#pragma unroll
-    for (int q = 1; q < R; ++q) v[q] = ctw<+1>(v[q], TWR ? wr[q] : tw[N + q * R + k1]);
-#pragma unroll
-    for (int q = 0; q < R; ++q) p[LP::off_blk(q, k1)] = v[q];
-  }
-  __syncthreads();
-#pragma unroll
+  // Rows: the R threads of a row are R consecutive lanes of one warp, and a warp
+  // keeps its rows through all row steps, so the steps are separated by warp
+  // barriers only.  Per row: inverse step 1 (pruned input, n2 = k1), inverse
+  // step 2 + V(r) + forward step 1 in registers, forward step 2 (pruned output).
+  static_assert(32 % R == 0, "a row's threads must share a warp");
+#pragma unroll 1
   for (int c = 0; c < NCH; ++c) {
     const int y = c * LPC + tid / R;
     const bool act = rowthr && y < N;
     C* p = pl + FP::row(act ? y : 0);
     C v[R];
+    if (act) {
+#pragma unroll
+      for (int n1 = 0; n1 < R; ++n1)
+        v[n1] = (PR::IN_OK && !PR::in_live(n1)) ? mkc<C>(0, 0) : p[LP::off_blk(n1, k1)];
+      rdft<R, +1, N>(v, tw);
+#pragma unroll
+      for (int q = 1; q < R; ++q) v[q] = ctw<+1>(v[q], TWR ? wr[q] : tw[N + q * R + k1]);
+#pragma unroll
+      for (int q = 0; q < R; ++q) p[LP::off_blk(q, k1)] = v[q];
+    }
+    __syncwarp();
     if (act) {
       T vr[R];                                      // V(r) of this row, loaded here to keep registers free
 #pragma unroll
@@ -525,14 +527,25 @@ WB_DEV void plane_vloc_fused_unit(C* __restrict__ sticks, const StickTab& st, co
 #pragma unroll
       for (int q = 1; q < R; ++q) v[q] = ctw<-1>(v[q], TWR ? wr[q] : tw[N + q * R + k1]);
     }
-    __syncthreads();
+    __syncwarp();
     if (act) {
 #pragma unroll
       for (int q = 0; q < R; ++q) p[LP::off_blk(q, k1)] = v[q];
     }
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int n2 = 0; n2 < R; ++n2) v[n2] = p[LP::off_blk(k1, n2)];
+      rdft<R, -1, N>(v, tw);
+    }
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int k2 = 0; k2 < R; ++k2)
+        if (!PR::OUT_OK || PR::out_live(k2)) p[LP::off(k1 + R * k2)] = v[k2];
+    }
   }
   __syncthreads();
-  fft_step2<N, -1, PNT, false, true, PRUNE_OUT>(pl, OffFRows<N, C>{}, 1, N, tw);
   fused_cols<N, -1, PRUNE_OUT, C>(pl, st, tw);
   plane_gather<N, C, FP>(pl, sz, st.st_pos, st.nst);
 }
