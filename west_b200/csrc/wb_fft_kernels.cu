@@ -54,30 +54,87 @@ WB_DEV C* smem_tw() {
   return reinterpret_cast<C*>(smraw);
 }
 
+// Twiddles of one thread (2N entries over the block), held in registers so
+// that their global loads are issued with the unit's other loads and stored
+// to shared memory after the zero fill.
+template <int N, class C>
+struct TwRegs {
+  static constexpr int PER = (2 * N + 255) / 256;
+  C v[PER];
+  WB_DEV void load(const C* __restrict__ twg) {
+    constexpr int N2 = FftSplit<N>::N2;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int i = threadIdx.x + 256 * k;
+      if (i < N) v[k] = twg[i];
+      else if (i < 2 * N) v[k] = twg[(((i - N) % N2) * ((i - N) / N2)) % N];
+    }
+  }
+  WB_DEV void store(C* tw) const {
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int i = threadIdx.x + 256 * k;
+      if (i < 2 * N) tw[i] = v[k];
+    }
+  }
+};
+
+// G coefficients prefetched per thread before the zero fill (the rest of a
+// stick group's G vectors, if any, are read in a second loop).
+constexpr int kZPre = 2;
+
 template <int N, bool PR, class C>
-WB_DEV void zinv_unit(const C* __restrict__ src, long ld, const int2* __restrict__ items, const StickTab& st,
-                      C* __restrict__ out, int qg, int item) {
+__global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld,
+                                              const int2* __restrict__ items, StickTab st,
+                                              C* __restrict__ out,
+                                              const C* __restrict__ twg, const int* dn) {
+  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;  // beyond the device item count
+  static_assert(ZNT == 256, "TwRegs assumes 256 threads");
   constexpr int LS = LinePad<N>::LEN | 1;  // odd line stride: conflict-free transposes
-  const C* tw = smem_tw<C>();
+  using LP = LinePad<N>;
+  C* tw = smem_tw<C>();
   C* zb = smem_tw<C>() + 2 * N;
+  const int qg = blockIdx.x, item = blockIdx.y;
   const int q0 = qg * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
-  for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = mkc<C>(0, 0);  // pads too
-  __syncthreads();
   const int2 it = items[item];
   const C* a = src + (long)it.x * ld;
   const C* b = src + (long)(it.y >= 0 ? it.y : it.x) * ld;
   const bool two = it.y >= 0;
   const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
-  for (int g = g0 + threadIdx.x; g < g1; g += ZNT) {
-    const int2 qz = st.g_qz[g];
-    const C a1 = a[g];
-    const C a2 = two ? b[g] : mkc<C>(0, 0);
+  TwRegs<N, C> twr;
+  twr.load(twg);
+  C pa[kZPre], pb[kZPre];
+  int2 pq[kZPre];
+#pragma unroll
+  for (int k = 0; k < kZPre; ++k) {
+    const int g = g0 + threadIdx.x + k * ZNT;
+    if (g < g1) {
+      pq[k] = st.g_qz[g];
+      pa[k] = a[g];
+      pb[k] = two ? b[g] : mkc<C>(0, 0);
+    }
+  }
+  // zero what step 1 reads: with pruning only the live inputs (the sphere's z
+  // lie in the outer quarters), otherwise the whole lines
+  if constexpr (PR && Prune<N>::IN_OK) {
+    constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2, NLIVE = N1 / 2;
+    for (int e = threadIdx.x; e < 2 * ZSG * NLIVE * N2; e += ZNT) {
+      const int l = e / (NLIVE * N2), r = e % (NLIVE * N2);
+      const int h = r / N2, n2 = r % N2;
+      const int n1 = h < NLIVE / 2 ? h : N1 - NLIVE + h;
+      zb[l * LS + LP::off_blk(n1, n2)] = mkc<C>(0, 0);
+    }
+  } else {
+    for (int i = threadIdx.x; i < 2 * ZSG * LS; i += ZNT) zb[i] = mkc<C>(0, 0);
+  }
+  twr.store(tw);
+  __syncthreads();
+  auto put = [&](int2 qz, C a1, C a2) {
     // pos = a1 + i a2 ; neg = conj(a1 - i a2)
     const C pos = mkc<C>(a1.x - a2.y, a1.y + a2.x);
     const C neg = mkc<C>(a1.x + a2.y, a2.x - a1.y);
     const int z = qz.y;
-    using LP = LinePad<N>;
     if (qz.x < 2) {  // the (0,0) stick is its own mirror
       if (z != 0) { zb[LP::off((z + N) % N)] = pos; zb[LP::off((N - z) % N)] = neg; }
       else zb[0] = neg;  // G = 0: the -G store wins, as in the reference loop
@@ -86,7 +143,12 @@ WB_DEV void zinv_unit(const C* __restrict__ src, long ld, const int2* __restrict
       zb[l * LS + LP::off((z + N) % N)] = pos;
       zb[(l ^ 1) * LS + LP::off((N - z) % N)] = neg;
     }
-  }
+  };
+#pragma unroll
+  for (int k = 0; k < kZPre; ++k)
+    if (g0 + (int)threadIdx.x + k * ZNT < g1) put(pq[k], pa[k], pb[k]);
+  for (int g = g0 + threadIdx.x + kZPre * ZNT; g < g1; g += ZNT)
+    put(st.g_qz[g], a[g], two ? b[g] : mkc<C>(0, 0));
   __syncthreads();
   fft_lines<N, +1, ZNT, false, true, PR ? PRUNE_IN : PRUNE_NONE>(zb, OffLinear{LS}, 1, 2 * nq, tw);
   const int ns = 2 * nq;
@@ -97,41 +159,41 @@ WB_DEV void zinv_unit(const C* __restrict__ src, long ld, const int2* __restrict
   }
 }
 
-template <int N, bool PR, class C>
-__global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld,
-                                              const int2* __restrict__ items, StickTab st,
-                                              C* __restrict__ out,
-                                              const C* __restrict__ twg, const int* dn) {
-  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;  // beyond the device item count
-  load_tw<N>(smem_tw<C>(), twg);
-  zinv_unit<N, PR, C>(src, ld, items, st, out, blockIdx.x, blockIdx.y);
-}
-
 // ---------------------------------------------------------------------------
 // z pass, forward: sticks -> sphere with the Gamma unpack, then an epilogue
 // ---------------------------------------------------------------------------
+// The twiddles are loaded into registers with the sticks and stored after
+// them.  An epilogue reads its per-G inputs through Epi::pre (prefetching them
+// before the transform was measured slower: the extra registers cost more
+// occupancy than the hidden latency gained).
 template <int N, bool PR, class C, class Epi>
-WB_DEV void zfwd_unit(const C* __restrict__ sticks, const int2* __restrict__ items, const StickTab& st,
-                      const Epi& epi, int qg, int item) {
+__global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
+                                              const int2* __restrict__ items, StickTab st,
+                                              const C* __restrict__ twg, Epi epi, const int* dn) {
+  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;
   constexpr int LS = LinePad<N>::LEN | 1;
-  const C* tw = smem_tw<C>();
+  using LP = LinePad<N>;
+  using T = real_t<C>;
+  C* tw = smem_tw<C>();
   C* zb = smem_tw<C>() + 2 * N;
+  const int qg = blockIdx.x, item = blockIdx.y;
   const int q0 = qg * ZSG;
   const int nq = min(ZSG, st.nsp - q0);
   const int ns = 2 * nq;
   const C* s0 = sticks + (long)item * N * st.nst + 2 * q0;
+  TwRegs<N, C> twr;
+  twr.load(twg);
+  const int2 it = items[item];
+  const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
   for (int e = threadIdx.x; e < ns * N; e += ZNT) {
     const int s = e % ns, z = e / ns;
     zb[s * LS + LinePad<N>::off(z)] = s0[(long)z * st.nst + s];
   }
+  twr.store(tw);
   __syncthreads();
   fft_lines<N, -1, ZNT, false, true, PR ? PRUNE_OUT : PRUNE_NONE>(zb, OffLinear{LS}, 1, ns, tw);
-  const int2 it = items[item];
-  const int g0 = st.sp_gstart[q0], g1 = st.sp_gstart[q0 + nq];
-  for (int g = g0 + threadIdx.x; g < g1; g += ZNT) {
-    const int2 qz = st.g_qz[g];
+  auto take = [&](int g, int2 qz, const typename Epi::Pre& pr) {
     const int z = qz.y;
-    using LP = LinePad<N>;
     C ap, am;
     if (qz.x < 2) {
       ap = zb[LP::off((z + N) % N)];
@@ -141,26 +203,19 @@ WB_DEV void zfwd_unit(const C* __restrict__ sticks, const int2* __restrict__ ite
       ap = zb[l * LS + LP::off((z + N) % N)];
       am = zb[(l ^ 1) * LS + LP::off((N - z) % N)];
     }
-    using T = real_t<C>;
     const C fp = mkc<C>(T(0.5) * (ap.x + am.x), T(0.5) * (ap.y + am.y));
     const C fm = mkc<C>(T(0.5) * (ap.x - am.x), T(0.5) * (ap.y - am.y));
-    epi(g, it, mkc<C>(fp.x, fm.y), mkc<C>(fp.y, -fm.x));
-  }
-}
-
-template <int N, bool PR, class C, class Epi>
-__global__ void __launch_bounds__(ZNT) k_zfwd(const C* __restrict__ sticks,
-                                              const int2* __restrict__ items, StickTab st,
-                                              const C* __restrict__ twg, Epi epi, const int* dn) {
-  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;
-  load_tw<N>(smem_tw<C>(), twg);
-  zfwd_unit<N, PR, C, Epi>(sticks, items, st, epi, blockIdx.x, blockIdx.y);
+    epi(g, it, pr, mkc<C>(fp.x, fm.y), mkc<C>(fp.y, -fm.x));
+  };
+  for (int g = g0 + threadIdx.x; g < g1; g += ZNT) take(g, st.g_qz[g], epi.pre(g, it));
 }
 
 struct EpiStore {
   double2* dst;
   long ld;
-  WB_DEV void operator()(int g, int2 it, double2 b1, double2 b2) const {
+  struct Pre {};
+  WB_DEV Pre pre(int, int2) const { return {}; }
+  WB_DEV void operator()(int g, int2 it, const Pre&, double2 b1, double2 b2) const {
     dst[(long)it.x * ld + g] = b1;
     if (it.y >= 0) dst[(long)it.y * ld + g] = b2;
   }
@@ -176,17 +231,26 @@ struct EpiHpsiT {
   long ld;
   const T* g2kin;
   const T* ecol;
-  WB_DEV void one(int g, int c, C vp) const {
-    const C p = P[(long)c * ld + g];
-    const T k = g2kin[g];
+  struct Pre {
+    C p1, p2;
+    T k;
+  };
+  WB_DEV Pre pre(int g, int2 it) const {
+    Pre r;
+    r.p1 = P[(long)it.x * ld + g];
+    r.p2 = it.y >= 0 ? P[(long)it.y * ld + g] : mkc<C>(0, 0);
+    r.k = g2kin[g];
+    return r;
+  }
+  WB_DEV void one(int g, int c, C p, T k, C vp) const {
     C h = mkc<C>(fma(k, p.x, vp.x), fma(k, p.y, vp.y));
     if (g == 0) h.y = T(0);
     const T e = ecol[c];
     Tv[(long)c * ld + g] = mkc<C>(fma(-e, p.x, h.x), fma(-e, p.y, h.y));
   }
-  WB_DEV void operator()(int g, int2 it, C b1, C b2) const {
-    one(g, it.x, b1);
-    if (it.y >= 0) one(g, it.y, b2);
+  WB_DEV void operator()(int g, int2 it, const Pre& pr, C b1, C b2) const {
+    one(g, it.x, pr.p1, pr.k, b1);
+    if (it.y >= 0) one(g, it.y, pr.p2, pr.k, b2);
   }
 };
 using EpiHpsi = EpiHpsiT<double2>;
@@ -199,9 +263,14 @@ struct EpiDng {
   long ld;
   const int* perm;
   const double* sqvc;
-  WB_DEV void operator()(int g, int2 it, double2 b1, double2 b2) const {
-    const double s = (g == 0) ? 0.0 : sqvc[g];
-    const long r = perm[g];
+  struct Pre {
+    double s;
+    int r;
+  };
+  WB_DEV Pre pre(int g, int2) const { return {(g == 0) ? 0.0 : sqvc[g], perm[g]}; }
+  WB_DEV void operator()(int g, int2 it, const Pre& pr, double2 b1, double2 b2) const {
+    const double s = pr.s;
+    const long r = pr.r;
     dng[(long)it.x * ld + r] = make_double2(s * b1.x, s * b1.y);
     if (it.y >= 0) dng[(long)it.y * ld + r] = make_double2(s * b2.x, s * b2.y);
   }
