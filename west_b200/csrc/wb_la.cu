@@ -61,20 +61,27 @@ __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict_
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-#pragma unroll 2
-  for (int k = kb + warp * 4; k < ke; k += 4 * TN_W) {
+  // operands of the next k step are loaded while this step's MMAs run
+  double av[4], bv[4];
+  auto load = [&](int k, double* a, double* b) {
     const int kk = k + lk;
     const bool kok = kk < ke;
-    double av[4], bv[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      av[i] = (aok[i] && kok) ? __ldg(arow[i] + kk) : 0.0;
-      bv[i] = (bok[i] && kok) ? __ldg(bcol[i] + kk) : 0.0;
+      a[i] = (aok[i] && kok) ? __ldg(arow[i] + kk) : 0.0;
+      b[i] = (bok[i] && kok) ? __ldg(bcol[i] + kk) : 0.0;
     }
+  };
+  load(kb + warp * 4, av, bv);
+  for (int k = kb + warp * 4; k < ke; k += 4 * TN_W) {
+    double an[4], bn[4];
+    load(k + 4 * TN_W, an, bn);
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
       for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { av[i] = an[i]; bv[i] = bn[i]; }
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a)
@@ -177,7 +184,7 @@ __global__ void __launch_bounds__(128) k_gemm_nn(const double* __restrict__ W, l
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-#pragma unroll 2
+#pragma unroll 4
   for (int r = 0; r < M; r += 4) {
     const int rr = r + lk;
     const bool rok = rr < M;
