@@ -582,8 +582,9 @@ void apply_A32(wb_ctx* c, const float2* Pv, float2* Tv, const int* cols, const i
 // ---------------------------------------------------------------------------
 // CUDA graphs of the PCG loops
 // ---------------------------------------------------------------------------
-// One masked PCG pass (prec/rho, compaction, operator, update, loop control)
-// is captured into the body of a conditional WHILE node, so the whole loop runs
+// One masked PCG pass (operator, update + the next iteration's prec/rho,
+// compaction, loop control) is captured into the body of a conditional WHILE
+// node, so the whole loop runs
 // from one graph launch with its convergence test on the device.  The kernels
 // take the active count from device memory and size their grids for the
 // workspace capacity; the graph is rebuilt when a buffer, the capacity or tr2
@@ -626,7 +627,7 @@ int capture_loop(wb_ctx* c, wb_ctx::LoopGraph& lg, std::vector<const void*> key,
   // 1. the bucket of this pass
   if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    loop_bucket(hs, dn, kMinBucketItems, nb, s);
+    loop_bucket(hs, dn, st, kMinBucketItems, nb, s);
     cudaGraph_t g1 = nullptr;
     e = cudaStreamEndCapture(s, &g1);
   }
@@ -707,15 +708,14 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
                                     c->part32.p, c->C32.p,    c->ecol32.p, st,          (const void*)(intptr_t)cap};
     const int* dn = c->nact_in.as<int>();
     rc = capture_loop(c, c->loop32, key, tr2, cap, dn, st, true, [&](int nmax) {
-      cg_prec_rho32(c->act_in.as<int>(), nmax, c->g32.as<float2>(), c->P32.as<float2>(), c->iprec.as<double>(), nocc,
-                    c->rho_in.as<double>(), c->conv_in.as<unsigned char>(), 0, kInnerRhoReduction,
-                    c->rho0.as<double>(), tr2, npw, ld, s, dn, st + 1);
-      cg_compact(c->conv_in.as<unsigned char>(), cap, c->act_in.as<int>(), c->items_in.as<int2>(),
-                 c->nact_in.as<int>(), nullptr, s, st);
       apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), c->act_in.as<int>(), c->items_in.as<int2>(), nmax,
                 nsplit32, dn);
-      cg_update32(c->act_in.as<int>(), nmax, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(),
-                  c->T32.as<float2>(), npw, ld, s, dn);
+      cg_step32(c->act_in.as<int>(), nmax, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(),
+                c->T32.as<float2>(), c->iprec.as<double>(), nocc, c->rho_in.as<double>(),
+                c->conv_in.as<unsigned char>(), 0, c->maxiter, kInnerRhoReduction, c->rho0.as<double>(), tr2, npw,
+                ld, s, dn, st + 1);
+      cg_compact(c->conv_in.as<unsigned char>(), cap, c->act_in.as<int>(), c->items_in.as<int2>(),
+                 c->nact_in.as<int>(), nullptr, s, st);
     });
     if (rc) return rc;
     loop_init(st, nsys, true, s);
@@ -746,22 +746,22 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     if (nact == 0 || outer == kMaxRefinements - 1) break;
     c->stats.refinements += 1;
     WB_CU(cudaMemcpyAsync(cin, conv, nsys, cudaMemcpyDeviceToDevice, s));
-    cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), graph ? nullptr : c->nact_host, s);
+    cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), nullptr, s);
     int nin = nact;
-    // each refinement restarts the FP32 PCG from d = 0 on the FP64 residual
+    // each refinement restarts the FP32 PCG from d = 0 on the FP64 residual; its
+    // preconditioning stops at rho < max(1e-10 rho_outer, tr2): the first
+    // correction from x0 is the reference's own PCG (same Krylov space, same test)
+    if (c->maxiter > 0) {
+      Stage g(c, WB_STAGE_CG, 2, nin);
+      cg_prec_rho32(ain, nin, c->g32.as<float2>(), c->P32.as<float2>(), c->iprec.as<double>(), nocc,
+                    c->rho_in.as<double>(), cin, 1, kInnerRhoReduction, c->rho0.as<double>(), tr2, npw, ld, s);
+      cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), graph ? nullptr : c->nact_host, s);
+    }
     if (graph && c->maxiter > 0) {
       loop_init(st, nsys, false, s);
       WB_CU(cudaGraphLaunch(c->loop32.exec, s));
     }
     for (int it = 1; !graph && it <= c->maxiter; ++it) {
-      {
-        Stage g(c, WB_STAGE_CG, 2, nin);
-        // stop at rho < max(1e-10 rho_outer, tr2): the first correction from x0 is the
-        // reference's own PCG (same Krylov space, same stopping test)
-        cg_prec_rho32(ain, nin, c->g32.as<float2>(), c->P32.as<float2>(), c->iprec.as<double>(), nocc,
-                      c->rho_in.as<double>(), cin, it, kInnerRhoReduction, c->rho0.as<double>(), tr2, npw, ld, s);
-        cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
-      }
       WB_CU(cudaStreamSynchronize(s));
       nin = *c->nact_host;
       if (nin == 0) break;
@@ -769,9 +769,11 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
       c->stats.cg_active_sum += nin;
       apply_A32(c, c->P32.as<float2>(), c->T32.as<float2>(), ain, iin, nin, nsplit32);
       {
-        Stage g(c, WB_STAGE_CG, 1, nin);
-        cg_update32(ain, nin, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(), c->T32.as<float2>(), npw,
-                    ld, s);
+        Stage g(c, WB_STAGE_CG, 2, nin);
+        cg_step32(ain, nin, c->d32.as<float2>(), c->g32.as<float2>(), c->P32.as<float2>(), c->T32.as<float2>(),
+                  c->iprec.as<double>(), nocc, c->rho_in.as<double>(), cin, it, c->maxiter, kInnerRhoReduction,
+                  c->rho0.as<double>(), tr2, npw, ld, s);
+        cg_compact(cin, nsys, ain, iin, c->nact_in.as<int>(), c->nact_host, s);
       }
     }
     {
@@ -787,7 +789,7 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
     WB_CU(cudaStreamSynchronize(s));
     inner_total = c->loop_host[3];
-    loop_stats(c, inner_total, c->kinetic_only ? 7 : 10);
+    loop_stats(c, inner_total, c->kinetic_only ? 6 : 9);
   }
   *iters_out = inner_total;
   if (c->umma) {  // a bounded wait of a tensor-core GEMM that ran out leaves its code here
@@ -874,6 +876,11 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
     }
     int nact = nsys;
     const bool graph = graph_mode(c) && c->maxiter > 0;
+    if (c->maxiter > 0) {                                        // iteration 1: prec, rho, test (:146-222)
+      Stage g(c, WB_STAGE_CG, 2, nsys);
+      cg_prec_rho(act, nsys, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, 1, tr2, npw, ld, s);
+      cg_compact(conv, nsys, act, items, c->nact.as<int>(), graph ? nullptr : c->nact_host, s);
+    }
     if (graph) {                                                 // :146-330 as one graph launch
       const int cap = c->cap_nsys;
       const int nsplit_cap = gemm_tn_splits(c->nproj, cap, K, c->tune.dmma_ctas);
@@ -882,11 +889,10 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
       std::vector<const void*> key = {B, X, G, T, c->sticks.p, act, items, dn, conv, c->rho.p, c->part.p, c->C.p,
                                       c->ecol.p, st, (const void*)(intptr_t)cap};
       int rc = capture_loop(c, c->loop64, key, tr2, cap, dn, st, false, [&](int nmax) {
-        cg_prec_rho(act, nmax, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, 0, tr2, npw, ld, s, dn,
-                    st + 1);
-        cg_compact(conv, cap, act, items, c->nact.as<int>(), nullptr, s, st);
         apply_A(c, B, T, act, items, nmax, cap, nsplit_cap, dn);
-        cg_update(act, nmax, X, G, B, T, npw, ld, s, dn);
+        cg_step(act, nmax, X, G, B, T, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, 0, c->maxiter, tr2,
+                npw, ld, s, dn, st + 1);
+        cg_compact(conv, cap, act, items, c->nact.as<int>(), nullptr, s, st);
       });
       if (rc) return rc;
       loop_init(st, nsys, true, s);
@@ -894,14 +900,9 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
       WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
       WB_CU(cudaStreamSynchronize(s));
       iters = c->loop_host[2];
-      loop_stats(c, iters, c->kinetic_only ? 7 : 10);
+      loop_stats(c, c->loop_host[3], c->kinetic_only ? 6 : 9);
     }
     for (int it = 1; !graph && it <= c->maxiter; ++it) {        // :146
-      {
-        Stage g(c, WB_STAGE_CG, 2, nact);
-        cg_prec_rho(act, nact, G, B, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, it, tr2, npw, ld, s);
-        cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
-      }
       WB_CU(cudaStreamSynchronize(s));
       nact = *c->nact_host;
       iters = it;
@@ -909,8 +910,11 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
       c->stats.cg_active_sum += nact;
       apply_A(c, B, T, act, items, nact, nsys, nsplit);          // :251
       {
-        Stage g(c, WB_STAGE_CG, 1, nact);
-        cg_update(act, nact, X, G, B, T, npw, ld, s);            // :253-329
+        Stage g(c, WB_STAGE_CG, 2, nact);
+        // :253-329, then iteration it + 1's :146-222
+        cg_step(act, nact, X, G, B, T, c->iprec.as<double>(), nocc, c->rho.as<double>(), conv, it, c->maxiter, tr2,
+                npw, ld, s);
+        cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
       }
     }
     {
@@ -1375,16 +1379,20 @@ int noalloc_run(wb_ctx* c, const NoallocWs& w, int mb, const double2* dvg, long 
     noalloc_apply_A(c, w, w.X, w.T, w.act, w.items, nsys);
     sub_into(w.T, w.B, w.G, npw, nsys, ld, s);
     int nact = nsys;
-    for (int it = 1; it <= c->maxiter; ++it) {
-      cg_prec_rho(w.act, nact, w.G, w.B, c->iprec.as<double>(), nocc, w.rho, w.conv, it, tr2, npw, ld, s);
+    if (c->maxiter > 0) {
+      cg_prec_rho(w.act, nact, w.G, w.B, c->iprec.as<double>(), nocc, w.rho, w.conv, 1, tr2, npw, ld, s);
       cg_compact(w.conv, nsys, w.act, w.items, w.nact, c->nact_host, s);
+    }
+    for (int it = 1; it <= c->maxiter; ++it) {
       WB_CU(cudaStreamSynchronize(s));
       nact = *c->nact_host;
       iters = it;
       if (nact == 0) break;
       c->stats.cg_active_sum += nact;
       noalloc_apply_A(c, w, w.B, w.T, w.act, w.items, nact);
-      cg_update(w.act, nact, w.X, w.G, w.B, w.T, npw, ld, s);
+      cg_step(w.act, nact, w.X, w.G, w.B, w.T, c->iprec.as<double>(), nocc, w.rho, w.conv, it, c->maxiter, tr2, npw,
+              ld, s);
+      cg_compact(w.conv, nsys, w.act, w.items, w.nact, c->nact_host, s);
     }
     count_unconverged(w.conv, nocc, mb, w.unconv, s);
   } else {

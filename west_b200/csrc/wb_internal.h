@@ -112,11 +112,21 @@ void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int*
                 cudaStream_t s, const int* nsys_dev = nullptr);
 void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
                long ld, cudaStream_t s, const int* dn = nullptr);
+// One PCG step after the operator: the update of iteration `iter` and, unless
+// iter == maxiter, the preconditioning / rho / convergence test / direction of
+// iteration iter + 1 (the iteration comes from *iter_dev when given).
+void cg_step(const int* act, int nact, double2* x, double2* g, double2* P, const double2* T, const double* iprec,
+             int nocc, double* rho_prev, unsigned char* conv, int iter, int maxiter, double tr2, int npw, long ld,
+             cudaStream_t s, const int* dn = nullptr, const int* iter_dev = nullptr);
+void cg_step32(const int* act, int nact, float2* x, float2* g, float2* P, const float2* T, const double* iprec,
+               int nocc, double* rho_prev, unsigned char* conv, int iter, int maxiter, double eta, const double* rel,
+               double floor, int npw, long ld, cudaStream_t s, const int* dn = nullptr,
+               const int* iter_dev = nullptr);
 void count_unconverged(const unsigned char* conv, int nocc, int mb, int* out, cudaStream_t s);
 // loop state of the graph-captured PCG loops: int st[8] (wb_la.cu)
 void loop_init(int* st, int nsys, bool reset_totals, cudaStream_t s);
 void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, bool inner, cudaStream_t s);
-void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int min_items, int nbuckets, cudaStream_t s);
+void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int* st, int min_items, int nbuckets, cudaStream_t s);
 
 // ---- mixed form: FP32 inner PCG and FP64 refinement (wb_la.cu) ----
 // inner test: rho < max(eta * rel[j], floor)

@@ -494,6 +494,92 @@ void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P
   k_cg_update<float2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, x, g, P, T, npw, ld);
 }
 
+// One PCG step after the operator, in one kernel: the update of iteration
+// `iter` (k_cg_update: a = <P|g>, c = <P|T>, x -= a/c P, g -= a/c T) and,
+// unless iter == maxiter, iteration iter + 1's preconditioning, rho, test and
+// direction (k_cg_prec_rho: h = M g, rho = <h|g>, P = -h + rho/rho_prev P).
+// One CTA per system; the new g is preconditioned and its rho summed in the
+// update's own pass, and the direction pass re-reads g (just written) and P
+// (read twice already) from L2, so the vectors make fewer trips to DRAM than
+// with two kernels with the active-list compaction between them.
+template <class C>
+__global__ void __launch_bounds__(256) k_cg_step(const int* __restrict__ act, const int* dn, C* __restrict__ x,
+                                                 C* __restrict__ g, C* __restrict__ P, const C* __restrict__ T,
+                                                 const double* __restrict__ iprec, int nocc, double* rho_prev,
+                                                 unsigned char* conv, int iter_host, const int* iter_dev, int maxiter,
+                                                 double tr2, const double* __restrict__ rel, double floor, int npw,
+                                                 long ld) {
+  using R = real_t<C>;
+  __shared__ double red[16];
+  const int n = dev_count(dn, gridDim.x);
+  const int iter = iter_dev ? *iter_dev : iter_host;
+  const bool prec = iter + 1 <= maxiter;  // the reference leaves its loop before this preconditioning otherwise
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const int j = act[b];
+    const C* tj = T + (long)j * ld;
+    C* pj = P + (long)j * ld;
+    C* gj = g + (long)j * ld;
+    C* xj = x + (long)j * ld;
+    const double* ip = iprec + (long)(j % nocc) * npw;
+    double a = 0.0, c = 0.0;
+    for (int i = threadIdx.x; i < npw; i += 256) {
+      const C p = pj[i], gv = gj[i], tv = tj[i];
+      double da = fma((double)p.x, (double)gv.x, (double)p.y * (double)gv.y);
+      double dc = fma((double)p.x, (double)tv.x, (double)p.y * (double)tv.y);
+      if (i == 0) { da -= 0.5 * (double)p.x * (double)gv.x; dc -= 0.5 * (double)p.x * (double)tv.x; }
+      a += da;
+      c += dc;
+    }
+    const double2 s = block_sum2<256>(a, c, red);
+    const R r = R((2.0 * s.x) / (2.0 * s.y));
+    double tt = 0.0, t0 = 0.0;
+    for (int i = threadIdx.x; i < npw; i += 256) {
+      const C p = pj[i], tv = tj[i];
+      const C xv = xj[i], gv = gj[i];
+      xj[i] = mkc<C>(fma(-r, p.x, xv.x), fma(-r, p.y, xv.y));
+      const C gn = mkc<C>(fma(-r, tv.x, gv.x), fma(-r, tv.y, gv.y));
+      gj[i] = gn;
+      if (prec) {
+        const double w = ip[i];
+        const double hx = (double)gn.x * w, hy = (double)gn.y * w;
+        tt = fma(hx, (double)gn.x, fma(hy, (double)gn.y, tt));
+        if (i == 0) t0 = hx * (double)gn.x;
+      }
+    }
+    if (!prec) continue;
+    const double2 s2 = block_sum2<256>(tt, t0, red);
+    const double rho = 2.0 * s2.x - s2.y;
+    const double thr = rel ? fmax(tr2 * rel[j], floor) : tr2;
+    if (rho < thr) {  // block-uniform
+      if (threadIdx.x == 0) conv[j] = 1;
+      continue;
+    }
+    const double beta = rho / rho_prev[j];  // iteration iter + 1 >= 2
+    __syncthreads();
+    if (threadIdx.x == 0) rho_prev[j] = rho;
+    for (int i = threadIdx.x; i < npw; i += 256) {
+      const double w = ip[i];
+      const C gv = gj[i], pv = pj[i];
+      const double hx = (double)gv.x * w, hy = (double)gv.y * w;
+      pj[i] = mkc<C>(R(fma(beta, (double)pv.x, -hx)), R(fma(beta, (double)pv.y, -hy)));
+    }
+  }
+}
+void cg_step(const int* act, int nact, double2* x, double2* g, double2* P, const double2* T, const double* iprec,
+             int nocc, double* rho_prev, unsigned char* conv, int iter, int maxiter, double tr2, int npw, long ld,
+             cudaStream_t s, const int* dn, const int* iter_dev) {
+  if (nact <= 0) return;
+  k_cg_step<double2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, x, g, P, T, iprec, nocc, rho_prev, conv, iter,
+                                                        iter_dev, maxiter, tr2, nullptr, 0.0, npw, ld);
+}
+void cg_step32(const int* act, int nact, float2* x, float2* g, float2* P, const float2* T, const double* iprec,
+               int nocc, double* rho_prev, unsigned char* conv, int iter, int maxiter, double eta, const double* rel,
+               double floor, int npw, long ld, cudaStream_t s, const int* dn, const int* iter_dev) {
+  if (nact <= 0) return;
+  k_cg_step<float2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, x, g, P, T, iprec, nocc, rho_prev, conv, iter,
+                                                       iter_dev, maxiter, eta, rel, floor, npw, ld);
+}
+
 // ---------------------------------------------------------------------------
 // FP64 iterative refinement around the FP32 PCG (mixed form)
 // ---------------------------------------------------------------------------
@@ -782,22 +868,18 @@ void loop_init(int* st, int nsys, bool reset_totals, cudaStream_t s) {
   k_loop_init<<<1, 1, 0, s>>>(st, nsys, reset_totals ? 1 : 0);
 }
 
-// End of one PCG pass: linsolve's loop over iter = 1..n_dfpt_maxiter, leaving
-// when no system is active (linsolve_sternheimer_m_wfcts.f90:146,222); every
-// FP32 correction solve of the mixed form is bounded the same way (inner = 1
-// also counts its passes over all refinements in st[3]).  Sets the WHILE
-// condition of the graph.
+// End of one PCG pass (operator, update of iteration st[1] and the
+// preconditioning of iteration st[1] + 1, active list): linsolve's loop over
+// iter = 1..n_dfpt_maxiter, left when no system is active
+// (linsolve_sternheimer_m_wfcts.f90:146,222); every FP32 correction solve of
+// the mixed form is bounded the same way.  Sets the WHILE condition of the
+// graph; for the FP64 loop (inner = 0) it leaves the reference's iteration
+// count in st[2]: the passes that did work, plus the one whose test found no
+// system left.
 __global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxiter, int inner) {
   const int n = *nact, it = st[1];
-  long long* sum = reinterpret_cast<long long*>(st + 4);
-  long long* boxes = reinterpret_cast<long long*>(st + 6);
-  if (n > 0) {
-    *sum += n;
-    *boxes += 2 * ((n + 1) / 2);
-    if (inner) st[3] += 1;
-  }
-  if (!inner) st[2] = it;
   const bool more = n > 0 && it < maxiter;
+  if (!inner && !more) st[2] = st[3] + (n == 0 ? 1 : 0);
   if (more) st[1] = it + 1;
   cudaGraphSetConditional(h, more ? 1u : 0u);
 }
@@ -805,16 +887,24 @@ void loop_ctl(cudaGraphConditionalHandle h, const int* nact, int* st, int maxite
   k_loop_ctl<<<1, 1, 0, s>>>(h, nact, st, maxiter, inner ? 1 : 0);
 }
 
-// SWITCH value of a pass: the smallest bucket k with min_items << k >= the
-// active band-pair items (last bucket: the workspace capacity).
-__global__ void k_loop_bucket(cudaGraphConditionalHandle h, const int* nact, int min_items, int nbuckets) {
-  const int items = (*nact + 1) / 2;
+// Start of a pass: counts the pass's work (st[3] passes with active systems,
+// their active-system and FFT-item sums) and sets the SWITCH value: the
+// smallest bucket k with min_items << k >= the active band-pair items (last
+// bucket: the workspace capacity).
+__global__ void k_loop_bucket(cudaGraphConditionalHandle h, const int* nact, int* st, int min_items, int nbuckets) {
+  const int n = *nact;
+  if (n > 0) {
+    *reinterpret_cast<long long*>(st + 4) += n;
+    *reinterpret_cast<long long*>(st + 6) += 2 * ((n + 1) / 2);
+    st[3] += 1;
+  }
+  const int items = (n + 1) / 2;
   int k = 0;
   while (k < nbuckets - 1 && (min_items << k) < items) ++k;
   cudaGraphSetConditional(h, (unsigned)k);
 }
-void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int min_items, int nbuckets, cudaStream_t s) {
-  k_loop_bucket<<<1, 1, 0, s>>>(h, nact, min_items, nbuckets);
+void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int* st, int min_items, int nbuckets, cudaStream_t s) {
+  k_loop_bucket<<<1, 1, 0, s>>>(h, nact, st, min_items, nbuckets);
 }
 
 __global__ void k_count_unconverged(const unsigned char* __restrict__ conv, int nocc, int mb, int* __restrict__ out) {
