@@ -160,16 +160,41 @@ void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double*
 // ---------------------------------------------------------------------------
 // Y[col j][k] = beta Y[col j][k] + sum_r W[r][k] C[j][r]
 // CTA: 4 warps x 32 rows of k, 32 columns j; inner loop over r in steps of 4.
+// With beta != 0 (and 16-byte aligned rows of Y) the CTA's Y tile is copied
+// into shared memory by cp.async at the start, so its DRAM latency overlaps
+// the MMAs instead of stalling the epilogue.  Row stride 130 doubles: the four
+// column groups of a half-warp's epilogue reads fall on disjoint banks.
 // ---------------------------------------------------------------------------
+constexpr int NN_YLD = 130;
+
+WB_DEV void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+
 __global__ void __launch_bounds__(128) k_gemm_nn(const double* __restrict__ W, long ldw, int M,
                                                  const double* __restrict__ C, double* __restrict__ Y, long ldy,
                                                  const int* __restrict__ cols, int ncol_host, const int* dn, int K,
-                                                 double beta) {
+                                                 double beta, int stage_y) {
+  __shared__ __align__(16) double ysh[32 * NN_YLD];
   const int ncol = dev_count(dn, ncol_host);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lr = lane >> 2, lk = lane & 3;
-  const int k0 = blockIdx.x * 128 + warp * 32, j0 = blockIdx.y * 32;
+  const int kbase = blockIdx.x * 128;
+  const int k0 = kbase + warp * 32, j0 = blockIdx.y * 32;
   if (j0 >= ncol) return;
+  const bool pre = stage_y && beta != 0.0;
+  if (pre) {  // Y[col(j0 + jl)][kbase + 2q, +1] -> ysh[jl][2q, +1]  (K is even: a pair never straddles K)
+    for (int e = threadIdx.x; e < 32 * 64; e += 128) {
+      const int jl = e >> 6, q = e & 63;
+      const int j = j0 + jl, k = kbase + 2 * q;
+      if (j < ncol && k < K) {
+        const int col = cols ? cols[j] : j;
+        cp_async16(ysh + jl * NN_YLD + 2 * q, Y + (long)col * ldy + k);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  }
   bool kok[4], jok[4];
   const double* crow[4];
 #pragma unroll
@@ -200,18 +225,24 @@ __global__ void __launch_bounds__(128) k_gemm_nn(const double* __restrict__ W, l
 #pragma unroll
       for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
   }
+  if (pre) {
+    asm volatile("cp.async.wait_all;\n" ::);
+    __syncthreads();
+  }
 #pragma unroll
   for (int b = 0; b < 4; ++b)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int j = j0 + b * 8 + 2 * lk + h;
+      const int jl = b * 8 + 2 * lk + h, j = j0 + jl;
       if (j >= ncol) continue;
       const int col = cols ? cols[j] : j;
       double* y = Y + (long)col * ldy;
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
-        const int k = k0 + a * 8 + lr;
-        if (k < K) y[k] = (beta == 0.0 ? 0.0 : beta * y[k]) + acc[a][b][h];
+        const int kl = warp * 32 + a * 8 + lr, k = kbase + kl;
+        if (k >= K) continue;
+        const double old = beta == 0.0 ? 0.0 : (pre ? ysh[jl * NN_YLD + kl] : y[k]);
+        y[k] = beta * old + acc[a][b][h];
       }
     }
 }
@@ -219,8 +250,9 @@ __global__ void __launch_bounds__(128) k_gemm_nn(const double* __restrict__ W, l
 void gemm_nn(const double* W, long ldw, int M, const double* C, double* Y, long ldy, const int* cols, int ncol,
              int K, double beta, cudaStream_t s, const int* dn) {
   if (ncol <= 0 || M <= 0) return;
+  const int stage_y = (K % 2 == 0) && (ldy % 2 == 0) && ((uintptr_t)Y % 16 == 0);
   dim3 grid((K + 127) / 128, (ncol + 31) / 32);
-  k_gemm_nn<<<grid, 128, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, dn, K, beta);
+  k_gemm_nn<<<grid, 128, 0, s>>>(W, ldw, M, C, Y, ldy, cols, ncol, dn, K, beta, stage_y);
 }
 
 // ---------------------------------------------------------------------------
