@@ -27,8 +27,11 @@
 
 namespace wb {
 
-constexpr int ZSG = 16;     // stick pairs per CTA in the z passes
-constexpr int ZNT = 256;
+// z passes: 8 stick pairs per CTA of 128 threads (measured against 16/256 and
+// 4/64 at 64^3: more, smaller CTAs overlap one CTA's loads with another's
+// transform and stores; zfwd 0.30 instead of 0.34 us per FP64 item)
+constexpr int ZSG = 8;
+constexpr int ZNT = 128;
 constexpr int PNT = 256;
 
 // 2N-entry twiddle table: natural order, then the step-1 factors (wb_fft.cuh)
@@ -44,7 +47,7 @@ WB_DEV void load_tw(C* tw, const C* twg) {
 // ---------------------------------------------------------------------------
 // z pass, inverse: sphere coefficients of a pair of columns -> sticks
 // ---------------------------------------------------------------------------
-// One unit = stick pairs [16 qg, 16 qg + 16) of band-pair item `item`.
+// One unit = stick pairs [ZSG qg, ZSG qg + ZSG) of band-pair item `item`.
 // Shared memory of every unit: the twiddles (2N), then the work area.  A unit
 // takes its pointers from the dynamic shared array itself so that a unit body
 // compiled as a separate function still addresses shared memory directly.
@@ -59,13 +62,13 @@ WB_DEV C* smem_tw() {
 // to shared memory after the zero fill.
 template <int N, class C>
 struct TwRegs {
-  static constexpr int PER = (2 * N + 255) / 256;
+  static constexpr int PER = (2 * N + ZNT - 1) / ZNT;
   C v[PER];
   WB_DEV void load(const C* __restrict__ twg) {
     constexpr int N2 = FftSplit<N>::N2;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-      const int i = threadIdx.x + 256 * k;
+      const int i = threadIdx.x + ZNT * k;
       if (i < N) v[k] = twg[i];
       else if (i < 2 * N) v[k] = twg[(((i - N) % N2) * ((i - N) / N2)) % N];
     }
@@ -73,7 +76,7 @@ struct TwRegs {
   WB_DEV void store(C* tw) const {
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-      const int i = threadIdx.x + 256 * k;
+      const int i = threadIdx.x + ZNT * k;
       if (i < 2 * N) tw[i] = v[k];
     }
   }
@@ -89,7 +92,6 @@ __global__ void __launch_bounds__(ZNT) k_zinv(const C* __restrict__ src, long ld
                                               C* __restrict__ out,
                                               const C* __restrict__ twg, const int* dn) {
   if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;  // beyond the device item count
-  static_assert(ZNT == 256, "TwRegs assumes 256 threads");
   constexpr int LS = LinePad<N>::LEN | 1;  // odd line stride: conflict-free transposes
   using LP = LinePad<N>;
   C* tw = smem_tw<C>();
