@@ -76,6 +76,7 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self.skip = 0
+        self.end = None
         self._t = None
 
     def __enter__(self):
@@ -110,7 +111,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        lines = self.lines[self.skip:] or self.lines
+        lines = self.lines[self.skip:self.end] or self.lines[self.skip:] or self.lines
         for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
@@ -231,6 +232,9 @@ def run_b200(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # the clock sampler starts before the warm-up: its start-up leaves the GPU
+    # idle for up to a second, which must not precede the first timed step
+    clk = ClockSampler(local_rank).__enter__()
     # warm-up (also settles the device workspace)
     for _ in range(args.warmup):
         op.apply_operator(m, dvg_d, dng_d, TR2)
@@ -241,18 +245,23 @@ def run_b200(args, rank, world, local_rank):
     launches = 0
     iters, act_sum, boxes = [], 0, 0
     barrier(); torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(args.steps):
+    clk.skip = len(clk.lines)  # clock samples of the timed region only
+    try:
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        ev[0].record()
+        for i in range(args.steps):
             ierr = op.apply_operator(m, dvg_d, dng_d, TR2)
+            ev[i + 1].record()
             st = op.stats()
             launches += st["launches"]
             iters.append(st["cg_iterations"]); act_sum += st["cg_active_sum"]; boxes += st["fft_boxes"]
-        e1.record()
         torch.cuda.synchronize()
         barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1))
+        clk.end = len(clk.lines)
+    finally:
+        clk.__exit__(None, None, None)
+    ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+    step_ms = [round(ev[i].elapsed_time(ev[i + 1]), 2) for i in range(args.steps)]
     # roofline: the same steps with CUDA events on the library stream around the
     # dominant stage (the local-potential FFT); events need the eager loop, and
     # cost 2-5% of a step, so they stay out of the timed region above
@@ -309,7 +318,8 @@ def run_b200(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": steps_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian pseudo-atoms, exact ground state)",
             "config": _config(args, {"parallelism": f"perturbation shards x{world}", "npw": npw,
-                                     "cg_iterations": iters, "system_build_s": round(t_sys, 1)}),
+                                     "cg_iterations": iters, "system_build_s": round(t_sys, 1),
+                                     "step_ms": step_ms}),
             "clocks": clk.summary(),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(m * npw * 16),
                     "d2h_bytes_per_step": int(m * npw * 16), "matches_device_path": e2e_ok},
