@@ -201,6 +201,10 @@ typedef struct wb_davidson_params {
   double tr2_dfpt;     /* PCG threshold of the iterations                        */
   double trev_pdep;    /* absolute eigenvalue convergence                        */
   double trev_pdep_rel;/* relative eigenvalue convergence                        */
+  int n_steps_write_restart; /* 0: no restart files; k: write them every k iterations
+                                (k = 1: also after the two starting steps)         */
+  int restart;         /* 1: resume from restart_dir (wstat_calculation 'R')      */
+  const char* restart_dir;   /* wstat_restart_dir (Wstat/davidson_restart.f90 layout) */
 } wb_davidson_params;
 
 /* What davidson_diago_gamma reports (exec.davitr of wstat.json). */
@@ -224,6 +228,14 @@ typedef struct wb_davidson_info {
  * ev, their convergence flags in conv and, when pdep != NULL, the eigenvectors
  * [ld_pdep, n_pdep_eigen] (host memory).  The subspace eigensolver is a
  * Jacobi method on the GPU (diagox uses LAPACK DSYEV / cuSOLVER in WEST).
+ */
+/*
+ * Restart hand-off (Wstat/davidson_restart.f90:33-411, same files as WEST):
+ * restart_dir/summary.json (dav_iter, notcnv, nbase, conv, ev, ew), hr_vr.dat
+ * (Fortran unformatted sequential: hr then vr, n_pdep_basis^2 doubles each) and
+ * V<j>.dat / N<j>.dat (j = 000001..nbase, the pdep file format) are written at
+ * the reference's checkpoints and removed on convergence; with restart = 1 the
+ * solve resumes from them (dvg0 may then be NULL).
  */
 int wb_davidson(wb_ctx* ctx, const wb_davidson_params* params, const double* dvg0, int ld_dvg0, double* ev,
                 int* conv, double* pdep, int ld_pdep, wb_davidson_info* info);

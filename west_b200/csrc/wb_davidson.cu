@@ -295,13 +295,17 @@ struct Dav {
 
 extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double* dvg0, int ld_dvg0, double* ev_out,
                            int* conv_out, double* pdep, int ld_pdep, wb_davidson_info* info) {
-  if (!c || !p || !dvg0 || !ev_out) return fail(WB_ERR_ARG, "null argument");
+  if (!c || !p || !ev_out || (!dvg0 && !p->restart)) return fail(WB_ERR_ARG, "null argument");
+  if ((p->n_steps_write_restart > 0 || p->restart) && !p->restart_dir)
+    return fail(WB_ERR_ARG, "restart files need restart_dir");
+  if (p->n_steps_write_restart < 0) return fail(WB_ERR_ARG, "n_steps_write_restart < 0");
   const int nvec = p->n_pdep_eigen, nvecx = p->n_pdep_basis;
   if (nvec < 1 || nvecx < 2 * nvec)
     return fail(WB_ERR_ARG, "need n_pdep_eigen >= 1 and n_pdep_basis >= 2 n_pdep_eigen (davidson_diago.f90:107)");
   if (nvecx > 1024) return fail(WB_ERR_UNSUPPORTED, "n_pdep_basis > 1024 is not provided by the Jacobi eigensolver");
   if (p->n_pdep_maxiter < 1) return fail(WB_ERR_ARG, "n_pdep_maxiter < 1");
-  if (ld_dvg0 < c->npw || (pdep && ld_pdep < c->npw)) return fail(WB_ERR_ARG, "leading dimension smaller than npw");
+  if ((dvg0 && ld_dvg0 < c->npw) || (pdep && ld_pdep < c->npw))
+    return fail(WB_ERR_ARG, "leading dimension smaller than npw");
   const auto t0 = std::chrono::steady_clock::now();
   WB_CU(cudaSetDevice(c->device));
   WB_CU(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -340,20 +344,63 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
   WB_CU(cudaMemsetAsync(d.dng, 0, colb * nvecx, s));
   WB_CU(cudaMemsetAsync(d.hr, 0, sizeof(double) * nvecx * nvecx, s));
   WB_CU(cudaMemsetAsync(d.vr, 0, sizeof(double) * nvecx * nvecx, s));
-  WB_CU(cudaMemcpy2DAsync(d.dvg, colb, dvg0, sizeof(double2) * ld_dvg0, colb, nvec, cudaMemcpyHostToDevice, s));
   std::vector<double> ew(nvecx, 0.0), ev(nvec, 0.0), wtmp(nvec);
   std::vector<int> conv(nvec, 0);
   int nbase = nvec, notcnv = nvec, rc;
-  // starting steps (davidson_diago.f90:171-247)
-  if ((rc = d.mgs(0, nvec))) return rc;
-  if ((rc = d.apply(0, nvec, -1.0))) return rc;                          // lite solver
-  WB_CU(cudaMemcpyAsync(d.dvg, d.dng, colb * nvecx, cudaMemcpyDeviceToDevice, s));   // dvg = dng
-  if ((rc = d.mgs(0, nvec))) return rc;
-  if ((rc = d.apply(0, nvec, std::min(1e-4, 1e8 * p->tr2_dfpt)))) return rc;
-  if ((rc = d.build_hr(0, nvec, nvec))) return rc;
-  if ((rc = d.diagox(nbase, wtmp))) return rc;
-  for (int i = 0; i < nvec; ++i) ew[i] = ev[i] = wtmp[i];
-  int dav_iter = 0;
+  int dav_iter = -2;
+  // restart files (davidson_restart.f90): the state at the end of a step, the
+  // basis columns [0, nbase) and hr/vr copied to the host
+  auto checkpoint = [&]() -> int {
+    DavRestart r;
+    r.dav_iter = dav_iter;
+    r.notcnv = notcnv;
+    r.nbase = nbase;
+    r.conv = conv;
+    r.ev = ev;
+    r.ew = ew;
+    r.hr.resize((size_t)nvecx * nvecx);
+    r.vr.resize((size_t)nvecx * nvecx);
+    std::vector<double> hv((size_t)2 * d.ld * nbase), hn((size_t)2 * d.ld * nbase);
+    WB_CU(cudaMemcpyAsync(hv.data(), d.dvg, colb * nbase, cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaMemcpyAsync(hn.data(), d.dng, colb * nbase, cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaMemcpyAsync(r.hr.data(), d.hr, sizeof(double) * r.hr.size(), cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaMemcpyAsync(r.vr.data(), d.vr, sizeof(double) * r.vr.size(), cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaStreamSynchronize(s));
+    return dav_restart_write(p->restart_dir, r, nvec, nvecx, d.npw, hv.data(), hn.data(), d.ld);
+  };
+  const int nsw = p->n_steps_write_restart;
+  if (p->restart) {                                                        // wstat_calculation 'R' (:154-159)
+    DavRestart r;
+    std::vector<double> hv((size_t)2 * d.ld * nvecx), hn((size_t)2 * d.ld * nvecx);
+    if ((rc = dav_restart_read(p->restart_dir, r, nvec, nvecx, d.npw, hv.data(), hn.data(), d.ld))) return rc;
+    WB_CU(cudaMemcpyAsync(d.dvg, hv.data(), colb * r.nbase, cudaMemcpyHostToDevice, s));
+    WB_CU(cudaMemcpyAsync(d.dng, hn.data(), colb * r.nbase, cudaMemcpyHostToDevice, s));
+    WB_CU(cudaMemcpyAsync(d.hr, r.hr.data(), sizeof(double) * r.hr.size(), cudaMemcpyHostToDevice, s));
+    WB_CU(cudaMemcpyAsync(d.vr, r.vr.data(), sizeof(double) * r.vr.size(), cudaMemcpyHostToDevice, s));
+    WB_CU(cudaStreamSynchronize(s));
+    dav_iter = r.dav_iter;
+    nbase = r.nbase;
+    notcnv = r.notcnv;
+    conv = r.conv;
+    ev = r.ev;
+    ew = r.ew;
+  } else {                                                                 // from scratch (:161-199)
+    WB_CU(cudaMemcpy2DAsync(d.dvg, colb, dvg0, sizeof(double2) * ld_dvg0, colb, nvec, cudaMemcpyHostToDevice, s));
+    if ((rc = d.mgs(0, nvec))) return rc;
+    if ((rc = d.apply(0, nvec, -1.0))) return rc;                          // lite solver
+    dav_iter = -1;
+    if (nsw == 1 && (rc = checkpoint())) return rc;
+  }
+  if (dav_iter == -1) {                                                    // extra starting step (:204-247)
+    WB_CU(cudaMemcpyAsync(d.dvg, d.dng, colb * nvecx, cudaMemcpyDeviceToDevice, s));   // dvg = dng
+    if ((rc = d.mgs(0, nvec))) return rc;
+    if ((rc = d.apply(0, nvec, std::min(1e-4, 1e8 * p->tr2_dfpt)))) return rc;
+    if ((rc = d.build_hr(0, nvec, nvec))) return rc;
+    if ((rc = d.diagox(nbase, wtmp))) return rc;
+    for (int i = 0; i < nvec; ++i) ew[i] = ev[i] = wtmp[i];
+    dav_iter = 0;
+    if (nsw == 1 && (rc = checkpoint())) return rc;
+  }
   bool refreshed = false;
   for (int kter = 1; kter <= p->n_pdep_maxiter; ++kter) {                 // :259
     ++dav_iter;
@@ -391,6 +438,8 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
       if (notcnv == 0 || kter == p->n_pdep_maxiter) {
         if ((rc = d.refresh(d.dvg, nbase, nvec))) return rc;              // eigenvectors for the caller
         refreshed = true;
+        if (notcnv == 0 && p->restart_dir && (nsw > 0 || p->restart))
+          dav_restart_clear(p->restart_dir, nvecx);                       // :376
         break;
       }
       if ((rc = d.refresh(d.dvg, nbase, nvec))) return rc;                // :397-398
@@ -402,6 +451,7 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
       WB_CU(cudaMemcpyAsync(d.vr, eye.data(), sizeof(double) * eye.size(), cudaMemcpyHostToDevice, s));
       WB_CU(cudaStreamSynchronize(s));
     }
+    if (nsw > 0 && dav_iter % nsw == 0 && (rc = checkpoint())) return rc;  // :421-422
   }
   if (!refreshed && (rc = d.refresh(d.dvg, nbase, nvec))) return rc;
   if (pdep)

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace wb {
 
 // Stick decomposition of the Gamma half sphere (built on the host from nl).
@@ -45,6 +47,22 @@ bool fft_fusable(int n, const StickTab& st);
 // kernels: the fused local-potential layout (fused) or the padded-row one,
 // for elem_bytes 8 (FP32 complex) or 16 (FP64 complex)
 int fft_plane_offset(int n, bool fused, int elem_bytes, int x, int y);
+
+// Davidson restart hand-off in WEST's layout (Wstat/davidson_restart.f90):
+// <dir>/summary.json (dav_iter, notcnv, nbase, conv, ev, ew), <dir>/hr_vr.dat
+// (Fortran unformatted: hr then vr, n_pdep_basis^2 doubles each) and the basis
+// <dir>/V<j>.dat, N<j>.dat (j = 000001.., pdep file format) for j <= nbase.
+// dvg/dng are host arrays [ld, nbase] complex in WEST's G order.
+struct DavRestart {
+  int dav_iter = 0, notcnv = 0, nbase = 0;
+  std::vector<int> conv;
+  std::vector<double> ev, ew, hr, vr;
+};
+int dav_restart_write(const char* dir, const DavRestart& r, int nvec, int nvecx, int npw, const double* dvg,
+                      const double* dng, long ld);
+int dav_restart_read(const char* dir, DavRestart& r, int nvec, int nvecx, int npw, double* dvg, double* dng,
+                     long ld);
+void dav_restart_clear(const char* dir, int nvecx);
 void fft_zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks);
 void fft_plane_vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs);
 void fft_zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, const float2* P,

@@ -57,7 +57,8 @@ class WbStats(ctypes.Structure):
 
 class WbDavidsonParams(ctypes.Structure):
     _fields_ = [("n_pdep_eigen", _i), ("n_pdep_basis", _i), ("n_pdep_maxiter", _i),
-                ("tr2_dfpt", _d), ("trev_pdep", _d), ("trev_pdep_rel", _d)]
+                ("tr2_dfpt", _d), ("trev_pdep", _d), ("trev_pdep_rel", _d),
+                ("n_steps_write_restart", _i), ("restart", _i), ("restart_dir", ctypes.c_char_p)]
 
 
 class WbDavidsonInfo(ctypes.Structure):

@@ -16,6 +16,7 @@ copies.
 from __future__ import annotations
 
 import ctypes
+import os
 import sys
 
 import numpy as np
@@ -145,20 +146,30 @@ class ResponseOperator:
 
 
     def davidson(self, dvg0, n_pdep_eigen, n_pdep_times=4, n_pdep_maxiter=100, tr2_dfpt=1e-16,
-                 trev_pdep=1e-3, trev_pdep_rel=1e-1):
+                 trev_pdep=1e-3, trev_pdep_rel=1e-1, restart_dir=None, n_steps_write_restart=0,
+                 restart=False):
         """PDEP Davidson (davidson_diago_gamma, Wstat/davidson_diago.f90:31) from the
         starting basis dvg0 [npwqx, >= n_pdep_eigen] (do_randomize's output).
+        With restart_dir, writes WEST's restart files every n_steps_write_restart
+        iterations (davidson_restart.f90) and, with restart=True (wstat_calculation
+        'R'), resumes from them (dvg0 may then be None).
         Returns (ev, conv, pdep eigenvectors [npwqx, n_pdep_eigen], info dict)."""
         nvec = int(n_pdep_eigen)
+        rdir = None if restart_dir is None else os.fsencode(restart_dir)
         prm = _lib.WbDavidsonParams(nvec, nvec * int(n_pdep_times), int(n_pdep_maxiter), float(tr2_dfpt),
-                                    float(trev_pdep), float(trev_pdep_rel))
-        d0 = np.asfortranarray(dvg0[:, :nvec], dtype=np.complex128)
+                                    float(trev_pdep), float(trev_pdep_rel), int(n_steps_write_restart),
+                                    int(bool(restart)), rdir)
+        if dvg0 is None:
+            d0, ld0, npwx = None, 0, int(self.system.npw)
+        else:
+            d0 = np.asfortranarray(dvg0[:, :nvec], dtype=np.complex128)
+            ld0, npwx = d0.shape[0], d0.shape[0]
         ev = np.zeros(nvec)
         conv = np.zeros(nvec, dtype=np.int32)
-        vec = np.zeros((d0.shape[0], nvec), dtype=np.complex128, order="F")
+        vec = np.zeros((npwx, nvec), dtype=np.complex128, order="F")
         info = _lib.WbDavidsonInfo()
-        _lib.check(self._lib.wb_davidson(self._ctx, ctypes.byref(prm), _ptr(d0), d0.shape[0], _ptr(ev), _ptr(conv),
-                                         _ptr(vec), vec.shape[0], ctypes.byref(info)))
+        _lib.check(self._lib.wb_davidson(self._ctx, ctypes.byref(prm), None if d0 is None else _ptr(d0), ld0,
+                                         _ptr(ev), _ptr(conv), _ptr(vec), vec.shape[0], ctypes.byref(info)))
         if self.verbose and not info.converged:
             sys.stdout.write(f"     WARNING : {info.notcnv:5d} eigenvalues not converged in chidiago\n")
         return ev, conv.astype(bool), vec, {k: getattr(info, k) for k, _ in info._fields_}
