@@ -230,6 +230,21 @@ typedef struct wb_davidson_info {
  * Jacobi method on the GPU (diagox uses LAPACK DSYEV / cuSOLVER in WEST).
  */
 /*
+ * Operator hook of the Davidson: when set, wb_davidson calls fn instead of its
+ * own apply_operator for every batch of new basis vectors.  dvg/dng are device
+ * pointers to the batch (columns col0 .. col0+m-1 of the basis, WEST's G order,
+ * leading dimension ld); fn writes dng = sqvc chi0 sqvc dvg with PCG threshold
+ * tr2 (< 0: lite solver) and returns 0 or a wb error code.  The hook is how the
+ * perturbation-sharded multi-GPU Davidson runs: each rank applies the operator
+ * to its cyclic share of the columns (WEST's pert%l2g, davidson_diago.f90:
+ * 185-196,313-324) and one all-gather of dng (NCCL over NVLink) gives every rank
+ * the whole batch; the small dense steps then run redundantly on every rank.
+ * fn = NULL restores the library's own apply_operator.
+ */
+typedef int (*wb_apply_fn)(void* user, int col0, int m, const double* dvg, double* dng, int ld, double tr2);
+int wb_davidson_set_apply(wb_ctx* ctx, wb_apply_fn fn, void* user);
+
+/*
  * Restart hand-off (Wstat/davidson_restart.f90:33-411, same files as WEST):
  * restart_dir/summary.json (dav_iter, notcnv, nbase, conv, ev, ew), hr_vr.dat
  * (Fortran unformatted sequential: hr then vr, n_pdep_basis^2 doubles each) and

@@ -70,3 +70,49 @@ def test_two_rank_gloo_sharding_matches_single_rank():
         p.join(timeout=300)
         assert p.exitcode == 0
     assert q.get(timeout=10) < 1e-13
+
+
+@pytest.mark.parametrize("col0,m,nranks", [(0, 4, 2), (5, 7, 2), (8, 3, 4), (16, 1, 3)])
+def test_batch_rows_split_the_batch(col0, m, nranks):
+    from west_b200.distribute import batch_owner_rows
+    rows = [batch_owner_rows(col0, m, nranks, r) for r in range(nranks)]
+    assert sorted(sum(rows, [])) == list(range(m))
+    for r in range(nranks):
+        assert all((col0 + i) % nranks == r for i in rows[r])
+
+
+def _gather_main(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    from west_b200.distribute import batch_owner_rows, gather_batch
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g = torch.Generator().manual_seed(3)
+        ok = True
+        for col0, m in ((0, 4), (5, 7), (9, 1)):
+            x = torch.randn((m, 11), generator=g, dtype=torch.complex128)    # same on every rank
+            rows = batch_owner_rows(col0, m, world, rank)
+            local = 2.0 * x[rows] + 1j                                        # this rank's share of the operator
+            full = gather_batch(local, col0, m, world, rank)
+            ok = ok and bool(torch.equal(full, 2.0 * x + 1j))
+        out.put((rank, ok))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_batch_gather():
+    """The exchange step of the sharded Davidson apply: each rank's rows of a batch,
+    all-gathered, reassemble the batch in its original order on every rank."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    res = dict(q.get(timeout=10) for _ in range(2))
+    assert res == {0: True, 1: True}

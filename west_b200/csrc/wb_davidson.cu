@@ -253,9 +253,16 @@ struct Dav {
   int apply(int col0, int n, double tr2) {
     unconv.assign(std::max(n, 1), 0);
     const auto t0 = std::chrono::steady_clock::now();
-    const int rc = wb_apply_operator_device(c, n, reinterpret_cast<const double*>(dvg + (long)col0 * ld), (int)ld,
-                                            reinterpret_cast<double*>(dng + (long)col0 * ld), (int)ld, tr2, 1,
-                                            unconv.data());
+    const double* x = reinterpret_cast<const double*>(dvg + (long)col0 * ld);
+    double* y = reinterpret_cast<double*>(dng + (long)col0 * ld);
+    int rc;
+    if (c->dav_apply) {
+      WB_CU(cudaStreamSynchronize(s));  // the hook runs on its own streams
+      rc = c->dav_apply(c->dav_apply_user, col0, n, x, y, (int)ld, tr2);
+      if (rc) return fail(rc, "Davidson operator hook failed (code " + std::to_string(rc) + ")");
+    } else {
+      rc = wb_apply_operator_device(c, n, x, (int)ld, y, (int)ld, tr2, 1, unconv.data());
+    }
     apply_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     ++apply_calls;
     applied += n;
@@ -292,6 +299,13 @@ struct Dav {
 };
 
 }  // namespace
+
+extern "C" int wb_davidson_set_apply(wb_ctx* c, wb_apply_fn fn, void* user) {
+  if (!c) return fail(WB_ERR_ARG, "null context");
+  c->dav_apply = fn;
+  c->dav_apply_user = fn ? user : nullptr;
+  return WB_OK;
+}
 
 extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double* dvg0, int ld_dvg0, double* ev_out,
                            int* conv_out, double* pdep, int ld_pdep, wb_davidson_info* info) {

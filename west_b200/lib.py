@@ -25,7 +25,7 @@ EXPORTS = (
     "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
     "wb_apply_operator_device_noalloc",
     "wb_apply_operator_multi", "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling",
-    "wb_set_graphs", "wb_get_tuning", "wb_set_autotune", "wb_davidson",
+    "wb_set_graphs", "wb_get_tuning", "wb_set_autotune", "wb_davidson", "wb_davidson_set_apply",
     "wb_pdep_db_write",
     "wb_pdep_db_read", "wb_last_error", "wb_version",
 )
@@ -59,6 +59,11 @@ class WbDavidsonParams(ctypes.Structure):
     _fields_ = [("n_pdep_eigen", _i), ("n_pdep_basis", _i), ("n_pdep_maxiter", _i),
                 ("tr2_dfpt", _d), ("trev_pdep", _d), ("trev_pdep_rel", _d),
                 ("n_steps_write_restart", _i), ("restart", _i), ("restart_dir", ctypes.c_char_p)]
+
+
+# int (*wb_apply_fn)(void* user, int col0, int m, const double* dvg, double* dng, int ld, double tr2)
+WB_APPLY_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_int, ctypes.c_double)
 
 
 class WbDavidsonInfo(ctypes.Structure):
@@ -101,6 +106,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.wb_set_autotune.argtypes = [_p, _i]
     lib.wb_apply_operator_multi.argtypes = [_i, _p, _p, _p, _p, _p, _p, _d, _i, _p, _i]
     lib.wb_get_stats.argtypes = [_p, ctypes.POINTER(WbStats)]
+    lib.wb_davidson_set_apply.argtypes = [_p, WB_APPLY_FN, _p]
     lib.wb_davidson.argtypes = [_p, ctypes.POINTER(WbDavidsonParams), _p, _i, _p, _p, _p, _i,
                                 ctypes.POINTER(WbDavidsonInfo)]
     lib.wb_pdep_db_write.argtypes = [ctypes.c_char_p, _i, _p, _p, _i, _p, _p, _i, _i]

@@ -107,6 +107,12 @@ class ResponseOperator:
         """Tune launch shapes on the first batch of each form (default) or keep the built-in ones."""
         _lib.check(self._lib.wb_set_autotune(self._ctx, int(bool(enable))))
 
+    def set_davidson_apply(self, fn):
+        """Operator hook of davidson() (wb_davidson_set_apply): a lib.WB_APPLY_FN, or
+        None for the library's own apply_operator.  See distribute.ShardedDavidsonApply."""
+        self._dav_hook = fn
+        _lib.check(self._lib.wb_davidson_set_apply(self._ctx, fn if fn is not None else _lib.WB_APPLY_FN(), None))
+
     def tuning(self) -> dict:
         """Launch shapes the autotuner chose (wb_get_tuning)."""
         t = _lib.WbTuning()
