@@ -383,39 +383,60 @@ __global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict
 
 // RHS of the Sternheimer equation, dfpt_module.f90:245-260:
 // (psi_v1(r) + i psi_v2(r)) * dv_p(r) / N^3 -> forward -> sticks
+// One CTA per (plane z, perturbation p) loops over the band pairs: dv_p(r) of
+// the plane is read once into registers (thread t owns elements t + PNT q)
+// instead of once per band pair, and the psi planes come from L2 (the grid of
+// one CTA per band pair read 8.6 GB of boxes per c2 call; 1.7 against 2.1 ms).
 template <int N, bool PR>
-__global__ void __launch_bounds__(PNT) k_plane_rhs(const double2* __restrict__ evcr,
+__global__ void __launch_bounds__(PNT, 2) k_plane_rhs(const double2* __restrict__ evcr,
                                                    const double2* __restrict__ dvbox, int npv,
                                                    StickTab st, double2* __restrict__ sticks,
                                                    const double2* __restrict__ twg) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* tw = reinterpret_cast<double2*>(smraw);
   double2* pl = tw + 2 * N;
-  const int z = blockIdx.x, k = blockIdx.y, p = blockIdx.z;
+  const int z = blockIdx.x, p = blockIdx.y;
   load_tw<N>(tw, twg);
-  const double2* ps = evcr + ((long)k * N + z) * N * N;
+  constexpr int PER = (N * N + PNT - 1) / PNT;
+  constexpr double inv = 1.0 / ((double)N * N * N);
   const double2* dv = dvbox + ((long)(p >> 1) * N + z) * N * N;
   const bool hi = p & 1;
-  constexpr double inv = 1.0 / ((double)N * N * N);
-  for (int e = threadIdx.x; e < N * N; e += PNT) {
-    const double2 d = dv[e];
-    const double w = (hi ? d.y : d.x) * inv;
-    pl[Plane<N>::at_lin(e)] = cscale(ps[e], w);
+  double w[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * PNT;
+    w[q] = 0.0;
+    if (e < N * N) {
+      const double2 d = dv[e];
+      w[q] = (hi ? d.y : d.x) * inv;
+    }
   }
-  __syncthreads();
-  plane_fft_rows<N, -1, PR>(pl, tw);
-  plane_fft_cols<N, -1, PR>(pl, st, tw);
-  const long item = (long)p * npv + k;
-  plane_gather<N>(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+  for (int k = 0; k < npv; ++k) {
+    const double2* ps = evcr + ((long)k * N + z) * N * N;
+    __syncthreads();  // the previous band pair's gather is done with the plane
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e = threadIdx.x + q * PNT;
+      if (e < N * N) pl[Plane<N>::at_lin(e)] = cscale(ps[e], w[q]);
+    }
+    __syncthreads();
+    plane_fft_rows<N, -1, PR>(pl, tw);
+    plane_fft_cols<N, -1, PR>(pl, st, tw);
+    const long item = (long)p * npv + k;
+    plane_gather<N>(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+  }
 }
 
 // Density response, dfpt_module.f90:403-423 and :478:
 // drho_p(r) = sum_v occ_v psi_v(r) dpsi_v(r), two perturbations per CTA,
 // then (drho_p1 + i drho_p2) * scale -> forward -> sticks.
-// acc is per-CTA scratch in global memory ([pp][z][N*N] double2), owned
-// element-wise by the thread that writes it.
+// acc is per-CTA scratch in global memory ([pp][z][N*N] double2) that parks
+// the first perturbation's density once; each element is owned by the thread
+// that writes it.  The band sums run in registers (a read-modify-write of acc
+// per band pair made the kernel DRAM-bound: 12.6 GB per c2 call); two CTAs per
+// SM (a few hundred bytes of spills) beat one (2.5 against 2.9 ms per c2 call).
 template <int N, bool PR>
-__global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ dsticks,
+__global__ void __launch_bounds__(PNT, 2) k_plane_drho(const double2* __restrict__ dsticks,
                                                     const double2* __restrict__ evcr,
                                                     const double* __restrict__ occ, int nocc,
                                                     int mb, StickTab st, double2* __restrict__ acc,
@@ -427,14 +448,16 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
   const int z = blockIdx.x, pp = blockIdx.y;
   const int npv = (nocc + 1) / 2;
   load_tw<N>(tw, twg);
+  // a perturbation's density of this plane is accumulated in registers (thread t
+  // owns plane elements t + PNT q); the first of the two is parked in acc once
   double2* ac = acc + ((long)pp * N + z) * N * N;
+  constexpr int PER = (N * N + PNT - 1) / PNT;
+  double a[PER];
   for (int pi = 0; pi < 2; ++pi) {
     const int p = 2 * pp + pi;
-    if (p >= mb) {
-      for (int e = threadIdx.x; e < N * N; e += PNT) ac[e].y = 0.0;
-      break;
-    }
-    for (int k = 0; k < npv; ++k) {
+#pragma unroll
+    for (int q = 0; q < PER; ++q) a[q] = 0.0;
+    for (int k = 0; p < mb && k < npv; ++k) {
       const long item = (long)p * npv + k;
       __syncthreads();
       plane_zero<N, PR>(pl, st);
@@ -446,19 +469,29 @@ __global__ void __launch_bounds__(PNT) k_plane_drho(const double2* __restrict__ 
       const double o1 = occ[2 * k];
       const double o2 = (2 * k + 1 < nocc) ? occ[2 * k + 1] : 0.0;
       const double2* ps = evcr + ((long)k * N + z) * N * N;
-      for (int e = threadIdx.x; e < N * N; e += PNT) {
-        const double2 d = pl[Plane<N>::at_lin(e)], s = ps[e];
-        const double c = fma(o1 * s.x, d.x, o2 * s.y * d.y);
-        if (pi == 0) {
-          if (k == 0) ac[e].x = c; else ac[e].x += c;
-        } else {
-          if (k == 0) ac[e].y = c; else ac[e].y += c;
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int e = threadIdx.x + q * PNT;
+        if (e < N * N) {
+          const double2 d = pl[Plane<N>::at_lin(e)], s = ps[e];
+          a[q] += fma(o1 * s.x, d.x, o2 * s.y * d.y);
         }
+      }
+    }
+    if (pi == 0) {
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int e = threadIdx.x + q * PNT;
+        if (e < N * N) ac[e].x = a[q];
       }
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < N * N; e += PNT) pl[Plane<N>::at_lin(e)] = cscale(ac[e], scale);
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * PNT;
+    if (e < N * N) pl[Plane<N>::at_lin(e)] = make_double2(ac[e].x * scale, a[q] * scale);
+  }
   __syncthreads();
   plane_fft_rows<N, -1, PR>(pl, tw);
   plane_fft_cols<N, -1, PR>(pl, st, tw);
@@ -741,7 +774,7 @@ struct FftN {
   }
   static void rhs(const FftArgs& f, const double2* evcr, const double2* dvbox, int npv, int mb, double2* sticks) {
     if (mb <= 0) return;
-    const dim3 g(N, npv, mb);
+    const dim3 g(N, mb);
     if (f.st.prune)
       k_plane_rhs<N, true><<<g, PNT, psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
     else
