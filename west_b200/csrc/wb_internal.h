@@ -128,8 +128,6 @@ void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const d
 // nact_host may be null (no host copy); nsys_dev, if given, overrides nsys
 void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int* nact_dev, int* nact_host,
                 cudaStream_t s, const int* nsys_dev = nullptr);
-void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
-               long ld, cudaStream_t s, const int* dn = nullptr);
 // One PCG step after the operator: the update of iteration `iter` and, unless
 // iter == maxiter, the preconditioning / rho / convergence test / direction of
 // iteration iter + 1 (the iteration comes from *iter_dev when given).
@@ -151,8 +149,6 @@ void loop_bucket(cudaGraphConditionalHandle h, const int* nact, int* st, int min
 void cg_prec_rho32(const int* act, int nact, const float2* g, float2* P, const double* iprec, int nocc,
                    double* rho_prev, unsigned char* conv, int iter, double eta, const double* rel, double floor,
                    int npw, long ld, cudaStream_t s, const int* dn = nullptr, const int* iter_dev = nullptr);
-void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
-                 cudaStream_t s, const int* dn = nullptr);
 void refine_residual(const int* act, int nact, const double2* B, const double2* T, const double* iprec, int nocc,
                      double tr2, unsigned char* conv, double* rho0, float2* g32, float2* d32, int npw, long ld,
                      cudaStream_t s);

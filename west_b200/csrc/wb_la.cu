@@ -481,55 +481,12 @@ void cg_compact(const unsigned char* conv, int nsys, int* act, int2* items, int*
   if (nact_host) cudaMemcpyAsync(nact_host, nact_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
 }
 
-// a = <P|g>, c = <P|T> (Gamma); x -= (a/c) P ; g -= (a/c) T     (:253-322)
-template <class C>
-__global__ void __launch_bounds__(256) k_cg_update(const int* __restrict__ act, const int* dn, C* __restrict__ x,
-                                                   C* __restrict__ g, const C* __restrict__ P,
-                                                   const C* __restrict__ T, int npw, long ld) {
-  using R = real_t<C>;
-  __shared__ double red[16];
-  const int n = dev_count(dn, gridDim.x);
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
-    const int j = act[b];
-    const C* pj = P + (long)j * ld;
-    const C* tj = T + (long)j * ld;
-    C* gj = g + (long)j * ld;
-    C* xj = x + (long)j * ld;
-    double a = 0.0, c = 0.0;
-    for (int i = threadIdx.x; i < npw; i += 256) {
-      const C p = pj[i], gv = gj[i], t = tj[i];
-      double da = fma((double)p.x, (double)gv.x, (double)p.y * (double)gv.y);
-      double dc = fma((double)p.x, (double)t.x, (double)p.y * (double)t.y);
-      if (i == 0) { da -= 0.5 * (double)p.x * (double)gv.x; dc -= 0.5 * (double)p.x * (double)t.x; }
-      a += da;
-      c += dc;
-    }
-    const double2 s = block_sum2<256>(a, c, red);
-    const double rd = (2.0 * s.x) / (2.0 * s.y);
-    const R r = R(rd);
-    for (int i = threadIdx.x; i < npw; i += 256) {
-      const C p = pj[i], t = tj[i];
-      C xv = xj[i], gv = gj[i];
-      xj[i] = mkc<C>(fma(-r, p.x, xv.x), fma(-r, p.y, xv.y));
-      gj[i] = mkc<C>(fma(-r, t.x, gv.x), fma(-r, t.y, gv.y));
-    }
-  }
-}
-void cg_update(const int* act, int nact, double2* x, double2* g, const double2* P, const double2* T, int npw,
-               long ld, cudaStream_t s, const int* dn) {
-  if (nact <= 0) return;
-  k_cg_update<double2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, x, g, P, T, npw, ld);
-}
-void cg_update32(const int* act, int nact, float2* x, float2* g, const float2* P, const float2* T, int npw, long ld,
-                 cudaStream_t s, const int* dn) {
-  if (nact <= 0) return;
-  k_cg_update<float2><<<sys_grid(nact, dn), 256, 0, s>>>(act, dn, x, g, P, T, npw, ld);
-}
 
 // One PCG step after the operator, in one kernel: the update of iteration
-// `iter` (k_cg_update: a = <P|g>, c = <P|T>, x -= a/c P, g -= a/c T) and,
-// unless iter == maxiter, iteration iter + 1's preconditioning, rho, test and
-// direction (k_cg_prec_rho: h = M g, rho = <h|g>, P = -h + rho/rho_prev P).
+// `iter` (a = <P|g>, c = <P|T> with the Gamma dot, x -= a/c P, g -= a/c T;
+// linsolve_sternheimer_m_wfcts.f90:253-329) and, unless iter == maxiter,
+// iteration iter + 1's preconditioning, rho, test and direction (as
+// k_cg_prec_rho: h = M g, rho = <h|g>, P = -h + rho/rho_prev P).
 // One CTA per system; the new g is preconditioned and its rho summed in the
 // update's own pass, and the direction pass re-reads g (just written) and P
 // (read twice already) from L2, so the vectors make fewer trips to DRAM than
