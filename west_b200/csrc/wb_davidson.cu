@@ -92,7 +92,8 @@ __global__ void k_mgs_axpy(double2* __restrict__ a, long ld, int npw, int k, int
 
 // Cyclic two-sided Jacobi on the upper triangle of hr[:n, :n] (what DSYEV 'U'
 // reads in matdiago_dsy, Tools/linear_algebra_kernel.f90:84), round-robin
-// ordering so each round rotates n/2 disjoint (p, q) planes in parallel.
+// ordering so each round rotates n/2 disjoint (p, q) planes in parallel,
+// applying J^T A J block by block in one pass (two barriers per round).
 // One CTA; A and V row-major in shared memory when in_smem (n <= kJacobiSmemN),
 // else in global scratch.  Writes the nsel lowest eigenvalues to w and their
 // eigenvectors to vr(:, 0:nsel) (ld ldv).
@@ -166,24 +167,47 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ hr, 
         cs[k] = c; sn[k] = s; pp[k] = p; qq[k] = q;
       }
       __syncthreads();
-      for (int e = tid; e < npairs * n; e += nt) {      // rows: A <- J^T A
-        const int k = e / n, j = e % n;
-        const int p = pp[k], q = qq[k];
-        if (q >= n || sn[k] == 0.0) continue;
-        const double c = cs[k], s = sn[k];
-        const double ap = A[p * n + j], aq = A[q * n + j];
-        A[p * n + j] = c * ap - s * aq;
-        A[q * n + j] = s * ap + c * aq;
+      // A <- J^T A J in one pass: the round's planes are disjoint, so each 2x2
+      // block (rows p1, q1 of plane k1; columns p2, q2 of plane k2) is owned by
+      // one thread, which rotates its rows, then its columns (the same
+      // arithmetic as a row pass followed by a column pass); V <- V J alongside
+      for (int e = tid; e < npairs * npairs; e += nt) {
+        const int k1 = e / npairs, k2 = e % npairs;
+        const int p1 = pp[k1], q1 = qq[k1], p2 = pp[k2], q2 = qq[k2];
+        const bool r2 = q1 < n, c2 = q2 < n;  // the padding index of odd n has no row / column
+        const double ca = cs[k1], sa = sn[k1], cb = cs[k2], sb = sn[k2];
+        const double a = A[p1 * n + p2];
+        const double b = c2 ? A[p1 * n + q2] : 0.0;
+        const double cc = r2 ? A[q1 * n + p2] : 0.0;
+        const double d = (r2 && c2) ? A[q1 * n + q2] : 0.0;
+        double ra = a, rb = b, rc = cc, rd = d;
+        if (r2 && sa != 0.0) {
+          ra = ca * a - sa * cc;
+          rc = sa * a + ca * cc;
+          rb = ca * b - sa * d;
+          rd = sa * b + ca * d;
+        }
+        if (c2 && sb != 0.0) {
+          A[p1 * n + p2] = cb * ra - sb * rb;
+          A[p1 * n + q2] = sb * ra + cb * rb;
+          if (r2) {
+            A[q1 * n + p2] = cb * rc - sb * rd;
+            A[q1 * n + q2] = sb * rc + cb * rd;
+          }
+        } else {
+          A[p1 * n + p2] = ra;
+          if (c2) A[p1 * n + q2] = rb;
+          if (r2) {
+            A[q1 * n + p2] = rc;
+            if (c2) A[q1 * n + q2] = rd;
+          }
+        }
       }
-      __syncthreads();
-      for (int e = tid; e < npairs * n; e += nt) {      // columns: A <- A J, V <- V J
+      for (int e = tid; e < npairs * n; e += nt) {      // V <- V J
         const int k = e / n, i = e % n;
         const int p = pp[k], q = qq[k];
         if (q >= n || sn[k] == 0.0) continue;
         const double c = cs[k], s = sn[k];
-        const double ap = A[i * n + p], aq = A[i * n + q];
-        A[i * n + p] = c * ap - s * aq;
-        A[i * n + q] = s * ap + c * aq;
         const double vp = V[i * n + p], vq = V[i * n + q];
         V[i * n + p] = c * vp - s * vq;
         V[i * n + q] = s * vp + c * vq;
