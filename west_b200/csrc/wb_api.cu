@@ -598,9 +598,17 @@ bool graph_mode(const wb_ctx* c) { return c->use_graphs && c->prof == 0; }
 constexpr int kMinBucketItems = 16;
 
 template <class Pass>
-int capture_loop(wb_ctx* c, wb_ctx::LoopGraph& lg, std::vector<const void*> key, double tr2, int cap, const int* dn,
-                 int* st, bool shared_budget, Pass pass) {
-  if (lg.exec && lg.key == key && lg.tr2 == tr2) return WB_OK;
+int capture_loop(wb_ctx* c, wb_ctx::LoopCache& cache, std::vector<const void*> key, double tr2, int cap,
+                 const int* dn, int* st, bool shared_budget, Pass pass) {
+  for (int i = 0; i < 2; ++i) {
+    const wb_ctx::LoopGraph& g = cache.slot[i];
+    if (g.exec && g.key == key && g.tr2 == tr2) {
+      cache.last = i;
+      return WB_OK;
+    }
+  }
+  cache.last = 1 - cache.last;  // replace the least recently used graph
+  wb_ctx::LoopGraph& lg = cache.slot[cache.last];
   lg.release();
   const int cap_items = (cap + 1) / 2;
   int nb = 1;
@@ -759,7 +767,7 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     }
     if (graph && c->maxiter > 0) {
       loop_init(st, nsys, false, s);
-      WB_CU(cudaGraphLaunch(c->loop32.exec, s));
+      WB_CU(cudaGraphLaunch(c->loop32.cur(), s));
     }
     for (int it = 1; !graph && it <= c->maxiter; ++it) {
       WB_CU(cudaStreamSynchronize(s));
@@ -896,7 +904,7 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
       });
       if (rc) return rc;
       loop_init(st, nsys, true, s);
-      WB_CU(cudaGraphLaunch(c->loop64.exec, s));
+      WB_CU(cudaGraphLaunch(c->loop64.cur(), s));
       WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
       WB_CU(cudaStreamSynchronize(s));
       iters = c->loop_host[2];

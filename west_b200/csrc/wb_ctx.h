@@ -91,7 +91,19 @@ struct wb_ctx {
       key.clear();
     }
   };
-  LoopGraph loop64, loop32;
+  // two graphs per form: a Davidson alternates tr2 (1e-4 in its extra starting
+  // step, tr2_dfpt in its iterations), and re-instantiating the graph at each
+  // change cost tens of ms per solve
+  struct LoopCache {
+    LoopGraph slot[2];
+    int last = 0;  // the slot of the latest capture or hit
+    cudaGraphExec_t cur() const { return slot[last].exec; }
+    void release() {
+      slot[0].release();
+      slot[1].release();
+    }
+  };
+  LoopCache loop64, loop32;
   int use_graphs = 1;
   int cap_nsys = 0;          // systems the per-call workspace is sized for (grow-only)
   // autotuned launch shapes (set on the first batch of each form, then fixed)
