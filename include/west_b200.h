@@ -178,15 +178,24 @@ int wb_set_graphs(wb_ctx* ctx, int enable);
  * they run (a host code whose GPU memory is owned by its own pool, a
  * latency-bound loop that cannot take cudaMalloc's implicit synchronisation,
  * an allocation policy that forbids allocations after set-up).  Same
- * arguments and results as wb_apply_operator_device; dvg and dng are device
- * buffers supplied by the caller.  Every per-call buffer comes from one
- * file-scope device array of WB_NOALLOC_SCRATCH_BYTES that each GPU loading
- * the library holds until the process exits; a call whose buffers do not fit
- * returns WB_ERR_ARG with the size it would need.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress), so make that
- * first call before any stream capture.  All calls, from every context on
- * the device, share the one array and its leftover contents: calls that
- * overlap on the GPU (other threads or streams) race and corrupt each other.
+ * arguments and results as wb_apply_operator_device in the FP64 form; dvg and
+ * dng are device buffers supplied by the caller.  Limits:
+ *   - FP64 only: on a context set to WB_PRECISION_MIXED it returns
+ *     WB_ERR_UNSUPPORTED;
+ *   - every per-call buffer comes from one file-scope device array of
+ *     WB_NOALLOC_SCRATCH_BYTES that each GPU loading the library holds until
+ *     the process exits; a call whose buffers do not fit returns WB_ERR_ARG
+ *     with the size it would need;
+ *   - the PCG loop runs eagerly (a host read of the active count per
+ *     iteration, no CUDA graph) with the built-in launch shapes (no
+ *     autotuning), and wb_get_stats reports only m, cg_iterations and
+ *     cg_active_sum for it;
+ *   - the first call on each context looks up the array's device address
+ *     (cudaGetSymbolAddress) with the context's device current, so make that
+ *     first call before any stream capture;
+ *   - all calls, from every context on the device, share the one array and
+ *     its leftover contents: calls that overlap on the GPU (other threads or
+ *     streams) race and corrupt each other.
  * Nothing is allocated by this call; the context (wb_ctx_create) must exist.
  */
 #define WB_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)

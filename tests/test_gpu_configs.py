@@ -1,0 +1,153 @@
+"""Oracle parity on the benchmark configurations and on every FFT box edge the
+library provides, through the C ABI.
+
+What each test pins:
+* ``test_c2_bench_settings``: the 64^3 system the benchmark times (L = 20 bohr,
+  25 Ry, 8 s+p atoms, 32 bands) at the benchmark's tr2 = 1e-10 on 8
+  perturbations, FP64 and mixed, with dfpt's ierr; and the same with
+  n_dfpt_maxiter = 20, where most bands stop unconverged (ierr > 0).
+* ``test_box_edge``: one small synthetic system per box edge (16 ... 108:
+  radices 2, 3, 4, 5, 6, 8, 9, 10, 12), fixed PCG steps in FP64 and a
+  converged solve in FP64 and mixed; the odd band count runs the single-band
+  transforms.  The sphere reaches n/4 - 1 (pruned transforms, the QE relation
+  of the wavefunction sphere to the density box); ``test_box_edge_full_sphere``
+  fills the box up to n/2 - 2 (unpruned transforms).
+* ``test_c4c_80cube``: the 80^3 system of the uneven batch (L = 25 bohr, 25 Ry,
+  12 atoms, 64 bands), one perturbation at tr2 = 1e-10, FP64 and mixed.
+* ``test_c5_108cube_fixed_steps``: the 108^3 large cell (L = 30 bohr, 30 Ry,
+  20 atoms, 128 bands), one perturbation, 5 fixed PCG steps (FP64).
+
+Bars as in the other parity tests: relative 2-norm over the batch below 1e-10
+in FP64 and 1e-7 in the mixed form, identical ierr.  Fixed-step cases stop
+where the PCG iterate is well conditioned (5 steps), converged cases use a
+threshold no system sits on.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import west_oracle as O
+from west_b200.system import SystemSpec, build_system, perturbations
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-10
+TOL_MIXED = 1e-7
+EDGES = (16, 20, 24, 32, 36, 40, 48, 60, 64, 72, 80, 96, 100, 108)
+_CACHE = {}
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _cached(key, fn):
+    if key not in _CACHE:
+        _CACHE[key] = fn()
+    return _CACHE[key]
+
+
+def _gpu(s, dvg, tr2, precision="fp64", **kw):
+    from west_b200.wstat import ResponseOperator
+    op = ResponseOperator(s, verbose=False, **kw)
+    op.set_precision(precision)
+    dng = np.zeros_like(dvg, order="F")
+    ierr = op.apply_operator(dvg.shape[1], dvg, dng, tr2, 1)
+    st = op.stats()
+    op.close()
+    return dng, ierr, st
+
+
+def edge_spec(n, gmax):
+    """Cubic cell whose Gamma sphere reaches Miller index gmax in an n^3 box."""
+    L = 8.0 + n / 6.0
+    ecut = (gmax * 2.0 * math.pi / L) ** 2 * (1.0 + 1e-9)
+    return SystemSpec(L=L, ecutwfc=ecut, nr=n, natoms=2, nbnd_occ=3, proj="sp", seed=100 + n)
+
+
+def _edge_case(n, gmax):
+    def make():
+        s = build_system(edge_spec(n, gmax), "cuda")
+        assert max(abs(s.mill).max(axis=0)) == gmax
+        dvg = perturbations(s, 2, seed=n)
+        fixed, ferr = O.apply_operator(s, dvg, 0.0, maxiter=5)
+        conv, cerr = O.apply_operator(s, dvg, 1e-14, maxiter=400)
+        assert (cerr == 0).all()
+        return s, dvg, fixed, ferr, conv
+    return _cached(("edge", n, gmax), make)
+
+
+def _check_edge(n, gmax):
+    s, dvg, fixed, ferr, conv = _edge_case(n, gmax)
+    got, ierr, _ = _gpu(s, dvg, 0.0, n_dfpt_maxiter=5)
+    assert (ierr == ferr).all() and (ierr == s.nbnd_occ).all()
+    assert _rel(got, fixed) < TOL_FP64, ("fixed", _rel(got, fixed))
+    got, ierr, _ = _gpu(s, dvg, 1e-14, n_dfpt_maxiter=400)
+    assert (ierr == 0).all()
+    assert _rel(got, conv) < TOL_FP64, ("fp64", _rel(got, conv))
+    got, ierr, st = _gpu(s, dvg, 1e-14, "mixed", n_dfpt_maxiter=400)
+    assert (ierr == 0).all() and st["refinements"] >= 1
+    assert _rel(got, conv) < TOL_MIXED, ("mixed", _rel(got, conv))
+
+
+@pytest.mark.parametrize("n", EDGES)
+def test_box_edge(n):
+    _check_edge(n, n // 4 - 1)
+
+
+@pytest.mark.parametrize("n", (20, 24, 32, 36))
+def test_box_edge_full_sphere(n):
+    _check_edge(n, n // 2 - 2)
+
+
+def _c2_case():
+    def make():
+        s = build_system("c2", "cuda")
+        dvg = perturbations(s, 8)
+        ref, rerr = O.apply_operator(s, dvg, 1e-10)
+        return s, dvg, ref, rerr
+    return _cached("c2", make)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_c2_bench_settings(precision):
+    s, dvg, ref, rerr = _c2_case()
+    assert s.npw == 8440 and s.nr == 64 and s.nbnd_occ == 32
+    got, ierr, _ = _gpu(s, dvg, 1e-10, precision)
+    assert (rerr == 0).all() and (ierr == rerr).all()
+    tol = TOL_FP64 if precision == "fp64" else TOL_MIXED
+    assert _rel(got, ref) < tol, _rel(got, ref)
+
+
+def test_c2_unconverged_ierr():
+    """n_dfpt_maxiter = 20 at tr2 = 1e-10: dfpt's ierr counts the bands left
+    unconverged per perturbation (dfpt_module.f90:356-359)."""
+    s, dvg, _, _ = _c2_case()
+    ref, rerr = _cached("c2_20", lambda: O.apply_operator(s, dvg, 1e-10, maxiter=20))
+    got, ierr, _ = _gpu(s, dvg, 1e-10, n_dfpt_maxiter=20)
+    assert (rerr > 0).any()
+    assert (ierr == rerr).all(), (ierr, rerr)
+    assert _rel(got, ref) < TOL_FP64, _rel(got, ref)
+
+
+def test_c4c_80cube():
+    s = build_system("c4c", "cuda")
+    assert s.nr == 80 and s.nbnd_occ == 64
+    dvg = perturbations(s, 1)
+    ref, rerr = O.apply_operator(s, dvg, 1e-10)
+    assert (rerr == 0).all()
+    for precision, tol in (("fp64", TOL_FP64), ("mixed", TOL_MIXED)):
+        got, ierr, _ = _gpu(s, dvg, 1e-10, precision)
+        assert (ierr == 0).all(), precision
+        assert _rel(got, ref) < tol, (precision, _rel(got, ref))
+
+
+def test_c5_108cube_fixed_steps():
+    s = build_system("c5", "cuda")
+    assert s.nr == 108 and s.nbnd_occ == 128 and s.npw == 37387
+    dvg = perturbations(s, 1)
+    ref, rerr = O.apply_operator(s, dvg, 0.0, maxiter=5)
+    got, ierr, _ = _gpu(s, dvg, 0.0, n_dfpt_maxiter=5)
+    assert (ierr == rerr).all() and (ierr == s.nbnd_occ).all()
+    assert _rel(got, ref) < TOL_FP64, _rel(got, ref)

@@ -58,10 +58,28 @@ def test_davidson_rejects_small_basis(small):
         op.davidson(randomized_basis(small, 4), 4, n_pdep_times=1)
 
 
-def test_davidson_c1_configuration():
+_C1 = {}
+
+
+def _c1_oracle():
+    if not _C1:
+        s = build_system("c1", "cuda")
+        dvg0 = randomized_basis(s, 16)
+        rev, rconv, _, rit = O.davidson_diago_gamma(s, dvg0, 16, 64, tr2_dfpt=1e-10, trev_pdep=1e-6,
+                                                     trev_pdep_rel=1e-1)
+        _C1.update(s=s, dvg0=dvg0, rev=rev, rconv=rconv, rit=rit)
+    return _C1
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_davidson_c1_configuration(precision):
     """L = 15 bohr, 20 Ry, 48^3, 4 atoms, 8 bands; n_pdep_eigen 16, n_pdep_times 4,
-    PCG 1e-10, Davidson tolerance 1e-6."""
-    s = build_system("c1")
-    ev, conv, vec, info, rev, rconv, rvec, rit = _run(s, 16, 4, tr2=1e-10, trev=1e-6)
-    assert info["converged"] == 1 and rconv.all()
-    assert np.abs((ev - rev) / rev).max() < TOL_EV
+    PCG 1e-10, Davidson tolerance 1e-6; both forms against the FP64 oracle."""
+    from west_b200.wstat import ResponseOperator
+    c = _c1_oracle()
+    op = ResponseOperator(c["s"], verbose=False)
+    op.set_precision(precision)
+    ev, conv, vec, info = op.davidson(c["dvg0"], 16, n_pdep_times=4, tr2_dfpt=1e-10, trev_pdep=1e-6,
+                                      trev_pdep_rel=1e-1)
+    assert info["converged"] == 1 and c["rconv"].all()
+    assert np.abs((ev - c["rev"]) / c["rev"]).max() < TOL_EV

@@ -12,7 +12,6 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
-#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1249,24 +1248,24 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[WB_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-struct NoallocDevice {
-  std::once_flag once;
-  void* ptr = nullptr;
-  cudaError_t err = cudaSuccess;
-};
-NoallocDevice g_noalloc_dev[kMaxDevices];
-
-// Device address of the scratch array on the current device, looked up once
-// per device.  The host-side name g_noalloc_scratch is only a stand-in for
-// the symbol: it must never be passed to a kernel.
-int noalloc_scratch(int dev, unsigned char** out) {
-  if (dev < 0 || dev >= kMaxDevices) return fail(WB_ERR_UNSUPPORTED, "device index too large for the scratch table");
-  NoallocDevice& d = g_noalloc_dev[dev];
-  std::call_once(d.once, [&d] { d.err = cudaGetSymbolAddress(&d.ptr, g_noalloc_scratch); });
-  if (d.err != cudaSuccess || d.ptr == nullptr)
-    return fail(WB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(d.err));
-  *out = static_cast<unsigned char*>(d.ptr);
+// Device address of the scratch array for the context's device, looked up on
+// the context's first allocation-free call, with that device current, and kept
+// in the context: the address belongs to the CUDA context the library's module
+// is loaded in, so a context created later (after a cudaDeviceReset, say) makes
+// its own lookup.  A failed lookup is not kept; the next call tries again.  The
+// host-side name g_noalloc_scratch is only a stand-in for the symbol: it must
+// never be passed to a kernel.
+int noalloc_scratch(wb_ctx* c, unsigned char** out) {
+  if (!c->noalloc_base) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      cudaGetLastError();
+      return fail(WB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    }
+    c->noalloc_base = p;
+  }
+  *out = static_cast<unsigned char*>(c->noalloc_base);
   return WB_OK;
 }
 
@@ -1297,7 +1296,7 @@ void noalloc_layout(const wb_ctx* c, int mb, Carve& cv, NoallocWs& w) {
   const size_t nsys = (size_t)mb * c->nocc;
   const size_t npw = c->npw;
   const size_t stk1 = (size_t)c->nr * c->st.nst;
-  const size_t mp = (mb + 1) / 2;
+  const size_t mp = ((size_t)mb + 1) / 2;
   const size_t nitems = std::max<size_t>({(nsys + 1) / 2, (size_t)mb * c->npv, mp});
   w.nsplit = gemm_tn_splits(c->nproj, (int)nsys, 2 * c->npw);
   w.aux = cv.take<double2>(npw * mb);
@@ -1428,7 +1427,14 @@ extern "C" int wb_apply_operator_device_noalloc(wb_ctx* c, int m, const double* 
   if (m > 0 && (!dvg || !dng)) return fail(WB_ERR_ARG, "null dvg or dng");
   if (ld_dvg < c->npw || ld_dng < c->npw) return fail(WB_ERR_ARG, "leading dimension smaller than npw");
   if (std::isnan(tr2)) return fail(WB_ERR_ARG, "tr2 is NaN");
-  if (c->precision != WB_PRECISION_FP64) return fail(WB_ERR_UNSUPPORTED, "mixed precision is not built yet");
+  if (c->precision != WB_PRECISION_FP64)
+    return fail(WB_ERR_UNSUPPORTED, "the allocation-free entry point runs the FP64 form only");
+  // the four PCG vectors alone must fit: this bounds m before any int product
+  // of the layout (m * nbnd_occ systems, m * band pairs) is formed
+  if (4.0 * sizeof(double2) * (double)m * c->nocc * c->npw > (double)WB_NOALLOC_SCRATCH_BYTES)
+    return fail(WB_ERR_ARG, "m = " + std::to_string(m) + " perturbations do not fit the allocation-free entry "
+                "point's scratch of " + std::to_string((size_t)WB_NOALLOC_SCRATCH_BYTES) +
+                " bytes (WB_NOALLOC_SCRATCH_BYTES): use fewer perturbations per call");
   Carve probe{nullptr};
   NoallocWs w{};
   noalloc_layout(c, std::max(m, 1), probe, w);
@@ -1438,7 +1444,7 @@ extern "C" int wb_apply_operator_device_noalloc(wb_ctx* c, int m, const double* 
                 " (WB_NOALLOC_SCRATCH_BYTES): use fewer perturbations per call");
   WB_CU(cudaSetDevice(c->device));
   unsigned char* base = nullptr;
-  int rc = noalloc_scratch(c->device, &base);
+  int rc = noalloc_scratch(c, &base);
   if (rc) return rc;
   c->stats = wb_stats{};
   c->stats.m = m;

@@ -123,6 +123,9 @@ struct wb_ctx {
   DBuf dav_dvg, dav_dng, dav_tmp, dav_hr, dav_vr, dav_A, dav_V, dav_w, dav_part, dav_coef, dav_dots;
   wb_apply_fn dav_apply = nullptr;  // operator hook of the Davidson (wb_davidson_set_apply)
   void* dav_apply_user = nullptr;
+  // device address of the allocation-free entry point's scratch array, looked
+  // up on this context's first such call (null until then)
+  void* noalloc_base = nullptr;
   int ev_get() {
     if (evused == evpool.size()) {
       cudaEvent_t e;
