@@ -235,8 +235,9 @@ typedef struct wb_davidson_info {
  * the randomised starting basis (do_randomize, davidson_diago.f90:1121, host
  * memory).  Returns the n_pdep_eigen lowest eigenvalues of sqvc chi0 sqvc in
  * ev, their convergence flags in conv and, when pdep != NULL, the eigenvectors
- * [ld_pdep, n_pdep_eigen] (host memory).  The subspace eigensolver is a
- * Jacobi method on the GPU (diagox uses LAPACK DSYEV / cuSOLVER in WEST).
+ * [ld_pdep, n_pdep_eigen] (host memory).  The subspace eigensolver is
+ * wb_diagox's Jacobi method on the GPU (diagox uses LAPACK DSYEV / cuSOLVER in
+ * WEST); n_pdep_basis up to 4096.
  */
 /*
  * Operator hook of the Davidson: when set, wb_davidson calls fn instead of its
@@ -263,6 +264,18 @@ int wb_davidson_set_apply(wb_ctx* ctx, wb_apply_fn fn, void* user);
  */
 int wb_davidson(wb_ctx* ctx, const wb_davidson_params* params, const double* dvg0, int ld_dvg0, double* ev,
                 int* conv, double* pdep, int ld_pdep, wb_davidson_info* info);
+
+/*
+ * Subspace eigensolver of the Davidson, diagox_dsy (Wstat/wstat_tools.f90:48,
+ * serial_diagox_dsy :208, matdiago_dsy Tools/linear_algebra_kernel.f90:84):
+ * the nvec lowest eigenvalues of the real symmetric hr(1:nbase, 1:nbase)
+ * (upper triangle read, as DSYEV 'U') in ascending order into ew (host), and
+ * their orthonormal eigenvectors into vr(:, 1:nvec).  hr [ldh, nbase] and vr
+ * [ldv, nvec] are column-major device arrays of the context's device.  Cyclic
+ * Jacobi in one CTA up to nbase = 112, a parallel two-sided block Jacobi over
+ * many CTAs above (up to 4096); WEST uses LAPACK DSYEV / cuSOLVER here.
+ */
+int wb_diagox(wb_ctx* ctx, int nbase, int nvec, const double* hr, int ldh, double* ew, double* vr, int ldv);
 
 /*
  * PDEP database in WEST's format: pdep_db_write (IO_kernel/pdep_db.f90:56) with

@@ -96,7 +96,7 @@ def test_box_edge(n):
     _check_edge(n, n // 4 - 1)
 
 
-@pytest.mark.parametrize("n", (20, 24, 32, 36))
+@pytest.mark.parametrize("n", (16, 20, 24, 32, 36, 48, 64))
 def test_box_edge_full_sphere(n):
     _check_edge(n, n // 2 - 2)
 

@@ -50,6 +50,15 @@ def test_davidson_maxiter_exit(small):
     assert np.abs((ev - rev) / rev).max() < TOL_EV
 
 
+def test_davidson_block_jacobi_basis(small):
+    """n_pdep_basis = 128 > 112: the subspace eigensolver is the block Jacobi
+    over many CTAs (wb_diagox above the one-CTA size)."""
+    ev, conv, vec, info, rev, rconv, rvec, rit = _run(small, 32, 4)
+    assert info["converged"] == 1 and rconv.all()
+    assert info["dav_iter"] == rit
+    assert np.abs((ev - rev) / rev).max() < TOL_EV
+
+
 def test_davidson_rejects_small_basis(small):
     from west_b200.lib import WestB200Error
     from west_b200.wstat import ResponseOperator

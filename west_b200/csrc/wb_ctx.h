@@ -120,7 +120,7 @@ struct wb_ctx {
   int umma = 0, umma_M = 0;
   DBuf umma_braket_w, umma_update_w, umma_err;
   // PDEP Davidson state (wb_davidson)
-  DBuf dav_dvg, dav_dng, dav_tmp, dav_hr, dav_vr, dav_A, dav_V, dav_w, dav_part, dav_coef, dav_dots;
+  DBuf dav_dvg, dav_dng, dav_tmp, dav_hr, dav_vr, dav_A, dav_V, dav_w, dav_part, dav_coef, dav_dots, dav_bj;
   wb_apply_fn dav_apply = nullptr;  // operator hook of the Davidson (wb_davidson_set_apply)
   void* dav_apply_user = nullptr;
   // device address of the allocation-free entry point's scratch array, looked

@@ -8,7 +8,8 @@
 // Device work: Gamma bra-kets for hr (build_hr_real) on the DMMA split-K
 // GEMM, basis combinations (update_with_vr / refresh_with_vr) on the DMMA
 // accumulation GEMM, modified Gram-Schmidt (do_mgs) as per-vector reductions
-// and rank-1 updates, and a cyclic Jacobi eigensolver (diagox) in one CTA.
+// and rank-1 updates, and Jacobi eigensolvers (diagox): cyclic in one CTA for
+// bases up to 112, parallel two-sided block Jacobi over many CTAs above.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -233,6 +234,368 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ hr, 
   for (int k = tid; k < nsel; k += nt) w[k] = A[idx[k] * n + idx[k]];
 }
 
+// ---------------------------------------------------------------------------
+// Parallel two-sided block Jacobi for bases above kJacobiSmemN (up to 1024)
+// ---------------------------------------------------------------------------
+// The matrix (padded to npad = nb * kBJ with zero rows and columns, nb even) is
+// cut into nb blocks of kBJ indices.  A sweep runs nb - 1 rounds of the same
+// round-robin ordering as k_jacobi over blocks: in a round the nb / 2 disjoint
+// block pairs P = I u J each diagonalise their 2 kBJ x 2 kBJ submatrix
+// A[P, P] = U diag U^T in shared memory (one CTA per pair, the cyclic Jacobi
+// above, to convergence), then A <- Q^T A Q and V <- V Q with Q =
+// blockdiag(U_P), as independent tiles (pair x pair for A, rows x pair for V).
+// Sweeps stop when the off-diagonal Frobenius norm is below 1e-14 of the whole:
+// the rotations are applied as 32-term dot products, which leave rounding
+// residues of about sqrt(n) eps ||A|| off the diagonal, so k_jacobi's 1e-15 is
+// out of reach for large n; the eigenvalue error is second order in the
+// off-diagonal norm, and the selected eigenvalues are recomputed at the end as
+// Rayleigh quotients v^T hr v of the input matrix (first-order error in v only
+// enters squared).  A pair whose off-diagonal block holds less than its share
+// (1 / number of block pairs) of 1e-30 ||A||^2 keeps U = 1 and its tiles are
+// left alone.  Padded indices carry no coupling, so they never rotate; they are
+// excluded from the selection.
+constexpr int kBJ = 16;
+constexpr int kMaxBasis = 4096;
+constexpr int kBJ2 = 2 * kBJ;
+constexpr int kBJThreads = 256;
+
+__device__ __forceinline__ void bj_pair(int k, int r, int nb, int& I, int& J) {
+  const int a0 = (k == 0) ? 0 : 1 + ((k - 1 + r) % (nb - 1));
+  const int kk = nb - 1 - k;
+  const int b0 = 1 + ((kk - 1 + r) % (nb - 1));
+  I = min(a0, b0);
+  J = max(a0, b0);
+}
+__device__ __forceinline__ int bj_glob(int l, int I, int J) { return l < kBJ ? I * kBJ + l : J * kBJ + (l - kBJ); }
+
+__global__ void k_bj_init(const double* __restrict__ hr, long ldh, int n, int npad, double* __restrict__ A,
+                          double* __restrict__ V) {
+  const long nn = (long)npad * npad;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < nn; e += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / npad), j = (int)(e % npad);
+    double a = 0.0;
+    if (i < n && j < n) a = (i <= j) ? hr[(long)j * ldh + i] : hr[(long)i * ldh + j];
+    A[e] = a;
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+}
+
+// red[0] = sum of squared off-diagonal entries, red[1] = of all entries
+__global__ void k_bj_norms(const double* __restrict__ A, int npad, double* __restrict__ red) {
+  __shared__ double sh[2][32];
+  double off = 0.0, tot = 0.0;
+  const long nn = (long)npad * npad;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < nn; e += (long)gridDim.x * blockDim.x) {
+    const double v = A[e];
+    tot = fma(v, v, tot);
+    if (e / npad != e % npad) off = fma(v, v, off);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    off += __shfl_xor_sync(0xffffffffu, off, o);
+    tot += __shfl_xor_sync(0xffffffffu, tot, o);
+  }
+  if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = off; sh[1][threadIdx.x >> 5] = tot; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double so = 0.0, st = 0.0;
+    for (int i = 0; i < (int)blockDim.x / 32; ++i) { so += sh[0][i]; st += sh[1][i]; }
+    atomicAdd(red, so);
+    atomicAdd(red + 1, st);
+  }
+}
+
+// One CTA per block pair of round r: U_P (row-major, U[l][m]) of the pair's
+// 2 kBJ x 2 kBJ submatrix, or the identity with skip[k] = 1.
+__global__ void __launch_bounds__(kBJThreads) k_bj_solve(const double* __restrict__ A, int npad, int nb, int r,
+                                                         const double* __restrict__ red, double* __restrict__ U,
+                                                         int* __restrict__ skip, double skip_frac) {
+  constexpr int n = kBJ2, npairs = kBJ2 / 2;
+  __shared__ double S[n * n], Q[n * n];
+  __shared__ double cs[npairs], sn[npairs];
+  __shared__ int pp[npairs], qq[npairs];
+  __shared__ double sh[2][kBJThreads / 32];
+  __shared__ int done;
+  const int tid = threadIdx.x, k = blockIdx.x;
+  int I, J;
+  bj_pair(k, r, nb, I, J);
+  double offij = 0.0;
+  for (int e = tid; e < n * n; e += kBJThreads) {
+    const int i = e / n, j = e % n;
+    const double v = A[(long)bj_glob(i, I, J) * npad + bj_glob(j, I, J)];
+    S[e] = v;
+    Q[e] = (i == j) ? 1.0 : 0.0;
+    if (i < kBJ && j >= kBJ) offij = fma(v, v, offij);
+  }
+  for (int o = 16; o > 0; o >>= 1) offij += __shfl_xor_sync(0xffffffffu, offij, o);
+  if ((tid & 31) == 0) sh[0][tid >> 5] = offij;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int i = 0; i < kBJThreads / 32; ++i) s += sh[0][i];
+    done = (s <= skip_frac * red[1]) ? 1 : 0;
+  }
+  __syncthreads();
+  double* Uk = U + (long)k * n * n;
+  if (done) {
+    for (int e = tid; e < n * n; e += kBJThreads) Uk[e] = Q[e];
+    if (tid == 0) skip[k] = 1;
+    return;
+  }
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int e = tid; e < n * n; e += kBJThreads) {
+      const double v = S[e];
+      if (e / n == e % n) dia = fma(v, v, dia); else off = fma(v, v, off);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      dia += __shfl_xor_sync(0xffffffffu, dia, o);
+    }
+    __syncthreads();
+    if ((tid & 31) == 0) { sh[0][tid >> 5] = off; sh[1][tid >> 5] = dia; }
+    __syncthreads();
+    if (tid == 0) {
+      double to = 0.0, td = 0.0;
+      for (int i = 0; i < kBJThreads / 32; ++i) { to += sh[0][i]; td += sh[1][i]; }
+      done = (to <= 1e-32 * (td + to)) ? 1 : 0;
+    }
+    __syncthreads();
+    if (done) break;
+    for (int rr = 0; rr < n - 1; ++rr) {
+      if (tid < npairs) {
+        const int kq = tid;
+        const int a0 = (kq == 0) ? 0 : 1 + ((kq - 1 + rr) % (n - 1));
+        const int kk = n - 1 - kq;
+        const int b0 = 1 + ((kk - 1 + rr) % (n - 1));
+        const int p = min(a0, b0), q = max(a0, b0);
+        double c = 1.0, s = 0.0;
+        const double apq = S[p * n + q];
+        if (fabs(apq) > 1e-300) {
+          const double tau = (S[q * n + q] - S[p * n + p]) / (2.0 * apq);
+          const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          c = 1.0 / sqrt(1.0 + t * t);
+          s = t * c;
+        }
+        cs[kq] = c; sn[kq] = s; pp[kq] = p; qq[kq] = q;
+      }
+      __syncthreads();
+      for (int e = tid; e < npairs * npairs; e += kBJThreads) {   // S <- J^T S J, 2x2 block per thread
+        const int k1 = e / npairs, k2 = e % npairs;
+        const int p1 = pp[k1], q1 = qq[k1], p2 = pp[k2], q2 = qq[k2];
+        const double ca = cs[k1], sa = sn[k1], cb = cs[k2], sb = sn[k2];
+        const double a = S[p1 * n + p2], b = S[p1 * n + q2], cc = S[q1 * n + p2], d = S[q1 * n + q2];
+        const double ra = ca * a - sa * cc, rc = sa * a + ca * cc;
+        const double rb = ca * b - sa * d, rd = sa * b + ca * d;
+        S[p1 * n + p2] = cb * ra - sb * rb;
+        S[q1 * n + q2] = sb * rc + cb * rd;
+        if (k1 == k2 && sa != 0.0) {              // the plane's own pivot: zero by construction
+          S[p1 * n + q2] = 0.0;
+          S[q1 * n + p2] = 0.0;
+        } else {
+          S[p1 * n + q2] = sb * ra + cb * rb;
+          S[q1 * n + p2] = cb * rc - sb * rd;
+        }
+      }
+      for (int e = tid; e < npairs * n; e += kBJThreads) {         // Q <- Q J
+        const int kq = e / n, i = e % n;
+        const int p = pp[kq], q = qq[kq];
+        const double c = cs[kq], s = sn[kq];
+        const double vp = Q[i * n + p], vq = Q[i * n + q];
+        Q[i * n + p] = c * vp - s * vq;
+        Q[i * n + q] = s * vp + c * vq;
+      }
+      __syncthreads();
+    }
+  }
+  for (int e = tid; e < n * n; e += kBJThreads) Uk[e] = Q[e];
+  if (tid == 0) skip[k] = 0;
+}
+
+// A[P1, P2] <- U_P1^T A[P1, P2] U_P2 for the pair tile (blockIdx.x, blockIdx.y)
+__global__ void __launch_bounds__(kBJThreads) k_bj_apply_a(double* __restrict__ A, int npad, int nb, int r,
+                                                           const double* __restrict__ U,
+                                                           const int* __restrict__ skip) {
+  constexpr int n = kBJ2;
+  const int k1 = blockIdx.x, k2 = blockIdx.y;
+  if (skip[k1] && skip[k2]) return;
+  __shared__ double U1[n * n], U2[n * n], T[n * n];
+  int I1, J1, I2, J2;
+  bj_pair(k1, r, nb, I1, J1);
+  bj_pair(k2, r, nb, I2, J2);
+  const int tid = threadIdx.x;
+  for (int e = tid; e < n * n; e += kBJThreads) {
+    U1[e] = U[(long)k1 * n * n + e];
+    U2[e] = U[(long)k2 * n * n + e];
+    T[e] = A[(long)bj_glob(e / n, I1, J1) * npad + bj_glob(e % n, I2, J2)];
+  }
+  __syncthreads();
+  constexpr int PER = n * n / kBJThreads;
+  double o[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {                 // (U1^T T)[i][j]
+    const int e = tid + q * kBJThreads, i = e / n, j = e % n;
+    double s = 0.0;
+#pragma unroll 8
+    for (int l = 0; l < n; ++l) s = fma(U1[l * n + i], T[l * n + j], s);
+    o[q] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) T[tid + q * kBJThreads] = o[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {                 // (U1^T T U2)[i][j]
+    const int e = tid + q * kBJThreads, i = e / n, j = e % n;
+    double s = 0.0;
+#pragma unroll 8
+    for (int l = 0; l < n; ++l) s = fma(T[i * n + l], U2[l * n + j], s);
+    A[(long)bj_glob(i, I1, J1) * npad + bj_glob(j, I2, J2)] = s;
+  }
+}
+
+// V[rows, P] <- V[rows, P] U_P for rows [32 blockIdx.x, + 32) and pair blockIdx.y
+__global__ void __launch_bounds__(kBJThreads) k_bj_apply_v(double* __restrict__ V, int npad, int nb, int r,
+                                                           const double* __restrict__ U,
+                                                           const int* __restrict__ skip) {
+  constexpr int n = kBJ2;
+  const int k = blockIdx.y, r0 = blockIdx.x * n;
+  if (skip[k]) return;
+  __shared__ double Uk[n * n], T[n * n];
+  int I, J;
+  bj_pair(k, r, nb, I, J);
+  const int tid = threadIdx.x;
+  for (int e = tid; e < n * n; e += kBJThreads) {
+    Uk[e] = U[(long)k * n * n + e];
+    T[e] = V[(long)(r0 + e / n) * npad + bj_glob(e % n, I, J)];
+  }
+  __syncthreads();
+  constexpr int PER = n * n / kBJThreads;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = tid + q * kBJThreads, i = e / n, j = e % n;
+    double s = 0.0;
+#pragma unroll 8
+    for (int l = 0; l < n; ++l) s = fma(T[i * n + l], Uk[l * n + j], s);
+    V[(long)(r0 + i) * npad + bj_glob(j, I, J)] = s;
+  }
+}
+
+// The nsel lowest of the n real eigenvalues (diag A, padding excluded) in
+// ascending order into w, their eigenvectors (columns of V) into vr(:, 0:nsel).
+__global__ void __launch_bounds__(1024) k_bj_select(const double* __restrict__ A, const double* __restrict__ V,
+                                                    int n, int npad, int nsel, double* __restrict__ w,
+                                                    double* __restrict__ vr, long ldv, int* __restrict__ idx) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double li = A[(long)i * npad + i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double lj = A[(long)j * npad + j];
+      rank += (lj < li || (lj == li && j < i)) ? 1 : 0;
+    }
+    if (rank < nsel) { w[rank] = li; idx[rank] = i; }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nsel * n; e += blockDim.x) {
+    const int k = e / n, rr = e % n;
+    vr[(long)k * ldv + rr] = V[(long)rr * npad + idx[k]];
+  }
+}
+
+// For each selected eigenvector v_k (vr column k): w[k] <- v^T hr v / v^T v and
+// v <- v / |v|.  The many block rotations let the column norms of V drift by
+// about 1e-12, which would scale every eigenvalue by as much.  hr is read from
+// its upper triangle; one CTA per eigenvector.
+__global__ void __launch_bounds__(256) k_bj_rayleigh(const double* __restrict__ hr, long ldh, int n,
+                                                     double* __restrict__ vr, long ldv, double* __restrict__ w) {
+  __shared__ double sv[4096];
+  __shared__ double red[16];
+  const int k = blockIdx.x;
+  double* v = vr + (long)k * ldv;
+  for (int i = threadIdx.x; i < n; i += 256) sv[i] = v[i];
+  __syncthreads();
+  double vhv = 0.0, vv = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) {    // row i of hr: (i, j) = hr[j ldh + i] for j >= i, hr[i ldh + j] below
+    double hv = 0.0;
+    const double* col = hr + (long)i * ldh;
+    for (int j = 0; j < i; ++j) hv = fma(col[j], sv[j], hv);
+    for (int j = i; j < n; ++j) hv = fma(hr[(long)j * ldh + i], sv[j], hv);
+    vhv = fma(sv[i], hv, vhv);
+    vv = fma(sv[i], sv[i], vv);
+  }
+  const double2 r = block_sum2<256>(vhv, vv, red);
+  if (threadIdx.x == 0) w[k] = r.x / r.y;
+  const double sc = 1.0 / sqrt(r.y);
+  for (int i = threadIdx.x; i < n; i += 256) v[i] = sv[i] * sc;
+}
+
+// Scratch of the block Jacobi for bases up to nmax, in doubles.
+size_t bj_doubles(int nmax) {
+  int nb = (nmax + kBJ - 1) / kBJ;
+  nb += nb & 1;
+  const size_t npad = (size_t)nb * kBJ;
+  return 2 * npad * npad + (size_t)(nb / 2) * kBJ2 * kBJ2 + 2 + nmax + nb;
+}
+
+// Lowest nsel eigenpairs of the symmetric hr[:n, :n] (upper triangle, column
+// major, ld ldh): w (device, ascending) and vr(:, 0:nsel) (device, ld ldv).
+// scratch holds bj_doubles(n); red2 is pinned host memory for two doubles.
+int block_jacobi(const double* hr, long ldh, int n, int nsel, double* w, double* vr, long ldv, double* scratch,
+                 double* red_host, int* sweeps_out, cudaStream_t s) {
+  int nb = (n + kBJ - 1) / kBJ;
+  nb += nb & 1;
+  const int npad = nb * kBJ, npair = nb / 2;
+  double* A = scratch;
+  double* V = A + (size_t)npad * npad;
+  double* U = V + (size_t)npad * npad;
+  double* red = U + (size_t)npair * kBJ2 * kBJ2;
+  int* iw = reinterpret_cast<int*>(red + 2);  // skip flags, then the selection indices
+  int* skip = iw;
+  int* idx = iw + nb;
+  const int g = std::min(1184, (int)(((long)npad * npad + 255) / 256));
+  const double skip_frac = 1e-30 / (0.5 * nb * (nb - 1));
+  k_bj_init<<<g, 256, 0, s>>>(hr, ldh, n, npad, A, V);
+  int sweep = 0;
+  for (;; ++sweep) {
+    WB_CU(cudaMemsetAsync(red, 0, 2 * sizeof(double), s));
+    k_bj_norms<<<g, 256, 0, s>>>(A, npad, red);
+    WB_CU(cudaMemcpyAsync(red_host, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaStreamSynchronize(s));
+    if (red_host[0] <= 1e-28 * red_host[1] || sweep == 40) break;
+    for (int r = 0; r < nb - 1; ++r) {
+      k_bj_solve<<<npair, kBJThreads, 0, s>>>(A, npad, nb, r, red, U, skip, skip_frac);
+      k_bj_apply_a<<<dim3(npair, npair), kBJThreads, 0, s>>>(A, npad, nb, r, U, skip);
+      k_bj_apply_v<<<dim3(npad / kBJ2, npair), kBJThreads, 0, s>>>(V, npad, nb, r, U, skip);
+    }
+    WB_CU(cudaGetLastError());
+  }
+  k_bj_select<<<1, 1024, 0, s>>>(A, V, n, npad, nsel, w, vr, ldv, idx);
+  k_bj_rayleigh<<<nsel, 256, 0, s>>>(hr, ldh, n, vr, ldv, w);
+  WB_CU(cudaGetLastError());
+  *sweeps_out = sweep;
+  return WB_OK;
+}
+
+// diagox_dsy (Wstat/wstat_tools.f90:48): the one-CTA shared-memory Jacobi up
+// to kJacobiSmemN, the block Jacobi above.  A and V: n^2 doubles each of
+// global scratch (unused by the shared-memory path); bj: bj_doubles(n).
+int eigen_lowest(const double* hr, long ldh, int n, int nsel, double* w, double* vr, long ldv, double* A, double* V,
+                 double* bj, int* sweeps, cudaStream_t s) {
+  if (n > kJacobiSmemN) {
+    int sw = 0;
+    double red[2];
+    return block_jacobi(hr, ldh, n, nsel, w, vr, ldv, bj, red, &sw, s);
+  }
+  const size_t shm = jacobi_pairs_bytes(n) + 2 * sizeof(double) * n * n;
+  k_jacobi<<<1, 1024, shm, s>>>(hr, ldh, n, A, V, nsel, w, vr, ldv, sweeps, 1);
+  WB_CU(cudaGetLastError());
+  return WB_OK;
+}
+
+void jacobi_setup() {
+  cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(jacobi_pairs_bytes(kJacobiSmemN) + 2 * sizeof(double) * kJacobiSmemN * kJacobiSmemN));
+}
+
 struct Dav {
   wb_ctx* c;
   int npw, nvec, nvecx;
@@ -301,11 +664,10 @@ struct Dav {
     WB_CU(cudaGetLastError());
     return WB_OK;
   }
+  double* bj = nullptr;  // block Jacobi scratch (bases above kJacobiSmemN)
   int diagox(int nbase, std::vector<double>& ew_host) {  // lowest nvec eigenpairs of hr[:nbase, :nbase]
-    const int in_smem = nbase <= kJacobiSmemN ? 1 : 0;
-    const size_t shm = jacobi_pairs_bytes(nbase) + (in_smem ? 2 * sizeof(double) * nbase * nbase : 0);
-    k_jacobi<<<1, 1024, shm, s>>>(hr, nvecx, nbase, A, V, nvec, w, vr, nvecx, sweeps, in_smem);
-    WB_CU(cudaGetLastError());
+    int rc = eigen_lowest(hr, nvecx, nbase, nvec, w, vr, nvecx, A, V, bj, sweeps, s);
+    if (rc) return rc;
     WB_CU(cudaMemcpyAsync(ew_host.data(), w, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
     WB_CU(cudaStreamSynchronize(s));
     return WB_OK;
@@ -340,15 +702,15 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
   const int nvec = p->n_pdep_eigen, nvecx = p->n_pdep_basis;
   if (nvec < 1 || nvecx < 2 * nvec)
     return fail(WB_ERR_ARG, "need n_pdep_eigen >= 1 and n_pdep_basis >= 2 n_pdep_eigen (davidson_diago.f90:107)");
-  if (nvecx > 1024) return fail(WB_ERR_UNSUPPORTED, "n_pdep_basis > 1024 is not provided by the Jacobi eigensolver");
+  if (nvecx > kMaxBasis)
+    return fail(WB_ERR_UNSUPPORTED, "n_pdep_basis > " + std::to_string(kMaxBasis) + " is not provided");
   if (p->n_pdep_maxiter < 1) return fail(WB_ERR_ARG, "n_pdep_maxiter < 1");
   if ((dvg0 && ld_dvg0 < c->npw) || (pdep && ld_pdep < c->npw))
     return fail(WB_ERR_ARG, "leading dimension smaller than npw");
   const auto t0 = std::chrono::steady_clock::now();
   WB_CU(cudaSetDevice(c->device));
-  WB_CU(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(jacobi_pairs_bytes(kJacobiSmemN) +
-                                   2 * sizeof(double) * kJacobiSmemN * kJacobiSmemN)));
+  jacobi_setup();
+  WB_CU(cudaGetLastError());
   Dav d;
   d.c = c;
   d.npw = c->npw;
@@ -363,8 +725,10 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
       c->dav_A.ensure(sizeof(double) * nvecx * nvecx) || c->dav_V.ensure(sizeof(double) * nvecx * nvecx) ||
       c->dav_w.ensure(sizeof(double) * nvecx + 64) ||
       c->dav_part.ensure(sizeof(double) * (size_t)d.nsplit * nvecx * nvecx) ||
-      c->dav_coef.ensure(sizeof(double) * 2 * nvecx * nvecx) || c->dav_dots.ensure(sizeof(double) * (nvecx + 1)))
+      c->dav_coef.ensure(sizeof(double) * 2 * nvecx * nvecx) || c->dav_dots.ensure(sizeof(double) * (nvecx + 1)) ||
+      (nvecx > kJacobiSmemN && c->dav_bj.ensure(sizeof(double) * bj_doubles(nvecx))))
     return fail(WB_ERR_NOMEM, "device allocation of the Davidson basis failed");
+  d.bj = c->dav_bj.as<double>();
   d.dvg = c->dav_dvg.as<double2>();
   d.dng = c->dav_dng.as<double2>();
   d.tmp = c->dav_tmp.as<double2>();
@@ -506,5 +870,27 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
     info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     info->seconds_apply = d.apply_s;
   }
+  return WB_OK;
+}
+
+extern "C" int wb_diagox(wb_ctx* c, int nbase, int nvec, const double* hr, int ldh, double* ew, double* vr, int ldv) {
+  if (!c || !hr || !ew || !vr) return fail(WB_ERR_ARG, "null argument");
+  if (nbase < 1 || nvec < 1 || nvec > nbase) return fail(WB_ERR_ARG, "need 1 <= nvec <= nbase");
+  if (nbase > kMaxBasis) return fail(WB_ERR_UNSUPPORTED, "nbase > " + std::to_string(kMaxBasis) + " is not provided");
+  if (ldh < nbase || ldv < nbase) return fail(WB_ERR_ARG, "leading dimension smaller than nbase");
+  WB_CU(cudaSetDevice(c->device));
+  jacobi_setup();
+  WB_CU(cudaGetLastError());
+  const size_t nn = (size_t)nbase * nbase;
+  if (c->dav_A.ensure(sizeof(double) * nn) || c->dav_V.ensure(sizeof(double) * nn) ||
+      c->dav_w.ensure(sizeof(double) * nbase + 64) ||
+      (nbase > kJacobiSmemN && c->dav_bj.ensure(sizeof(double) * bj_doubles(nbase))))
+    return fail(WB_ERR_NOMEM, "device allocation of the eigensolver scratch failed");
+  double* w = c->dav_w.as<double>();
+  int rc = eigen_lowest(hr, ldh, nbase, nvec, w, vr, ldv, c->dav_A.as<double>(), c->dav_V.as<double>(),
+                        c->dav_bj.as<double>(), reinterpret_cast<int*>(w + nbase), c->stream);
+  if (rc) return rc;
+  WB_CU(cudaMemcpyAsync(ew, w, sizeof(double) * nvec, cudaMemcpyDeviceToHost, c->stream));
+  WB_CU(cudaStreamSynchronize(c->stream));
   return WB_OK;
 }

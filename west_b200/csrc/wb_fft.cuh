@@ -22,13 +22,13 @@ namespace wb {
 
 template <int N> struct FftSplit;
 template <> struct FftSplit<16> { static constexpr int N1 = 4, N2 = 4; };
-template <> struct FftSplit<20> { static constexpr int N1 = 5, N2 = 4; };
-template <> struct FftSplit<24> { static constexpr int N1 = 6, N2 = 4; };
+template <> struct FftSplit<20> { static constexpr int N1 = 4, N2 = 5; };
+template <> struct FftSplit<24> { static constexpr int N1 = 4, N2 = 6; };
 template <> struct FftSplit<32> { static constexpr int N1 = 8, N2 = 4; };
-template <> struct FftSplit<36> { static constexpr int N1 = 6, N2 = 6; };
+template <> struct FftSplit<36> { static constexpr int N1 = 4, N2 = 9; };
 template <> struct FftSplit<40> { static constexpr int N1 = 8, N2 = 5; };
 template <> struct FftSplit<48> { static constexpr int N1 = 8, N2 = 6; };
-template <> struct FftSplit<60> { static constexpr int N1 = 10, N2 = 6; };
+template <> struct FftSplit<60> { static constexpr int N1 = 12, N2 = 5; };
 template <> struct FftSplit<64> { static constexpr int N1 = 8, N2 = 8; };
 template <> struct FftSplit<72> { static constexpr int N1 = 8, N2 = 9; };
 template <> struct FftSplit<80> { static constexpr int N1 = 8, N2 = 10; };

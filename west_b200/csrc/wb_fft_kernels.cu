@@ -284,32 +284,32 @@ struct EpiDng {
 // Zero what the inverse transforms read: with pruning (PR) only the active
 // columns (which then are all x in [0, N/4) u [3N/4, N)) at live rows (y in
 // the same quarters), otherwise the whole plane.
-template <int N, bool PR, class C, class PL = Plane<N>>
+template <int N, bool PR, class C, class PL = Plane<N>, int NT = PNT>
 WB_DEV void plane_zero(C* pl, const StickTab& st) {
   if constexpr (PR && Prune<N>::IN_OK) {
     constexpr int NL = 2 * (N / 4);
     const int nc = st.ncols, nlow = st.xhi + 1;
-    for (int e = threadIdx.x; e < NL * nc; e += PNT) {
+    for (int e = threadIdx.x; e < NL * nc; e += NT) {
       const int l = e % nc, r = e / nc;
       const int x = l < nlow ? l : N - nc + l;
       const int y = r < N / 4 ? r : N - NL + r;
       pl[PL::at(x, y)] = mkc<C>(0, 0);
     }
   } else {
-    for (int e = threadIdx.x; e < PL::SIZE; e += PNT) pl[e] = mkc<C>(0, 0);
+    for (int e = threadIdx.x; e < PL::SIZE; e += NT) pl[e] = mkc<C>(0, 0);
   }
 }
 // stick positions are y*N + x in row-major plane order
-template <int N, class C, class PL = Plane<N>>
+template <int N, class C, class PL = Plane<N>, int NT = PNT>
 WB_DEV void plane_scatter(C* pl, const C* __restrict__ sz, const int* __restrict__ pos, int nst) {
-  for (int s = threadIdx.x; s < nst; s += PNT) {
+  for (int s = threadIdx.x; s < nst; s += NT) {
     const int p = pos[s];
     if (p >= 0) pl[PL::at_lin(p)] = sz[s];
   }
 }
-template <int N, class C, class PL = Plane<N>>
+template <int N, class C, class PL = Plane<N>, int NT = PNT>
 WB_DEV void plane_gather(const C* pl, C* __restrict__ sz, const int* __restrict__ pos, int nst) {
-  for (int s = threadIdx.x; s < nst; s += PNT) {
+  for (int s = threadIdx.x; s < nst; s += NT) {
     const int p = pos[s];
     sz[s] = p >= 0 ? pl[PL::at_lin(p)] : mkc<C>(0, 0);
   }
@@ -663,6 +663,164 @@ __global__ void __launch_bounds__(PNT, 3) k_plane_vloc_fused(C* __restrict__ sti
 }
 
 // ---------------------------------------------------------------------------
+// One-pass local-potential plane kernel for any split N = A x B (A = N1, B = N2)
+// ---------------------------------------------------------------------------
+// Rows: the inverse uses the split (A, B), the forward the transposed split
+// (B, A).  The inverse's second step leaves X[k1 + A k2] (k2 = 0..B-1) in the
+// thread owning k1, which is the input set {A n1' + n2'} of the forward's first
+// step for n2' = k1: the inverse step 2, the V(r) product and the forward
+// step 1 run in registers of one thread.  Each of the three row phases reads and
+// writes the same plane positions per thread, so they need one block barrier
+// between phases and none inside.  The forward's outputs k1' + B k2' are live
+// (pruned transforms) iff k2' lies in the outer quarters of A, the condition of
+// the inverse's live inputs, so A % 4 == 0 prunes both directions; the forward
+// column pass uses the transposed split for the same reason.
+
+// W_N^(n2 k1) for the step-1 twiddle of the split (S1, S2), k1 < S1, n2 < S2,
+// from the second half of the table (built for FftSplit<N>)
+template <int N, int S1, int S2, class C>
+WB_DEV C tw_step1(const C* tw, int k1, int n2) {
+  constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
+  static_assert(S1 * S2 == N && (S1 == N1 || S1 == N2), "split of N");
+  if constexpr (S1 == N1) return tw[N + k1 * N2 + n2];
+  else return tw[N + n2 * N2 + k1];
+}
+template <int S>
+WB_DEV constexpr bool outer_quarter(int i) { return i < S / 4 || i >= S - S / 4; }
+
+// Line transforms with an explicit split N = S1 x S2 over lines whose element e
+// sits at loff(l) + e es; consecutive threads take consecutive lines.  PIN:
+// only inputs S2 n1 + n2 with n1 in the outer quarters of S1 are nonzero; POUT:
+// only outputs k1 + S1 k2 with k2 in the outer quarters of S2 are stored.
+template <int N, int S1, int S2, int DIR, int NT, bool PIN, bool POUT, class Off, class C>
+WB_DEV void fft_lines_split(C* data, Off loff, int es, int nlines, const C* tw) {
+  static_assert(!PIN || S1 % 4 == 0, "input pruning needs S1 % 4 == 0");
+  static_assert(!POUT || S2 % 4 == 0, "output pruning needs S2 % 4 == 0");
+  for (int it = threadIdx.x; it < nlines * S2; it += NT) {
+    const int line = it % nlines, n2 = it / nlines;
+    C* p = data + loff(line);
+    C v[S1];
+#pragma unroll
+    for (int n1 = 0; n1 < S1; ++n1)
+      v[n1] = (PIN && !outer_quarter<S1>(n1)) ? mkc<C>(0, 0) : p[(S2 * n1 + n2) * es];
+    rdft<S1, DIR, N>(v, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < S1; ++k1) v[k1] = ctw<DIR>(v[k1], tw_step1<N, S1, S2>(tw, k1, n2));
+#pragma unroll
+    for (int k1 = 0; k1 < S1; ++k1) p[(S2 * k1 + n2) * es] = v[k1];
+  }
+  __syncthreads();
+  constexpr int LPC = NT / S1;
+  const int nch = (nlines + LPC - 1) / LPC;
+  for (int c = 0; c < nch; ++c) {
+    const int line = c * LPC + (int)threadIdx.x % LPC, k1 = (int)threadIdx.x / LPC;
+    const bool act = (int)threadIdx.x < LPC * S1 && line < nlines;
+    C* p = data + (act ? loff(line) : 0);
+    C v[S2];
+    if (act) {
+#pragma unroll
+      for (int n2 = 0; n2 < S2; ++n2) v[n2] = p[(S2 * k1 + n2) * es];
+      rdft<S2, DIR, N>(v, tw);
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int k2 = 0; k2 < S2; ++k2)
+        if (!POUT || outer_quarter<S2>(k2)) p[(k1 + S1 * k2) * es] = v[k2];
+    }
+  }
+  __syncthreads();
+}
+
+// Rows, phase 2: the inverse step 2 (B-point DFT of thread k1), V(r)/N^3 and the
+// forward step 1 of the split (B, A) with its twiddles, written back in place.
+template <int N, int NT, class C>
+WB_DEV void rows_vloc_middle(C* pl, const C* tw, const real_t<C>* __restrict__ vz) {
+  constexpr int A = FftSplit<N>::N1, B = FftSplit<N>::N2;
+  using LP = LinePad<N>;
+  using T = real_t<C>;
+  for (int it = threadIdx.x; it < N * A; it += NT) {
+    const int y = it / A, k1 = it % A;
+    C* p = pl + Plane<N>::row(y);
+    T vr[B];
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) vr[k2] = __ldg(vz + y * N + k1 + A * k2);
+    C v[B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) v[n2] = p[LP::off_blk(k1, n2)];
+    rdft<B, +1, N>(v, tw);                          // X[k1 + A k2]
+#pragma unroll
+    for (int k2 = 0; k2 < B; ++k2) v[k2] = cscale(v[k2], vr[k2]);
+    rdft<B, -1, N>(v, tw);                          // forward step 1, n2' = k1
+#pragma unroll
+    for (int q = 1; q < B; ++q) v[q] = ctw<-1>(v[q], tw_step1<N, B, A>(tw, q, k1));
+#pragma unroll
+    for (int q = 0; q < B; ++q) p[LP::off_blk(k1, q)] = v[q];
+  }
+}
+
+// Rows, phase 3: the forward step 2 of the split (B, A): thread k1' < B takes
+// Y[k1', n2'] from off_blk(n2', k1') and writes output k1' + B k2' to
+// off_blk(k2', k1'), the positions it read.
+template <int N, int NT, bool POUT, class C>
+WB_DEV void rows_forward_step2(C* pl, const C* tw) {
+  constexpr int A = FftSplit<N>::N1, B = FftSplit<N>::N2;
+  static_assert(!POUT || A % 4 == 0, "output pruning of the transposed split needs A % 4 == 0");
+  using LP = LinePad<N>;
+  for (int it = threadIdx.x; it < N * B; it += NT) {
+    const int y = it / B, k1 = it % B;
+    C* p = pl + Plane<N>::row(y);
+    C v[A];
+#pragma unroll
+    for (int n2 = 0; n2 < A; ++n2) v[n2] = p[LP::off_blk(n2, k1)];
+    rdft<A, -1, N>(v, tw);
+#pragma unroll
+    for (int k2 = 0; k2 < A; ++k2)
+      if (!POUT || outer_quarter<A>(k2)) p[LP::off_blk(k2, k1)] = v[k2];
+  }
+}
+
+template <int N, class C>
+static constexpr size_t psmem_c() { return sizeof(C) * (2 * N + Plane<N>::SIZE); }
+// threads per CTA of the one-pass kernel: 512 in FP32 (two CTAs of 56
+// registers per thread fit an SM up to 108^3) and in FP64 where the plane
+// allows only one CTA per SM (from 80^3 up), 256 otherwise
+template <int N, class C>
+constexpr int gen_threads() {
+  return (sizeof(C) == 8 || 2 * psmem_c<N, C>() > 227u * 1024u) ? 512 : 256;
+}
+
+template <int N, bool PR, class C>
+__global__ void __launch_bounds__(gen_threads<N, C>()) k_plane_vloc_gen(C* __restrict__ sticks, StickTab st,
+                                                                         const real_t<C>* __restrict__ vs,
+                                                                         const C* __restrict__ twg, const int* dn) {
+  constexpr int NT = gen_threads<N, C>();
+  constexpr int N1 = FftSplit<N>::N1, N2 = FftSplit<N>::N2;
+  constexpr bool RP = PR && (N1 % 4 == 0);  // pruned rows and columns, both directions
+  if (dn && (int)blockIdx.y >= dev_count<true>(dn, 0)) return;
+  C* tw = smem_tw<C>();
+  C* pl = smem_tw<C>() + 2 * N;
+  const int z = blockIdx.x, item = blockIdx.y;
+  C* sz = sticks + ((long)item * N + z) * st.nst;
+  load_tw<N>(tw, twg);
+  plane_zero<N, PR, C, Plane<N>, NT>(pl, st);
+  __syncthreads();
+  plane_scatter<N, C, Plane<N>, NT>(pl, sz, st.st_pos, st.nst);
+  __syncthreads();
+  const OffCols<N> cols{st.xhi + 1, st.ncols};
+  fft_lines_split<N, N1, N2, +1, NT, RP, false>(pl, cols, Plane<N>::RS, st.ncols, tw);
+  fft_step1<N, +1, NT, false, true, RP ? PRUNE_IN : PRUNE_NONE>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
+  __syncthreads();
+  rows_vloc_middle<N, NT>(pl, tw, vs + (long)z * N * N);
+  __syncthreads();
+  rows_forward_step2<N, NT, RP>(pl, tw);
+  __syncthreads();
+  if constexpr (RP) fft_lines_split<N, N2, N1, -1, NT, false, true>(pl, cols, Plane<N>::RS, st.ncols, tw);
+  else fft_lines_split<N, N1, N2, -1, NT, false, false>(pl, cols, Plane<N>::RS, st.ncols, tw);
+  plane_gather<N, C, Plane<N>, NT>(pl, sz, st.st_pos, st.nst);
+}
+
+// ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
 template <int N, class C = double2>
@@ -695,6 +853,14 @@ struct FftN {
       cudaFuncSetAttribute(k_plane_vloc_fused<N, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)fsmem<N, float2>());
     }
+    cudaFuncSetAttribute(k_plane_vloc_gen<N, false, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)psmem_c<N, double2>());
+    cudaFuncSetAttribute(k_plane_vloc_gen<N, true, double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)psmem_c<N, double2>());
+    cudaFuncSetAttribute(k_plane_vloc_gen<N, false, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)psmem_c<N, float2>());
+    cudaFuncSetAttribute(k_plane_vloc_gen<N, true, float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)psmem_c<N, float2>());
     for (int pr = 0; pr < 2; ++pr) {
       auto zi = pr ? k_zinv<N, true, float2> : k_zinv<N, false, float2>;
       auto zf = pr ? k_zfwd<N, true, float2, EpiHpsi32> : k_zfwd<N, false, float2, EpiHpsi32>;
@@ -705,12 +871,16 @@ struct FftN {
     }
   }
   static dim3 zgrid(const StickTab& st, int nitems) { return dim3((st.nsp + ZSG - 1) / ZSG, nitems); }
-  static bool fused(const StickTab& st) {
+  // one-pass plane kernels: the register-row kernel for 8 x 8 and 4 x 4 splits
+  // (pruned, sticks preloaded into registers), the generic one for every other
+  // box and stick table
+  static bool fused_square(const StickTab& st) {
     if constexpr (FUSABLE) return st.prune && st.nst <= kFusedMaxSticksPerThread * PNT;
     return false;
   }
+  static bool fused(const StickTab&) { return true; }
   template <class F>
-  static bool use_fused(const F& f) { return !f.unfused && fused(f.st); }
+  static bool use_fused(const F& f) { return !f.unfused; }
   // Local-potential transforms of the PCG operator, FP64 (C = double2) or the
   // FP32 inner solves (C = float2): one CTA per (stick group or plane, item);
   // with a device count (graph replays) nitems is the bound the grid is sized
@@ -729,11 +899,19 @@ struct FftN {
     if (nitems <= 0) return;
     constexpr size_t ps = psmem<N, C>();
     const dim3 g(N, nitems);
-    if constexpr (FUSABLE) {
-      if (use_fused(f)) {
-        k_plane_vloc_fused<N, C><<<g, PNT, fsmem<N, C>(), f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
-        return;
+    if (use_fused(f)) {
+      if constexpr (FUSABLE) {
+        if (fused_square(f.st)) {
+          k_plane_vloc_fused<N, C><<<g, PNT, fsmem<N, C>(), f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+          return;
+        }
       }
+      constexpr int gnt = gen_threads<N, C>();
+      if (f.st.prune)
+        k_plane_vloc_gen<N, true, C><<<g, gnt, psmem_c<N, C>(), f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+      else
+        k_plane_vloc_gen<N, false, C><<<g, gnt, psmem_c<N, C>(), f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
+      return;
     }
     if (f.st.prune) k_plane_vloc<N, true, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);
     else k_plane_vloc<N, false, C><<<g, PNT, ps, f.stream>>>(sticks, f.st, vs, f.tw, f.dcount);

@@ -25,7 +25,7 @@ EXPORTS = (
     "wb_ctx_create", "wb_ctx_destroy", "wb_apply_operator", "wb_apply_operator_device",
     "wb_apply_operator_device_noalloc",
     "wb_apply_operator_multi", "wb_set_precision", "wb_set_batch", "wb_get_stats", "wb_set_profiling",
-    "wb_set_graphs", "wb_get_tuning", "wb_set_autotune", "wb_davidson", "wb_davidson_set_apply",
+    "wb_set_graphs", "wb_get_tuning", "wb_set_autotune", "wb_davidson", "wb_davidson_set_apply", "wb_diagox",
     "wb_pdep_db_write",
     "wb_pdep_db_read", "wb_last_error", "wb_version",
 )
@@ -109,6 +109,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.wb_davidson_set_apply.argtypes = [_p, WB_APPLY_FN, _p]
     lib.wb_davidson.argtypes = [_p, ctypes.POINTER(WbDavidsonParams), _p, _i, _p, _p, _p, _i,
                                 ctypes.POINTER(WbDavidsonInfo)]
+    lib.wb_diagox.argtypes = [_p, _i, _i, _p, _i, _p, _p, _i]
     lib.wb_pdep_db_write.argtypes = [ctypes.c_char_p, _i, _p, _p, _i, _p, _p, _i, _i]
     lib.wb_pdep_db_read.argtypes = [ctypes.c_char_p, _i, _i, _p, _p, _i, _i]
     lib.wb_last_error.restype = ctypes.c_char_p

@@ -181,6 +181,20 @@ class ResponseOperator:
         return ev, conv.astype(bool), vec, {k: getattr(info, k) for k, _ in info._fields_}
 
 
+def diagox(op, hr, nbase, nvec):
+    """diagox_dsy (Wstat/wstat_tools.f90:48) through wb_diagox: the nvec lowest
+    eigenpairs of the symmetric hr[:nbase, :nbase] (upper triangle read).  hr is
+    a float64 CUDA tensor holding the column-major [ldh, nbase] array as a
+    row-major [nbase, ldh] tensor.  Returns (ew numpy [nvec], vr CUDA tensor
+    [nvec, ldv]: row k is eigenvector k)."""
+    import torch
+    ldh = int(hr.shape[1])
+    vr = torch.zeros((nvec, nbase), dtype=torch.float64, device=hr.device)
+    ew = np.zeros(nvec)
+    _lib.check(op._lib.wb_diagox(op._ctx, int(nbase), int(nvec), hr.data_ptr(), ldh, _ptr(ew), vr.data_ptr(), nbase))
+    return ew, vr
+
+
 def apply_operator_multi(ops, dvgs, dngs, tr2, iq=1):
     """Several ground states in one call (wb_apply_operator_multi): ops[i] maps
     dvgs[i] [npwqx_i, m_i] to dngs[i]; the systems run concurrently on one GPU.
