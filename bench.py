@@ -48,6 +48,13 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pdep", action="store_true", help="skip the time-to-PDEP Davidson run")
     ap.add_argument("--no-multi", action="store_true", help="skip the three-system uneven batch")
+    ap.add_argument("--large-davidson", action="store_true",
+                    help="only the 108^3 PDEP Davidson (n_pdep_eigen 256 x 4), FP64 and mixed: one JSON line")
+    ap.add_argument("--no-large-pdep", action="store_true",
+                    help="skip the 108^3 PDEP Davidson of the default run (about two minutes)")
+    ap.add_argument("--trev", type=float, default=1e-6, help="trev_pdep of --large-davidson")
+    ap.add_argument("--tr2-dfpt", type=float, default=TR2, help="tr2_dfpt of --large-davidson")
+    ap.add_argument("--n-pdep-eigen", type=int, default=256, help="n_pdep_eigen of --large-davidson")
     return ap.parse_args()
 
 
@@ -371,6 +378,12 @@ def run_b200(args, rank, world, local_rank):
                 line[key] = fn(local_rank, args)
             except Exception as e:  # a failed side measurement must not lose the headline line
                 line[key] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
+    if rank == 0 and world == 1 and not args.no_large_pdep:
+        try:
+            ld = _large_davidson(args, local_rank)
+            line["large_cell_pdep"] = {k: ld[k] for k in ("config", "fp64", "mixed", "mixed_vs_fp64", "clocks")}
+        except Exception as e:
+            line["large_cell_pdep"] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
     return line
 
 
@@ -502,8 +515,57 @@ def _time_to_pdep(device, precision):
             "ev": [float(x) for x in ev]}
 
 
+def _large_davidson(args, device):
+    """Wstat time-to-PDEP on the large cell: L = 30 bohr, 30 Ry, 108^3, 20 atoms (s+p),
+    nbnd_occ 128, n_pdep_eigen 256 x n_pdep_times 4 (basis 1024), PCG threshold
+    tr2_dfpt, Davidson tolerance trev_pdep; FP64 then mixed from the same
+    starting basis, with the largest relative eigenvalue difference."""
+    import torch
+    from west_b200.system import build_system, randomized_basis
+    from west_b200.wstat import ResponseOperator
+    t0 = time.time()
+    s = build_system("c5", device="cuda")
+    t_sys = time.time() - t0
+    nvec = args.n_pdep_eigen
+    dvg0 = randomized_basis(s, nvec)
+    out = {"metric": "Wstat time-to-PDEP (s), 108^3 large cell", "unit": "s", "higher_is_better": False,
+           "n_gpus": 1, "dtype": "f64 / mixed", "data": "synthetic (seeded Gaussian pseudo-atoms, LOBPCG ground state)",
+           "config": {"workload": f"Davidson c5: L=30 bohr, 30 Ry, 108^3, 20 atoms (sp), nbnd_occ=128, npw={s.npw}, "
+                                  f"n_pdep_eigen={nvec}, n_pdep_times=4, tr2_dfpt={args.tr2_dfpt:g}, "
+                                  f"trev_pdep={args.trev:g}, trev_pdep_rel=0.1",
+                      "system_build_s": round(t_sys, 1)}}
+    evs = {}
+    with ClockSampler(device) as clk:
+        for prec in ("fp64", "mixed"):
+            op = ResponseOperator(s, device=device, verbose=False)
+            op.set_precision(prec)
+            torch.cuda.synchronize()
+            ev, conv, _, info = op.davidson(dvg0, nvec, n_pdep_times=4, n_pdep_maxiter=100, tr2_dfpt=args.tr2_dfpt,
+                                            trev_pdep=args.trev, trev_pdep_rel=1e-1)
+            evs[prec] = ev
+            out[prec] = {"seconds": info["seconds"], "seconds_apply": info["seconds_apply"],
+                         "dav_iter": info["dav_iter"], "converged": bool(info["converged"]),
+                         "notcnv": info["notcnv"], "apply_calls": info["apply_calls"],
+                         "perturbations_applied": info["perturbations"],
+                         "ev_lowest": [float(x) for x in ev[:4]], "ev_highest": [float(x) for x in ev[-4:]]}
+            op.close()
+        clk.end = len(clk.lines)
+    rel = np.abs((evs["mixed"] - evs["fp64"]) / evs["fp64"])
+    out["mixed_vs_fp64"] = {"speedup": out["fp64"]["seconds"] / out["mixed"]["seconds"],
+                            "ev_max_rel_diff": float(rel.max()), "ev_median_rel_diff": float(np.median(rel)),
+                            "ev_max_abs_diff": float(np.abs(evs["mixed"] - evs["fp64"]).max())}
+    out["value"] = out["fp64"]["seconds"]
+    out["clocks"] = clk.summary()
+    return out
+
+
 def main():
     args = _args()
+    if args.large_davidson:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(_large_davidson(args, 0)), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

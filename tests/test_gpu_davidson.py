@@ -92,3 +92,27 @@ def test_davidson_c1_configuration(precision):
                                       trev_pdep_rel=1e-1)
     assert info["converged"] == 1 and c["rconv"].all()
     assert np.abs((ev - c["rev"]) / c["rev"]).max() < TOL_EV
+
+
+def test_davidson_108cube_reduced_both_forms():
+    """The 108^3 box (radix 12 x 9 transforms, one-pass plane kernel) in a
+    reduced system (3 bands, npw 36,763): 8 eigenpairs x 4, tight thresholds
+    (tr2_dfpt 1e-14, trev_pdep 1e-9), FP64 and mixed against the oracle's
+    Davidson at 1e-6."""
+    import math
+    from west_b200.system import SystemSpec
+    from west_b200.wstat import ResponseOperator
+    L = 8.0 + 108 / 6.0
+    spec = SystemSpec(L=L, ecutwfc=(26 * 2.0 * math.pi / L) ** 2 * (1.0 + 1e-9), nr=108, natoms=2, nbnd_occ=3,
+                      proj="sp", seed=208)
+    s = build_system(spec, "cuda")
+    dvg0 = randomized_basis(s, 8)
+    kw = dict(tr2_dfpt=1e-14, trev_pdep=1e-9, trev_pdep_rel=1e-1)
+    rev, rconv, _, rit = O.davidson_diago_gamma(s, dvg0, 8, 32, **kw)
+    assert rconv.all()
+    for precision in ("fp64", "mixed"):
+        op = ResponseOperator(s, verbose=False)
+        op.set_precision(precision)
+        ev, conv, _, info = op.davidson(dvg0, 8, n_pdep_times=4, **kw)
+        assert info["converged"] == 1, precision
+        assert np.abs((ev - rev) / rev).max() < TOL_EV, (precision, np.abs((ev - rev) / rev).max())
