@@ -50,7 +50,9 @@ typedef struct wb_system {
   const double* vrs;   /* [nr1*nr2*nr3] scf vrs(:,1) on the smooth grid (Ry)      */
   const double* evc;   /* [npwx, nbnd_occ] complex: wavefunctions evc             */
   const double* et;    /* [nbnd_occ] wvfct et(:,1) (Ry)                           */
-  const double* occupation; /* [nbnd_occ] westcom occupation(:,1)                 */
+  const double* occupation; /* [nbnd_occ] westcom occupation(:,1); bands below
+                               1 - 1e-3 are fractionally occupied (l_frac_occ,
+                               dfpt_module.f90:328-401, set_nbndocc.f90:58-69) */
   const double* vkb;   /* [npwx, nkb] complex: uspp vkb after init_us_2           */
   const double* deeq;  /* [nkb, nkb] KB coupling D, dense (block-diagonal per atom) */
   const double* sqvc;  /* [npw] pot3D%sqvc (Coulomb_kernel/class_coulomb.f90:173) */

@@ -8,7 +8,8 @@ What it restates, function by function, with the reference file:line each one
 follows (paths inside the WEST 6.2.0 tree):
 
 * ``apply_operator``            Wstat/apply_operator.f90:14-69
-* ``dfpt``                      DFPT_kernel/dfpt_module.f90:22-533 (Gamma branches)
+* ``dfpt``                      DFPT_kernel/dfpt_module.f90:22-533 (Gamma branches,
+                                fractional occupations :328-401)
 * ``linsolve_sternheimer``      DFPT_kernel/linsolve_sternheimer_m_wfcts.f90:14-382
 * ``apply_sternheimerop``       DFPT_kernel/apply_sternheimerop_to_m_wfcs.f90:14-84
 * ``precondition_m_wfcts``      DFPT_kernel/precondition_m_wfcts.f90:14-53
@@ -56,27 +57,33 @@ _WORKERS = int(os.environ.get("WEST_ORACLE_WORKERS", len(os.sched_getaffinity(0)
 # ----------------------------------------------------------------------------
 # FFTs in QE's convention on an nr^3 box stored x fastest.
 # ----------------------------------------------------------------------------
+def _edges(nr):
+    return tuple(int(x) for x in nr) if isinstance(nr, (tuple, list)) else (int(nr),) * 3
+
+
 def _boxes(a, nr):
-    return a.reshape(a.shape[:-1] + (nr, nr, nr))
+    n1, n2, n3 = _edges(nr)
+    return a.reshape(a.shape[:-1] + (n3, n2, n1))
 
 
 def invfft(box, nr):
-    """QE invfft 'Wave': f(r) = sum_G f(G) exp(+iGr), unscaled.  box [..., nnr]."""
+    """QE invfft 'Wave': f(r) = sum_G f(G) exp(+iGr), unscaled.  box [..., nnr],
+    nr the box edge or (nr1, nr2, nr3), x fastest."""
     x = _boxes(box, nr)
     if _sfft is not None:
         y = _sfft.ifftn(x, axes=(-3, -2, -1), norm="forward", workers=_WORKERS)
     else:
-        y = np.fft.ifftn(x, axes=(-3, -2, -1)) * nr ** 3
+        y = np.fft.ifftn(x, axes=(-3, -2, -1)) * x.shape[-1] * x.shape[-2] * x.shape[-3]
     return y.reshape(box.shape)
 
 
 def fwfft(box, nr):
-    """QE fwfft 'Wave': f(G) = (1/N^3) sum_r f(r) exp(-iGr).  box [..., nnr]."""
+    """QE fwfft 'Wave': f(G) = (1/N) sum_r f(r) exp(-iGr), N = nr1 nr2 nr3.  box [..., nnr]."""
     x = _boxes(box, nr)
     if _sfft is not None:
         y = _sfft.fftn(x, axes=(-3, -2, -1), norm="forward", workers=_WORKERS)
     else:
-        y = np.fft.fftn(x, axes=(-3, -2, -1)) / nr ** 3
+        y = np.fft.fftn(x, axes=(-3, -2, -1)) / (x.shape[-1] * x.shape[-2] * x.shape[-3])
     return y.reshape(box.shape)
 
 
@@ -87,12 +94,12 @@ def double_invfft_gamma(s, a1, a2):
     b = np.zeros((a1.shape[0], s.nnr), dtype=np.complex128)
     b[:, s.nl] = a1 + 1j * a2                              # :60
     b[:, s.nlm] = np.conj(a1 - 1j * a2)                    # :61 (wins at G=0)
-    return invfft(b, s.nr)
+    return invfft(b, s.nrs)
 
 
 def double_fwfft_gamma(s, a):
     """fft_at_gamma.f90:72-118.  a: box [k, nnr] -> (b1, b2) each [k, npw]."""
-    a = fwfft(np.atleast_2d(a), s.nr)
+    a = fwfft(np.atleast_2d(a), s.nrs)
     ap = a[:, s.nl]; am = a[:, s.nlm]
     fp = (ap + am) * 0.5                                   # :106
     fm = (ap - am) * 0.5                                   # :107
@@ -107,12 +114,12 @@ def single_invfft_gamma(s, a1):
     b = np.zeros((a1.shape[0], s.nnr), dtype=np.complex128)
     b[:, s.nl] = a1                                        # :152
     b[:, s.nlm] = np.conj(a1)                              # :153
-    return invfft(b, s.nr)
+    return invfft(b, s.nrs)
 
 
 def single_fwfft_gamma(s, a):
     """fft_at_gamma.f90:162-203."""
-    a = fwfft(np.atleast_2d(a), s.nr)
+    a = fwfft(np.atleast_2d(a), s.nrs)
     return a[:, s.nl]                                      # :194
 
 
@@ -175,7 +182,7 @@ def vloc_psi_gamma(s, psi):
     if m % 2:
         box = single_invfft_gamma(s, psi[:, m - 1])
         box *= s.vrs[None, :]
-        out[:, m - 1] = fwfft(box, s.nr)[0, s.nl]
+        out[:, m - 1] = fwfft(box, s.nrs)[0, s.nl]
     return out
 
 
@@ -287,18 +294,60 @@ def drho_gamma(s, dpsi):
     return (s.occupation[:, None] * box.real * box.imag).sum(0)
 
 
+DOCC_THR = 0.001   # westcom docc_thr (Modules/westcom.f90:417)
+DE_THR = 0.001     # westcom de_thr (Modules/westcom.f90:418)
+
+
+def nbnd_occ_full(s):
+    """Tools/set_nbndocc.f90:58-69: the highest band whose occupation exceeds
+    1 - docc_thr (all bands up to nbnd_occ count as fully occupied when the
+    occupations are integer)."""
+    full = np.flatnonzero(np.asarray(s.occupation) > 1.0 - DOCC_THR)
+    return int(full.max()) + 1 if full.size else 0
+
+
+def frac_coefficients(s, dvpsi):
+    """dfpt_module.f90:328-337 and :363-393 (Gamma): psi_dvpsi(j, i) =
+    <psi_j|dV psi_i> for the fractionally occupied bands j > nbnd_occ_full,
+    zeroed for j <= i and for |occ_i - occ_j| < docc_thr, else scaled by
+    (occ_i - occ_j) / occ_i / (e_i - e_j); degenerate pairs are an error as in
+    the reference (errore)."""
+    nb, nfull = s.nbnd_occ, nbnd_occ_full(s)
+    if nfull >= nb:
+        return None
+    ps = glbrak_gamma(s.evc[:, nfull:nb], dvpsi)           # [nfrac, nbnd]
+    occ, et = np.asarray(s.occupation), s.et
+    for i in range(nb):
+        for jf in range(nb - nfull):
+            j = nfull + jf
+            if j <= i:
+                ps[jf, i] = 0.0
+                continue
+            docc = occ[i] - occ[j]
+            if abs(docc) < DOCC_THR:
+                ps[jf, i] = 0.0
+                continue
+            de = et[i] - et[j]
+            if abs(de) < DE_THR:
+                raise ValueError("dfpt: fractional occupation degenerate orbitals")
+            ps[jf, i] *= docc / occ[i] / de
+    return ps
+
+
 def dfpt(s, dvg, tr2, maxiter=250, kinetic_only=False, eprec=None, trace=None):
-    """dfpt_module.f90:22-533 at Gamma, one k-point, no band groups, integer
-    occupations.  dvg [npw, m] -> (dng [npw, m], ierr [m])."""
+    """dfpt_module.f90:22-533 at Gamma, one k-point, no band groups, integer or
+    fractional occupations (l_frac_occ).  dvg [npw, m] -> (dng [npw, m], ierr [m])."""
     npw, m = dvg.shape
     l_dost = tr2 >= 0.0                                     # :130
     eprec = set_eprec(s) if eprec is None else eprec        # :211
     et = s.et[: s.nbnd_occ]
+    nfull = nbnd_occ_full(s)
     dng = np.zeros((npw, m), dtype=np.complex128)
     ierrs = np.zeros(m, dtype=np.int64)
     for ipert in range(m):                                  # :227
         aux_r = single_invfft_gamma(s, dvg[:, ipert])[0]    # :235
         dvpsi = dvpsi_rhs(s, aux_r)                         # :241-278
+        psi_dvpsi = frac_coefficients(s, dvpsi)             # :328-337, :363-393
         dvpsi = apply_alpha_pc(s, dvpsi, -1.0)              # :346
         dpsi = precondition_m_wfcts(s, dvpsi, eprec)        # :348
         if l_dost:                                          # :350-361
@@ -308,6 +357,8 @@ def dfpt(s, dvg, tr2, maxiter=250, kinetic_only=False, eprec=None, trace=None):
             ierrs[ipert] = ierr
             if trace is not None:
                 trace.append(tr)
+        if psi_dvpsi is not None:                           # :397-398 (DGEMM)
+            dpsi = dpsi + s.evc[:, nfull:s.nbnd_occ] @ psi_dvpsi
         aux_r = drho_gamma(s, dpsi)                          # :403-423
         aux_g = single_fwfft_gamma(s, aux_r.astype(np.complex128))[0]   # :478
         dng[:, ipert] += 2.0 * s.wk * aux_g / s.omega       # :485-487

@@ -157,3 +157,53 @@ def test_davidson_first_threshold_matches_reference_log():
     p = _pins()
     assert min(1e-4, 1e8 * p["tr2_dfpt"]) == p["davitr_dfpt_tr2"][0]
     assert all(t == p["tr2_dfpt"] for t in p["davitr_dfpt_tr2"][1:])
+
+
+def _sum_over_states_dng(s, dvg):
+    """dng from the independent-particle response written as a sum over all
+    eigenpairs of the dense Gamma Hamiltonian:
+    drho(r) = sum_{i<j} (f_i - f_j) / (e_i - e_j) psi_i(r) psi_j(r) <psi_j|dV|psi_i>,
+    f = the occupations of the occupied bands and 0 above; then the prefactors
+    of dfpt_module.f90:485-487 and apply_operator.f90:49-67."""
+    import math
+    from west_b200.system import _dense_gamma_hamiltonian
+    H = _dense_gamma_hamiltonian(dict(nr=s.nr, mill=s.mill, vrs=s.vrs, vkb=s.vkb, deeq=s.deeq,
+                                      g2kin=s.g2kin)).numpy()
+    w, v = np.linalg.eigh(0.5 * (H + H.T))
+    npw = s.npw
+    psi = np.empty((npw, w.size), dtype=np.complex128)
+    psi[0] = v[0]
+    psi[1:] = (v[1:npw] + 1j * v[npw:]) / math.sqrt(2.0)
+    f = np.zeros(w.size)
+    f[: s.nbnd_occ] = s.occupation
+    psir = np.stack([O.single_invfft_gamma(s, psi[:, k])[0].real for k in range(w.size)])
+    dng = np.zeros_like(dvg)
+    for p in range(dvg.shape[1]):
+        dv = O.single_invfft_gamma(s, dvg[:, p] * s.sqvc)[0].real
+        M = np.stack([O.single_fwfft_gamma(s, (psir[i] * dv).astype(np.complex128))[0] for i in range(w.size)], 1)
+        M = O.glbrak_gamma(psi, M)                       # M[j, i] = <psi_j|dV|psi_i>
+        drho = np.zeros(s.nnr)
+        for i in range(w.size):
+            for j in range(i + 1, w.size):
+                if f[i] != f[j]:
+                    drho += (f[i] - f[j]) / (w[i] - w[j]) * psir[i] * psir[j] * M[j, i]
+        g = O.single_fwfft_gamma(s, drho.astype(np.complex128))[0]
+        dng[:, p] = 2.0 * s.wk * g / s.omega * s.sqvc
+    dng[0] = 0.0
+    return dng
+
+
+@pytest.mark.parametrize("frac", [(), (0.5,)])
+def test_dfpt_matches_sum_over_states(frac):
+    """The Sternheimer route (integer occupations, and l_frac_occ with the
+    correction of dfpt_module.f90:328-401) against the sum over all states."""
+    import dataclasses
+    from west_b200.system import SPECS, build_system, perturbations
+    s = build_system(dataclasses.replace(SPECS["tiny"], frac_occ=frac))
+    if frac:
+        assert O.nbnd_occ_full(s) == s.nbnd_occ - 1
+    dvg = perturbations(s, 2)
+    got, ierr = O.apply_operator(s, dvg, 1e-26, maxiter=400)
+    ref = _sum_over_states_dng(s, dvg)
+    assert (ierr == 0).all()
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-9

@@ -304,6 +304,7 @@ int ensure_workspace(wb_ctx* c, int mb, long ld_in, long ld_out) {
   bad |= c->unconv.ensure(sizeof(int) * mb) != 0;
   bad |= c->items_pp.ensure(sizeof(int2) * mp) != 0;
   bad |= c->items_pk.ensure(sizeof(int2) * (size_t)mb * c->npv) != 0;
+  if (c->nfull < c->nocc) bad |= c->fcoef.ensure(sizeof(double) * nsys * (c->nocc - c->nfull)) != 0;
   if (bad) return fail(WB_ERR_NOMEM, "device workspace allocation failed for a batch of " + std::to_string(mb));
   return WB_OK;
 }
@@ -858,6 +859,11 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
     gemm_tn(Wevc, K, nocc, (const double*)B, 2 * ld, nullptr, nsys, K, nsplit, c->part.as<double>(), s);
     gamma_reduce(c->part.as<double>(), nsplit, nocc, nsys, Wevc, K, (const double*)B, 2 * ld, nullptr, nullptr, 0,
                  1.0, c->C.as<double>(), s);
+    // fractional occupations: <psi_j|dV psi_i> of the partly occupied bands j, scaled
+    // (dfpt_module.f90:328-337,363-393); C is reused by the PCG, so they are kept apart
+    if (c->nfull < nocc)
+      frac_coefficients(c->C.as<double>(), nocc, nsys, c->nfull, c->occ.as<double>(), c->et.as<double>(),
+                        c->fcoef.as<double>(), s);
     gemm_nn(Wevc, K, nocc, c->C.as<double>(), (double*)B, 2 * ld, nullptr, nsys, K, -1.0, s);
     // 5. dpsi = precondition(dvpsi)                    (dfpt_module.f90:348)
     precondition(B, X, c->iprec.as<double>(), nocc, npw, nsys, ld, s);
@@ -932,6 +938,11 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
     WB_CU(cudaMemsetAsync(c->unconv.p, 0, sizeof(int) * mb, s));
   }
   c->stats.cg_iterations = std::max(c->stats.cg_iterations, iters);
+  if (c->nfull < nocc) {                                // dpsi += evc_frac psi_dvpsi (dfpt_module.f90:397-398)
+    Stage g(c, WB_STAGE_OTHER, 1, nsys);
+    gemm_nn(Wevc + (size_t)c->nfull * K, K, nocc - c->nfull, c->fcoef.as<double>(), (double*)X, 2 * ld, nullptr, nsys,
+            K, 1.0, s);
+  }
   // 7. drho and dng                                   (dfpt_module.f90:403-487)
   {
     Stage g(c, WB_STAGE_DRHO, 3, (long long)mb * npv + mp);
@@ -1056,6 +1067,16 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
   c->omega = s->omega;
   c->wk = s->wk;
   c->alpha = s->alpha_pv;
+  // fractional occupations (Tools/set_nbndocc.f90:58-69): nbnd_occ_full is the
+  // highest band occupied above 1 - docc_thr; the correction of dfpt_module.f90:
+  // 363-398 needs non-degenerate energies wherever the occupations differ (:387)
+  for (int b = 0; b < c->nocc; ++b)
+    if (s->occupation[b] > 1.0 - 1e-3) c->nfull = b + 1;
+  for (int i = 0; i < c->nocc; ++i)
+    for (int r = std::max(i + 1, c->nfull); r < c->nocc; ++r)
+      if (std::fabs(s->occupation[i] - s->occupation[r]) >= 1e-3 && std::fabs(s->et[i] - s->et[r]) < 1e-3)
+        return bail(fail(WB_ERR_ARG, "fractional occupation degenerate orbitals (bands " + std::to_string(i + 1) +
+                                         " and " + std::to_string(r + 1) + ")"));
   std::vector<int> perm;
   int rc = build_tables(c, s, perm);
   if (rc) return bail(rc);
@@ -1121,7 +1142,7 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->D, &c->eprec, &c->et, &c->occ, &c->evcr, &c->iprec, &c->dvg_in, &c->dng_out, &c->aux, &c->dvbox, &c->B,
                   &c->X, &c->G, &c->T, &c->sticks, &c->sticks2, &c->acc, &c->part, &c->C, &c->rho, &c->conv,
                   &c->act, &c->items, &c->nact, &c->ecol, &c->epcol, &c->unconv, &c->items_pp, &c->items_pk,
-                  &c->iota_items, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
+                  &c->iota_items, &c->fcoef, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
                   &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots, &c->dav_bj, &c->W32, &c->D32, &c->g2kin32,
                   &c->vs32, &c->tw32, &c->g32, &c->P32, &c->T32, &c->d32, &c->sticks32, &c->part32, &c->C32,
                   &c->ecol32, &c->rho0, &c->rho_in, &c->conv_in, &c->act_in, &c->items_in, &c->nact_in,
@@ -1429,6 +1450,8 @@ extern "C" int wb_apply_operator_device_noalloc(wb_ctx* c, int m, const double* 
   if (std::isnan(tr2)) return fail(WB_ERR_ARG, "tr2 is NaN");
   if (c->precision != WB_PRECISION_FP64)
     return fail(WB_ERR_UNSUPPORTED, "the allocation-free entry point runs the FP64 form only");
+  if (c->nfull < c->nocc)
+    return fail(WB_ERR_UNSUPPORTED, "the allocation-free entry point has no fractional occupations");
   // the four PCG vectors alone must fit: this bounds m before any int product
   // of the layout (m * nbnd_occ systems, m * band pairs) is formed
   if (4.0 * sizeof(double2) * (double)m * c->nocc * c->npw > (double)WB_NOALLOC_SCRATCH_BYTES)

@@ -54,6 +54,7 @@ struct wb_ctx {
   cudaStream_t stream = nullptr;
   int npw = 0, nr = 0, nnr = 0, nocc = 0, nkb = 0, nproj = 0, npv = 0;
   int maxiter = 0, kinetic_only = 0, precision = WB_PRECISION_FP64, batch_cap = 0;
+  int nfull = 0;             // fully occupied bands (nbnd_occ_full); nocc - nfull fractional ones
   double omega = 0, wk = 0, alpha = 0;
   wb::StickTab st{};
   wb::FftArgs fa{};
@@ -61,7 +62,7 @@ struct wb_ctx {
   DBuf perm, gqz, spg, stpos, tw, g2kin, sqvc, vs, evc, W, D, eprec, et, occ, evcr, iprec;
   // per-call workspace
   DBuf dvg_in, dng_out, aux, dvbox, B, X, G, T, sticks, sticks2, acc, part, C, rho, conv, act, items, nact,
-      ecol, epcol, unconv, items_pp, items_pk, iota_items;
+      ecol, epcol, unconv, items_pp, items_pk, iota_items, fcoef;
   int* nact_host = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   wb_stats stats{};

@@ -121,6 +121,11 @@ void kinetic_hpsi(const double2* P, double2* T, const double* g2kin, const doubl
                   int npw, long ld, cudaStream_t s, const int* dn = nullptr);
 void set_eprec(const double2* evc, const double* g2kin, int npw, int nocc, double* eprec, cudaStream_t s);
 void fill_columns(const double* per_band, int nocc, int nsys, double* out, cudaStream_t s);
+// Fractional occupations (dfpt_module.f90:363-393): from C[j][r] = <psi_r|dV psi_i>
+// (j = p nocc + i, r < nocc) the coefficients fc[j][f] of the bands r = nfull + f:
+// 0 for r <= i or |occ_i - occ_r| < 1e-3, else C (occ_i - occ_r) / occ_i / (e_i - e_r)
+void frac_coefficients(const double* C, int nocc, int nsys, int nfull, const double* occ, const double* et,
+                       double* fc, cudaStream_t s);
 void cg_reset(unsigned char* conv, int nsys, cudaStream_t s);
 void cg_prec_rho(const int* act, int nact, const double2* g, double2* P, const double* iprec, int nocc,
                  double* rho_prev, unsigned char* conv, int iter, double tr2, int npw, long ld, cudaStream_t s,

@@ -356,6 +356,27 @@ void fill_columns(const double* per_band, int nocc, int nsys, double* out, cudaS
   k_fill_columns<<<(nsys + 255) / 256, 256, 0, s>>>(per_band, nocc, nsys, out);
 }
 
+__global__ void k_frac_coefficients(const double* __restrict__ C, int nocc, int nsys, int nfull,
+                                    const double* __restrict__ occ, const double* __restrict__ et,
+                                    double* __restrict__ fc) {
+  const int nfrac = nocc - nfull;
+  const long n = (long)nsys * nfrac;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const int j = (int)(e / nfrac), f = (int)(e % nfrac);
+    const int i = j % nocc, r = nfull + f;
+    double v = 0.0;
+    const double docc = occ[i] - occ[r];
+    if (r > i && fabs(docc) >= 1e-3) v = C[(long)j * nocc + r] * docc / occ[i] / (et[i] - et[r]);
+    fc[e] = v;
+  }
+}
+void frac_coefficients(const double* C, int nocc, int nsys, int nfull, const double* occ, const double* et,
+                       double* fc, cudaStream_t s) {
+  const long n = (long)nsys * (nocc - nfull);
+  if (n <= 0) return;
+  k_frac_coefficients<<<(int)std::min<long>((n + 255) / 256, 4096), 256, 0, s>>>(C, nocc, nsys, nfull, occ, et, fc);
+}
+
 // ---------------------------------------------------------------------------
 // masked PCG (linsolve_sternheimer_m_wfcts.f90:146-330), one CTA per system
 // ---------------------------------------------------------------------------

@@ -4,14 +4,14 @@ response operator.
 ``apply_operator`` (Wstat/apply_operator.f90:14) reads its ground state from
 Quantum ESPRESSO module variables: ``evc``, ``et``, ``g2kin``, ``vrs``,
 ``vkb``, ``deeq``, ``dffts%nl/nlm``, ``omega``, ``wk`` and the Coulomb factor
-``pot3D%sqvc``.  This module builds those arrays for a cubic cell filled with
-Gaussian pseudo-atoms, in QE's conventions:
+``pot3D%sqvc``.  This module builds those arrays for an orthorhombic (by
+default cubic) cell filled with Gaussian pseudo-atoms, in QE's conventions:
 
 * Rydberg units; kinetic energy ``g2kin = |G|^2 tpiba2``; ``e2 = 2``.
 * Gamma-only storage: the half sphere ``x > 0 | (x = 0, y > 0) | (x = y = 0,
   z >= 0)`` with ``psi(-G) = conj(psi(G))``, sorted by ``|G|^2`` so that G=0
   comes first (``gstart = 2`` in Fortran numbering).
-* ``nl``/``nlm``: box positions of +G / -G in an ``nr^3`` box, x fastest.
+* ``nl``/``nlm``: box positions of +G / -G in an ``nr1 x nr2 x nr3`` box, x fastest.
   They are returned 0-based here; the C ABI takes QE's 1-based values.
 * ``invfft`` is the unscaled sum over ``exp(+iGr)``; ``fwfft`` carries 1/N^3.
 
@@ -35,10 +35,10 @@ FPI = 4.0 * math.pi
 
 @dataclasses.dataclass(frozen=True)
 class SystemSpec:
-    """Parameters of a synthetic cubic Gamma-only system."""
-    L: float                 # cubic cell edge (bohr)
+    """Parameters of a synthetic orthorhombic (default cubic) Gamma-only system."""
+    L: float | tuple         # cell edge (bohr), or (Lx, Ly, Lz)
     ecutwfc: float           # wavefunction cutoff (Ry)
-    nr: int                  # FFT box edge
+    nr: int | tuple          # FFT box edge, or (nr1, nr2, nr3)
     natoms: int              # Gaussian pseudo-atoms at seeded uniform positions
     nbnd_occ: int            # occupied bands
     proj: str = "s"          # "s" or "sp": KB projectors per atom
@@ -48,6 +48,18 @@ class SystemSpec:
     dion: float = 1.0        # KB coupling D (Ry), diagonal
     nbnd_extra: int = 4      # empty bands computed beside the occupied ones
     seed: int = 0
+    frac_occ: tuple = ()     # occupations of the highest occupied bands (fractional
+                             # occupations, QE's wg / wk); the others are 1
+
+
+def cell_lengths(L) -> tuple:
+    """(Lx, Ly, Lz) of a cell given as one edge or three."""
+    return tuple(float(x) for x in L) if isinstance(L, (tuple, list)) else (float(L),) * 3
+
+
+def box_edges(nr) -> tuple:
+    """(nr1, nr2, nr3) of a box given as one edge or three."""
+    return tuple(int(x) for x in nr) if isinstance(nr, (tuple, list)) else (int(nr),) * 3
 
 
 # Workloads.  c1..c5 follow the five named configurations; ``tiny``/``small``
@@ -70,12 +82,12 @@ class GammaSystem:
     spec: SystemSpec
     omega: float
     tpiba2: float
-    nr: int
+    nr: int | tuple         # box edge (cubic) or (nr1, nr2, nr3)
     mill: np.ndarray        # int32 [npw, 3] Miller indices, |G| order, G=0 first
     g2kin: np.ndarray       # f64 [npw]
     nl: np.ndarray          # int64 [npw] 0-based box index of +G
     nlm: np.ndarray         # int64 [npw] 0-based box index of -G
-    vrs: np.ndarray         # f64 [nr^3] local potential on the box (x fastest)
+    vrs: np.ndarray         # f64 [nr1 nr2 nr3] local potential on the box (x fastest)
     vkb: np.ndarray         # c128 [npw, nkb]
     deeq: np.ndarray        # f64 [nkb, nkb]
     evc: np.ndarray         # c128 [npw, nbnd_occ]
@@ -99,50 +111,73 @@ class GammaSystem:
         return int(self.vkb.shape[1])
 
     @property
+    def nrs(self) -> tuple:
+        return box_edges(self.nr)
+
+    @property
     def nnr(self) -> int:
-        return self.nr ** 3
+        n1, n2, n3 = self.nrs
+        return n1 * n2 * n3
 
 
-def gamma_half_sphere(L: float, ecutwfc: float, nr: int):
-    """Miller indices of the Gamma half sphere |G|^2 tpiba2 <= ecutwfc,
-    sorted by |G|^2 (ties by Miller index) so that G=0 is first."""
-    tpiba2 = (2.0 * math.pi / L) ** 2
-    nmax = int(math.sqrt(ecutwfc / tpiba2)) + 1
-    r = np.arange(-nmax, nmax + 1)
-    i, j, k = np.meshgrid(r, r, r, indexing="ij")
+def gamma_half_sphere(L, ecutwfc: float, nr):
+    """Miller indices of the Gamma half sphere |G|^2 <= ecutwfc (Ry, bohr^-2) of an
+    orthorhombic cell L (one edge or three) in the box nr (one edge or three),
+    sorted by |G|^2 (ties by Miller index) so that G=0 is first.  Returns
+    (mill, tpiba2) with tpiba2 = (2 pi / Lx)^2 (QE's alat = Lx)."""
+    Ls, ns = cell_lengths(L), box_edges(nr)
+    b = [2.0 * math.pi / x for x in Ls]
+    nmax = [int(math.sqrt(ecutwfc) / bi) + 1 for bi in b]
+    i, j, k = np.meshgrid(np.arange(-nmax[0], nmax[0] + 1), np.arange(-nmax[1], nmax[1] + 1),
+                          np.arange(-nmax[2], nmax[2] + 1), indexing="ij")
     i, j, k = i.ravel(), j.ravel(), k.ravel()
-    n2 = i * i + j * j + k * k
-    keep = (n2 * tpiba2 <= ecutwfc) & ((i > 0) | ((i == 0) & (j > 0)) | ((i == 0) & (j == 0) & (k >= 0)))
+    if Ls[0] == Ls[1] == Ls[2]:        # cubic: integer |m|^2 as the sort key, exact ties
+        key = i * i + j * j + k * k
+        g2 = key * b[0] ** 2
+    else:
+        g2 = (i * b[0]) ** 2 + (j * b[1]) ** 2 + (k * b[2]) ** 2
+        key = g2
+    keep = (g2 <= ecutwfc) & ((i > 0) | ((i == 0) & (j > 0)) | ((i == 0) & (j == 0) & (k >= 0)))
     mill = np.stack([i[keep], j[keep], k[keep]], axis=1).astype(np.int32)
-    n2 = n2[keep]
-    order = np.lexsort((mill[:, 2], mill[:, 1], mill[:, 0], n2))
+    order = np.lexsort((mill[:, 2], mill[:, 1], mill[:, 0], key[keep]))
     mill = mill[order]
-    if np.abs(mill).max() * 2 >= nr:
-        raise ValueError(f"FFT box {nr} too small for cutoff {ecutwfc} Ry in cell {L}")
-    return mill, tpiba2
+    for d in range(3):
+        if np.abs(mill[:, d]).max() * 2 >= ns[d]:
+            raise ValueError(f"FFT box {ns} too small for cutoff {ecutwfc} Ry in cell {Ls}")
+    return mill, b[0] ** 2
 
 
-def box_index(mill: np.ndarray, nr: int) -> np.ndarray:
-    """0-based linear index (x fastest) of Miller triples in an nr^3 box."""
-    m = np.mod(mill.astype(np.int64), nr)
-    return m[:, 0] + nr * (m[:, 1] + nr * m[:, 2])
+def g2_of(mill: np.ndarray, L) -> np.ndarray:
+    """|G|^2 (bohr^-2 = Ry) of Miller triples in the orthorhombic cell L."""
+    b = np.array([2.0 * math.pi / x for x in cell_lengths(L)])
+    return ((mill.astype(np.float64) * b[None, :]) ** 2).sum(1)
+
+
+def box_index(mill: np.ndarray, nr) -> np.ndarray:
+    """0-based linear index (x fastest) of Miller triples in the box nr."""
+    n1, n2, n3 = box_edges(nr)
+    m = mill.astype(np.int64)
+    return np.mod(m[:, 0], n1) + n1 * (np.mod(m[:, 1], n2) + n2 * np.mod(m[:, 2], n3))
 
 
 def _local_potential(L, nr, tau, Z, sigma):
-    x = np.arange(nr) * (L / nr)
-    v = np.zeros((nr, nr, nr))          # [k][j][i] = (z, y, x)
+    (Lx, Ly, Lz), (n1, n2, n3) = cell_lengths(L), box_edges(nr)
+    x = np.arange(n1) * (Lx / n1)
+    y = np.arange(n2) * (Ly / n2)
+    z = np.arange(n3) * (Lz / n3)
+    v = np.zeros((n3, n2, n1))          # [k][j][i] = (z, y, x)
     for t in tau:
-        dx = x - t[0]; dx -= L * np.round(dx / L)
-        dy = x - t[1]; dy -= L * np.round(dy / L)
-        dz = x - t[2]; dz -= L * np.round(dz / L)
+        dx = x - t[0]; dx -= Lx * np.round(dx / Lx)
+        dy = y - t[1]; dy -= Ly * np.round(dy / Ly)
+        dz = z - t[2]; dz -= Lz * np.round(dz / Lz)
         d2 = dz[:, None, None] ** 2 + dy[None, :, None] ** 2 + dx[None, None, :] ** 2
         v += -Z * np.exp(-d2 / (2.0 * sigma * sigma))
     return v.ravel()
 
 
 def _kb_projectors(mill, L, tau, proj, sigma_p):
-    tpiba = 2.0 * math.pi / L
-    G = mill.astype(np.float64) * tpiba                    # [npw, 3] bohr^-1
+    b = np.array([2.0 * math.pi / x for x in cell_lengths(L)])
+    G = mill.astype(np.float64) * b[None, :]               # [npw, 3] bohr^-1
     g2 = (G * G).sum(1)
     radial = np.exp(-0.5 * sigma_p * sigma_p * g2)
     cols = []
@@ -162,15 +197,16 @@ def _dense_gamma_hamiltonian(sysd, device="cpu"):
     """Real symmetric Hamiltonian on the orthonormal Gamma basis
     {e_0, (e_G + e_-G)/sqrt2, i(e_G - e_-G)/sqrt2}."""
     import torch
-    nr = sysd["nr"]
+    n1, n2, n3 = box_edges(sysd["nr"])
     mill = torch.as_tensor(sysd["mill"].astype(np.int64), device=device)
-    vt = np.fft.fftn(sysd["vrs"].reshape(nr, nr, nr)) / nr ** 3     # V(G) on the box
+    vt = np.fft.fftn(sysd["vrs"].reshape(n3, n2, n1)) / (n1 * n2 * n3)   # V(G) on the box
     vt = torch.as_tensor(vt.ravel(), device=device)
     npw = mill.shape[0]
+    nn = torch.as_tensor([n1, n2, n3], device=device)
 
     def vidx(sign):
-        d = (mill[:, None, :] + sign * mill[None, :, :]) % nr
-        return d[..., 0] + nr * (d[..., 1] + nr * d[..., 2])
+        d = (mill[:, None, :] + sign * mill[None, :, :]) % nn
+        return d[..., 0] + n1 * (d[..., 1] + n2 * d[..., 2])
 
     B = torch.as_tensor(sysd["vkb"], device=device)
     D = torch.as_tensor(sysd["deeq"], device=device).to(B.dtype)
@@ -235,14 +271,15 @@ class _GammaH:
         import torch
         nr = sysd["nr"]
         mill = sysd["mill"]
-        self.nr = nr
+        self.nrs = box_edges(nr)
+        n1, n2, n3 = self.nrs
         self.nl = torch.as_tensor(box_index(mill, nr), device=device)
         self.nlm = torch.as_tensor(box_index(-mill, nr), device=device)
-        self.v = torch.as_tensor(sysd["vrs"].reshape(nr, nr, nr), device=device)
+        self.v = torch.as_tensor(sysd["vrs"].reshape(n3, n2, n1), device=device)
         self.g2 = torch.as_tensor(sysd["g2kin"], device=device)
         self.B = torch.as_tensor(sysd["vkb"], device=device)
         self.D = torch.as_tensor(sysd["deeq"], device=device).to(self.B.dtype)
-        self.chunk = max(1, int(2e9 // (16 * nr ** 3)))   # vectors per FFT batch (about 2 GB of boxes)
+        self.chunk = max(1, int(2e9 // (16 * n1 * n2 * n3)))   # vectors per FFT batch (about 2 GB of boxes)
 
     def dot(self, a, b):
         """Gamma Gram matrix <a_i|b_j> (real)."""
@@ -251,15 +288,15 @@ class _GammaH:
 
     def __call__(self, psi):
         import torch
-        nr = self.nr
+        n1, n2, n3 = self.nrs
         out = torch.empty_like(psi)
         for c0 in range(0, psi.shape[1], self.chunk):
             p = psi[:, c0:c0 + self.chunk]
             k = p.shape[1]
-            box = torch.zeros((k, nr ** 3), dtype=torch.complex128, device=psi.device)
+            box = torch.zeros((k, n1 * n2 * n3), dtype=torch.complex128, device=psi.device)
             box[:, self.nlm] = p.T.conj()
             box[:, self.nl] = p.T                       # G = 0: the +G store wins (psi(0) is real)
-            r = torch.fft.ifftn(box.view(k, nr, nr, nr), dim=(1, 2, 3), norm="forward") * self.v
+            r = torch.fft.ifftn(box.view(k, n3, n2, n1), dim=(1, 2, 3), norm="forward") * self.v
             g = torch.fft.fftn(r, dim=(1, 2, 3), norm="forward").reshape(k, -1)
             out[:, c0:c0 + k] = g[:, self.nl].T
         out += self.g2[:, None] * psi
@@ -327,9 +364,13 @@ def build_system(spec: SystemSpec | str, device: Optional[str] = None) -> GammaS
         device = "cpu"
     rng = np.random.default_rng(spec.seed)
     L, nr = spec.L, spec.nr
+    Ls = cell_lengths(L)
     mill, tpiba2 = gamma_half_sphere(L, spec.ecutwfc, nr)
-    tau = rng.uniform(0.0, L, size=(spec.natoms, 3))
-    g2kin = (mill.astype(np.float64) ** 2).sum(1) * tpiba2
+    tau = rng.uniform(0.0, 1.0, size=(spec.natoms, 3)) * np.array(Ls)[None, :]
+    if Ls[0] == Ls[1] == Ls[2]:
+        g2kin = (mill.astype(np.float64) ** 2).sum(1) * tpiba2
+    else:
+        g2kin = g2_of(mill, L)
     nl = box_index(mill, nr)
     nlm = box_index(-mill, nr)
     vrs = _local_potential(L, nr, tau, spec.Z, spec.sigma)
@@ -346,11 +387,14 @@ def build_system(spec: SystemSpec | str, device: Optional[str] = None) -> GammaS
     emin = et.min()
     emax = et[: spec.nbnd_occ].max()
     alpha_pv = max(2.0 * (emax - emin), 0.01)          # Tools/get_alpha_pv.f90:59-63
+    occ = np.ones(spec.nbnd_occ)
+    if spec.frac_occ:
+        occ[spec.nbnd_occ - len(spec.frac_occ):] = np.asarray(spec.frac_occ, dtype=np.float64)
     return GammaSystem(
-        spec=spec, omega=L ** 3, tpiba2=tpiba2, nr=nr, mill=mill, g2kin=g2kin,
+        spec=spec, omega=Ls[0] * Ls[1] * Ls[2], tpiba2=tpiba2, nr=nr, mill=mill, g2kin=g2kin,
         nl=nl, nlm=nlm, vrs=vrs, vkb=vkb, deeq=deeq,
         evc=np.ascontiguousarray(evc[:, : spec.nbnd_occ]), et=et,
-        occupation=np.ones(spec.nbnd_occ), sqvc=sqvc, alpha_pv=alpha_pv, tau=tau)
+        occupation=occ, sqvc=sqvc, alpha_pv=alpha_pv, tau=tau)
 
 
 def perturbations(sysm: GammaSystem, m: int, seed: int = 1234) -> np.ndarray:
@@ -371,7 +415,7 @@ def randomized_basis(sysm: GammaSystem, m: int, seed: int = 4321) -> np.ndarray:
     rng = np.random.default_rng(seed)
     rr = rng.random((sysm.npw, m))
     arg = 2.0 * math.pi * rng.random((sysm.npw, m))
-    g2 = (sysm.mill.astype(np.float64) ** 2).sum(1)
+    g2 = sysm.g2kin / sysm.tpiba2
     a = rr * np.exp(1j * arg) / (g2 + 1.0)[:, None]
     a[0] = 0.0
     return np.asfortranarray(a)
