@@ -59,7 +59,7 @@ def _sys_struct(tiny, **over):
     keep = {}
     s = L.WbSystem()
     s.npw = s.npwx = tiny.npw
-    s.nr1 = s.nr2 = s.nr3 = tiny.nr
+    s.nr1, s.nr2, s.nr3 = tiny.nrs
     s.nbnd_occ = tiny.nbnd_occ
     s.nkb = tiny.nkb
     s.n_dfpt_maxiter = 250
@@ -78,7 +78,7 @@ def _sys_struct(tiny, **over):
 
 @pytest.mark.parametrize("over,code,msg", [
     (dict(npw=0), L.WB_ERR_ARG, "npw"),
-    (dict(nr3=20), L.WB_ERR_UNSUPPORTED, "cubic"),
+    (dict(nr3=22), L.WB_ERR_UNSUPPORTED, "prime factor above 7"),
     (dict(nr1=17, nr2=17, nr3=17), L.WB_ERR_UNSUPPORTED, "FFT edge"),
     (dict(gstart=1), L.WB_ERR_UNSUPPORTED, "gstart"),
     (dict(nbnd_occ=0), L.WB_ERR_ARG, "nbnd_occ"),

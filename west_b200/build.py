@@ -21,7 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libwestb200.so")
-SOURCES = ["wb_api.cu", "wb_fft_kernels.cu", "wb_la.cu", "wb_davidson.cu", "wb_pdep.cu", "wb_umma.cu"]
+SOURCES = ["wb_api.cu", "wb_fft_kernels.cu", "wb_fft_rt.cu", "wb_la.cu", "wb_davidson.cu", "wb_pdep.cu", "wb_umma.cu"]
 HEADERS = ["wb_common.cuh", "wb_fft.cuh", "wb_internal.h", "wb_ctx.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -95,21 +95,27 @@ std::vector<std::pair<int, int>> stick_pair_order(int N, int prune, const std::m
   return order;
 }
 
+template <class T>
+int upload(const T* h, size_t n, DBuf& d);
+
 int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
-  const int N = s->nr1, npw = s->npw;
+  const int n1 = s->nr1, n2 = s->nr2, n3 = s->nr3, npw = s->npw;
+  const long nnr = (long)n1 * n2 * n3;
+  const bool rt = c->rt != 0;
+  const int N = rt ? 0 : n1;  // the compiled (cubic) edge
   struct GInfo { int mx, my, mz, ref; };
   std::vector<GInfo> gi(npw);
-  auto mill = [N](int v) { return v < (N + 1) / 2 ? v : v - N; };
+  auto mill = [](int v, int n) { return v < (n + 1) / 2 ? v : v - n; };
   std::map<long, long> seen;
   for (int i = 0; i < npw; ++i) {
     const long b = (long)s->nl[i] - 1;
-    if (b < 0 || b >= (long)N * N * N) return fail(WB_ERR_ARG, "nl out of range at G " + std::to_string(i + 1));
-    const int x = (int)(b % N), y = (int)((b / N) % N), z = (int)(b / ((long)N * N));
-    gi[i] = {mill(x), mill(y), mill(z), i};
-    if (2 * std::abs(gi[i].mx) >= N || 2 * std::abs(gi[i].my) >= N || 2 * std::abs(gi[i].mz) >= N)
+    if (b < 0 || b >= nnr) return fail(WB_ERR_ARG, "nl out of range at G " + std::to_string(i + 1));
+    const int x = (int)(b % n1), y = (int)((b / n1) % n2), z = (int)(b / ((long)n1 * n2));
+    gi[i] = {mill(x, n1), mill(y, n2), mill(z, n3), i};
+    if (2 * std::abs(gi[i].mx) >= n1 || 2 * std::abs(gi[i].my) >= n2 || 2 * std::abs(gi[i].mz) >= n3)
       return fail(WB_ERR_ARG, "G sphere reaches the box edge (aliasing) at G " + std::to_string(i + 1));
     const long bm = (long)s->nlm[i] - 1;
-    const long want = ((-gi[i].mx + N) % N) + (long)N * (((-gi[i].my + N) % N) + (long)N * ((-gi[i].mz + N) % N));
+    const long want = ((-gi[i].mx + n1) % n1) + (long)n1 * (((-gi[i].my + n2) % n2) + (long)n2 * ((-gi[i].mz + n3) % n3));
     if (bm != want) return fail(WB_ERR_ARG, "nlm is not the box index of -G at G " + std::to_string(i + 1));
     if (seen.count(b) || (i > 0 && seen.count(bm)))
       return fail(WB_ERR_ARG, "G and -G both stored (not a Gamma half sphere) at G " + std::to_string(i + 1));
@@ -123,7 +129,6 @@ int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
   };
   std::map<std::pair<int, int>, int> pairs;
   pairs[{0, 0}] = 0;
-  std::vector<std::pair<int, int>> keys;
   for (auto& g : gi) {
     int cx, cy, sd;
     canon(g.mx, g.my, cx, cy, sd);
@@ -133,8 +138,16 @@ int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
   const int nsp = (int)pairs.size();
   int mmax = 0;
   for (auto& g : gi) mmax = std::max({mmax, std::abs(g.mx), std::abs(g.my), std::abs(g.mz)});
-  const int prune = (4 * mmax < N && N % 4 == 0) ? 1 : 0;
-  std::vector<std::pair<int, int>> pair_xy = stick_pair_order(N, prune, pairs);
+  const int prune = (!rt && 4 * mmax < N && N % 4 == 0) ? 1 : 0;
+  std::vector<std::pair<int, int>> pair_xy;
+  if (!rt) {
+    pair_xy = stick_pair_order(N, prune, pairs);
+  } else {  // the runtime-size path: pairs in (y, x) order
+    for (auto& kv : pairs) pair_xy.push_back(kv.first);
+    std::stable_sort(pair_xy.begin() + 1, pair_xy.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+      return a.second != b.second ? a.second < b.second : a.first < b.first;
+    });
+  }
   for (int p = 1; p < nsp; ++p) pairs[pair_xy[p]] = p;
   std::vector<int> gq(npw), gside(npw);
   int xmax = 0;
@@ -164,10 +177,26 @@ int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
   for (int p = 0; p < nsp; ++p) spg[p + 1] += spg[p];
   const int nst = 2 * nsp;
   std::vector<int> stpos(nst, -1);
-  for (int p = 0; p < nsp; ++p) {
-    const int x = pair_xy[p].first, y = pair_xy[p].second;
-    stpos[2 * p] = ((y + N) % N) * N + ((x + N) % N);
-    if (p > 0) stpos[2 * p + 1] = ((-y + N) % N) * N + ((-x + N) % N);
+  if (!rt) {
+    for (int p = 0; p < nsp; ++p) {
+      const int x = pair_xy[p].first, y = pair_xy[p].second;
+      stpos[2 * p] = ((y + N) % N) * N + ((x + N) % N);
+      if (p > 0) stpos[2 * p + 1] = ((-y + N) % N) * N + ((-x + N) % N);
+    }
+  } else {
+    // active columns: every x of a stick or its mirror, x in [-xmax, xmax]
+    const int ncols = 2 * xmax + 1, cs = n2 | 1;
+    std::vector<int> colx(ncols);
+    for (int cidx = 0; cidx < ncols; ++cidx) colx[cidx] = (cidx - xmax + n1) % n1;
+    auto col_of = [&](int x) { return x + xmax; };
+    for (int p = 0; p < nsp; ++p) {
+      const int x = pair_xy[p].first, y = pair_xy[p].second;
+      stpos[2 * p] = col_of(x) * cs + (y + n2) % n2;
+      if (p > 0) stpos[2 * p + 1] = col_of(-x) * cs + (-y + n2) % n2;
+    }
+    c->geo.ncols = ncols;
+    c->geo.cs = cs;
+    if (upload(colx.data(), colx.size(), c->rt_colx)) return fail(WB_ERR_NOMEM, "device allocation failed");
   }
   // device copies
   if (c->gqz.ensure(sizeof(int2) * npw) || c->spg.ensure(sizeof(int) * (nsp + 1)) ||
@@ -190,6 +219,10 @@ int build_tables(wb_ctx* c, const wb_system* s, std::vector<int>& perm) {
     // are the active set (they are all zero-filled and transformed)
     c->st.xhi = N / 4 - 1;
     c->st.ncols = N / 2;
+  }
+  if (rt) {
+    c->geo.colx = c->rt_colx.as<int>();
+    c->geo.spos = c->stpos.as<int>();
   }
   return WB_OK;
 }
@@ -253,7 +286,7 @@ void pair_items(std::vector<int2>& it, int base, int n) {
 
 size_t per_pert_bytes(const wb_ctx* c) {
   const size_t vec = sizeof(double2) * (size_t)c->npw * c->nocc;
-  const size_t stk = sizeof(double2) * (size_t)c->nr * c->st.nst;
+  const size_t stk = sizeof(double2) * (size_t)c->nz * c->st.nst;
   const size_t mixed = c->precision == WB_PRECISION_MIXED ? 2 * vec + stk * (size_t)c->npv / 2 : 0;
   return mixed + 4 * vec                           // B, X, G, T (+ FP32 g, P, T, d and sticks)
          + stk * (size_t)c->npv                    // sticks (RHS / CG pairs / drho items)
@@ -278,7 +311,7 @@ int ensure_workspace(wb_ctx* c, int mb, long ld_in, long ld_out) {
   c->cap_nsys = (int)nsys;
   mb = (int)(nsys / c->nocc);
   const size_t vec = sizeof(double2) * (size_t)c->npw * nsys;
-  const size_t stk1 = sizeof(double2) * (size_t)c->nr * c->st.nst;
+  const size_t stk1 = sizeof(double2) * (size_t)c->nz * c->st.nst;
   const size_t mp = (mb + 1) / 2;
   const size_t nitems = std::max<size_t>({(nsys + 1) / 2, (size_t)mb * c->npv, mp, (size_t)c->npv});
   const int nsplit = gemm_tn_splits(c->nproj, (int)nsys, 2 * c->npw, 4);  // the tuner's largest target
@@ -478,17 +511,29 @@ int ensure_fp32(wb_ctx* c, int nsys, int nitems) {
   if (!c->have32) {
     if (c->W32.ensure(sizeof(float) * (size_t)K * c->nproj + 16) || c->D32.ensure(sizeof(float) * std::max(1, c->nkb * c->nkb)) ||
         c->g2kin32.ensure(sizeof(float) * c->npw) || c->vs32.ensure(sizeof(float) * (size_t)c->nnr) ||
-        c->tw32.ensure(sizeof(float2) * c->nr))
+        c->tw32.ensure(sizeof(float2) * std::max(c->nr, 1)))
       return fail(WB_ERR_NOMEM, "device allocation of FP32 constants failed");
+    if (c->rt) {
+      if (c->twx32.ensure(sizeof(float2) * c->geo.nx) || c->twy32.ensure(sizeof(float2) * c->geo.ny) ||
+          c->twz32.ensure(sizeof(float2) * c->geo.nz))
+        return fail(WB_ERR_NOMEM, "device allocation of FP32 constants failed");
+      to_float(c->twx.as<double>(), c->twx32.as<float>(), 2L * c->geo.nx, c->stream);
+      to_float(c->twy.as<double>(), c->twy32.as<float>(), 2L * c->geo.ny, c->stream);
+      to_float(c->twz.as<double>(), c->twz32.as<float>(), 2L * c->geo.nz, c->stream);
+      c->geo.twx32 = c->twx32.as<float2>();
+      c->geo.twy32 = c->twy32.as<float2>();
+      c->geo.twz32 = c->twz32.as<float2>();
+    }
     to_float(c->W.as<double>(), c->W32.as<float>(), (long)K * c->nproj, c->stream);
     if (c->nkb) to_float(c->D.as<double>(), c->D32.as<float>(), (long)c->nkb * c->nkb, c->stream);
     to_float(c->g2kin.as<double>(), c->g2kin32.as<float>(), c->npw, c->stream);
     to_float(c->vs.as<double>(), c->vs32.as<float>(), c->nnr, c->stream);
-    to_float(c->tw.as<double>(), c->tw32.as<float>(), 2L * c->nr, c->stream);
+    if (!c->rt) to_float(c->tw.as<double>(), c->tw32.as<float>(), 2L * c->nr, c->stream);
     c->fa32.n = c->nr;
     c->fa32.st = c->st;
     c->fa32.tw = c->tw32.as<float2>();
     c->fa32.stream = c->stream;
+    c->fa32.rt = c->rt ? &c->geo : nullptr;
     // the projector and Pv GEMMs on tensor cores: W split once into bf16 hi/lo tiles
     const int Msub = c->kinetic_only ? c->nocc : c->nproj;
     const double* Wsub = c->W.as<double>() + (c->kinetic_only ? (size_t)c->nkb * K : 0);
@@ -511,7 +556,7 @@ int ensure_fp32(wb_ctx* c, int nsys, int nitems) {
   if (c->umma) part_floats = std::max(part_floats, umma_part_floats(c->umma_M, nsys, K));
   bool bad = false;
   bad |= c->g32.ensure(vec) || c->P32.ensure(vec) || c->T32.ensure(vec) || c->d32.ensure(vec);
-  bad |= c->sticks32.ensure(sizeof(float2) * (size_t)c->nr * c->st.nst * nitems) != 0;
+  bad |= c->sticks32.ensure(sizeof(float2) * (size_t)c->nz * c->st.nst * nitems) != 0;
   bad |= c->part32.ensure(sizeof(float) * part_floats) != 0;
   bad |= c->C32.ensure(sizeof(float) * (size_t)nsys * c->nproj) != 0;
   bad |= c->ecol32.ensure(sizeof(float) * nsys) || c->rho0.ensure(sizeof(double) * nsys) ||
@@ -815,7 +860,7 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
 int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, long ld_out, double tr2,
               int* unconv_host) {
   cudaStream_t s = c->stream;
-  const int npw = c->npw, nocc = c->nocc, npv = c->npv, N = c->nr;
+  const int npw = c->npw, nocc = c->nocc, npv = c->npv;
   const int nsys = mb * nocc;
   const long ld = npw;
   const int K = 2 * npw;
@@ -947,7 +992,7 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
   {
     Stage g(c, WB_STAGE_DRHO, 3, (long long)mb * npv + mp);
     fft_zinv(c->fa, X, ld, c->items_pk.as<int2>(), mb * npv, stk);
-    const double scale = 2.0 * c->wk / c->omega / ((double)N * N * N);
+    const double scale = 2.0 * c->wk / c->omega / (double)c->nnr;
     fft_plane_drho(c->fa, stk, c->evcr.as<double2>(), c->occ.as<double>(), nocc, mb, c->acc.as<double2>(), scale,
                    c->sticks2.as<double2>());
     fft_zfwd_dng(c->fa, c->sticks2.as<double2>(), c->items_pp.as<int2>(), mp, dng, ld_out, c->perm.as<int>(),
@@ -1028,8 +1073,14 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
   if (!out || !s) return fail(WB_ERR_ARG, "null argument");
   *out = nullptr;
   if (s->npw <= 0 || s->npwx < s->npw) return fail(WB_ERR_ARG, "need 0 < npw <= npwx");
-  if (s->nr1 != s->nr2 || s->nr1 != s->nr3) return fail(WB_ERR_UNSUPPORTED, "only cubic FFT boxes are provided");
-  if (!fft_supported(s->nr1)) return fail(WB_ERR_UNSUPPORTED, "FFT edge " + std::to_string(s->nr1) + " not provided");
+  if (s->nr1 < 2 || s->nr2 < 2 || s->nr3 < 2) return fail(WB_ERR_ARG, "FFT box edges must be >= 2");
+  // compiled kernels for the listed cubic edges; every other box runs the
+  // runtime-size transforms, which need 2, 3, 5, 7-smooth edges
+  const bool compiled = s->nr1 == s->nr2 && s->nr1 == s->nr3 && fft_supported(s->nr1);
+  if (!compiled)
+    for (int e : {s->nr1, s->nr2, s->nr3})
+      if (rt_plan(e).ns == 0)
+        return fail(WB_ERR_UNSUPPORTED, "FFT edge " + std::to_string(e) + " has a prime factor above 7");
   if (s->nbnd_occ <= 0 || s->nkb < 0) return fail(WB_ERR_ARG, "bad nbnd_occ or nkb");
   if (s->gstart != 2) return fail(WB_ERR_UNSUPPORTED, "gstart must be 2 (G=0 on this process)");
   if (s->n_dfpt_maxiter < 0) return fail(WB_ERR_ARG, "n_dfpt_maxiter < 0");
@@ -1056,8 +1107,18 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
       cudaEventCreate(&c->tev0) != cudaSuccess || cudaEventCreate(&c->tev1) != cudaSuccess)
     return bail(fail(WB_ERR_CUDA, "stream/event creation failed"));
   c->npw = s->npw;
-  c->nr = s->nr1;
+  c->rt = compiled ? 0 : 1;
+  c->nr = compiled ? s->nr1 : 0;
+  c->nz = s->nr3;
   c->nnr = s->nr1 * s->nr2 * s->nr3;
+  if (c->rt) {
+    c->geo.nx = s->nr1;
+    c->geo.ny = s->nr2;
+    c->geo.nz = s->nr3;
+    c->geo.px = rt_plan(s->nr1);
+    c->geo.py = rt_plan(s->nr2);
+    c->geo.pz = rt_plan(s->nr3);
+  }
   c->nocc = s->nbnd_occ;
   c->nkb = s->nkb;
   c->nproj = s->nkb + s->nbnd_occ;
@@ -1081,17 +1142,42 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
   int rc = build_tables(c, s, perm);
   if (rc) return bail(rc);
   const int N = c->nr, npw = c->npw;
-  // twiddles exp(+2 pi i j / N), accurate host values
-  std::vector<double2> tw(N);
-  for (int j = 0; j < N; ++j) {
-    const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)j / (long double)N;
-    tw[j] = make_double2((double)cosl(a), (double)sinl(a));
-  }
+  // twiddles exp(+2 pi i j / n), accurate host values
+  auto twiddles = [](int n) {
+    std::vector<double2> t(n);
+    for (int j = 0; j < n; ++j) {
+      const long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)j / (long double)n;
+      t[j] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    return t;
+  };
   std::vector<double> g2(npw), sq(npw);
   for (int i = 0; i < npw; ++i) { g2[i] = s->g2kin[perm[i]]; sq[i] = s->sqvc[perm[i]]; }
   std::vector<double> vsc(c->nnr);
-  for (int i = 0; i < c->nnr; ++i) vsc[i] = s->vrs[i] / (double)c->nnr;
-  if ((rc = upload(tw.data(), N, c->tw)) || (rc = upload(g2.data(), npw, c->g2kin)) ||
+  if (!c->rt) {
+    for (int i = 0; i < c->nnr; ++i) vsc[i] = s->vrs[i] / (double)c->nnr;
+    if ((rc = upload(twiddles(N).data(), N, c->tw))) return bail(rc);
+  } else {
+    // V(r) / N at the digit-reversed positions the runtime transforms leave real space in
+    const int nx = s->nr1, ny = s->nr2, nz = s->nr3;
+    std::vector<int> rx(nx), ry(ny), rz(nz);
+    for (int p = 0; p < nx; ++p) rx[p] = rt_digit_reverse(c->geo.px, p);
+    for (int p = 0; p < ny; ++p) ry[p] = rt_digit_reverse(c->geo.py, p);
+    for (int p = 0; p < nz; ++p) rz[p] = rt_digit_reverse(c->geo.pz, p);
+    for (int pz = 0; pz < nz; ++pz)
+      for (int py = 0; py < ny; ++py)
+        for (int px = 0; px < nx; ++px)
+          vsc[((size_t)pz * ny + py) * nx + px] = s->vrs[((size_t)rz[pz] * ny + ry[py]) * nx + rx[px]] / (double)c->nnr;
+    if ((rc = upload(twiddles(nx).data(), nx, c->twx)) || (rc = upload(twiddles(ny).data(), ny, c->twy)) ||
+        (rc = upload(twiddles(nz).data(), nz, c->twz)))
+      return bail(rc);
+    c->geo.twx = c->twx.as<double2>();
+    c->geo.twy = c->twy.as<double2>();
+    c->geo.twz = c->twz.as<double2>();
+    if (rt_plane_smem(c->geo, 16, nullptr) == 0)
+      return bail(fail(WB_ERR_UNSUPPORTED, "the x-y plane of this box does not fit in shared memory"));
+  }
+  if ((rc = upload(g2.data(), npw, c->g2kin)) ||
       (rc = upload(sq.data(), npw, c->sqvc)) || (rc = upload(vsc.data(), c->nnr, c->vs)) ||
       (rc = upload(s->et, c->nocc, c->et)) || (rc = upload(s->occupation, c->nocc, c->occ)))
     return bail(rc);
@@ -1108,15 +1194,17 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
     if (c->nkb) std::memcpy(dd.data(), s->deeq, sizeof(double) * c->nkb * c->nkb);
     if ((rc = upload(dd.data(), dd.size(), c->D))) return bail(rc);
   }
-  fft_setup(N);
+  if (c->rt) rt_setup(c->geo);
+  else fft_setup(N);
   c->fa.n = N;
   c->fa.st = c->st;
   c->fa.tw = c->tw.as<double2>();
   c->fa.stream = c->stream;
+  c->fa.rt = c->rt ? &c->geo : nullptr;
   // eprec (set_eprec.f90) and psi_v(r) for all occupied bands, in pairs
   if (c->eprec.ensure(sizeof(double) * c->nocc) || c->evcr.ensure(sizeof(double2) * (size_t)c->nnr * c->npv) ||
       c->iota_items.ensure(sizeof(int2) * c->npv) ||
-      c->sticks.ensure(sizeof(double2) * (size_t)N * c->st.nst * c->npv))
+      c->sticks.ensure(sizeof(double2) * (size_t)c->nz * c->st.nst * c->npv))
     return bail(fail(WB_ERR_NOMEM, "device allocation failed"));
   set_eprec(c->evc.as<double2>(), c->g2kin.as<double>(), npw, c->nocc, c->eprec.as<double>(), c->stream);
   if (c->iprec.ensure(sizeof(double) * (size_t)npw * c->nocc)) return bail(fail(WB_ERR_NOMEM, "device allocation failed"));
@@ -1142,7 +1230,7 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->D, &c->eprec, &c->et, &c->occ, &c->evcr, &c->iprec, &c->dvg_in, &c->dng_out, &c->aux, &c->dvbox, &c->B,
                   &c->X, &c->G, &c->T, &c->sticks, &c->sticks2, &c->acc, &c->part, &c->C, &c->rho, &c->conv,
                   &c->act, &c->items, &c->nact, &c->ecol, &c->epcol, &c->unconv, &c->items_pp, &c->items_pk,
-                  &c->iota_items, &c->fcoef, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
+                  &c->iota_items, &c->fcoef, &c->rt_colx, &c->twx, &c->twy, &c->twz, &c->twx32, &c->twy32, &c->twz32, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
                   &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots, &c->dav_bj, &c->W32, &c->D32, &c->g2kin32,
                   &c->vs32, &c->tw32, &c->g32, &c->P32, &c->T32, &c->d32, &c->sticks32, &c->part32, &c->C32,
                   &c->ecol32, &c->rho0, &c->rho_in, &c->conv_in, &c->act_in, &c->items_in, &c->nact_in,
@@ -1316,7 +1404,7 @@ struct NoallocWs {
 void noalloc_layout(const wb_ctx* c, int mb, Carve& cv, NoallocWs& w) {
   const size_t nsys = (size_t)mb * c->nocc;
   const size_t npw = c->npw;
-  const size_t stk1 = (size_t)c->nr * c->st.nst;
+  const size_t stk1 = (size_t)c->nz * c->st.nst;
   const size_t mp = ((size_t)mb + 1) / 2;
   const size_t nitems = std::max<size_t>({(nsys + 1) / 2, (size_t)mb * c->npv, mp});
   w.nsplit = gemm_tn_splits(c->nproj, (int)nsys, 2 * c->npw);
@@ -1381,7 +1469,7 @@ void noalloc_apply_A(wb_ctx* c, const NoallocWs& w, const double2* Xv, double2* 
 int noalloc_run(wb_ctx* c, const NoallocWs& w, int mb, const double2* dvg, long ld_in, double2* dng, long ld_out,
                 double tr2, int* unconv_host) {
   cudaStream_t s = c->stream;
-  const int npw = c->npw, nocc = c->nocc, npv = c->npv, N = c->nr;
+  const int npw = c->npw, nocc = c->nocc, npv = c->npv;
   const int nsys = mb * nocc;
   const long ld = npw;
   const int K = 2 * npw;
@@ -1428,7 +1516,7 @@ int noalloc_run(wb_ctx* c, const NoallocWs& w, int mb, const double2* dvg, long 
   }
   c->stats.cg_iterations = std::max(c->stats.cg_iterations, iters);
   fft_zinv(c->fa, w.X, ld, w.items_pk, mb * npv, w.sticks);
-  const double scale = 2.0 * c->wk / c->omega / ((double)N * N * N);
+  const double scale = 2.0 * c->wk / c->omega / (double)c->nnr;
   fft_plane_drho(c->fa, w.sticks, c->evcr.as<double2>(), c->occ.as<double>(), nocc, mb, w.acc, scale, w.sticks2);
   fft_zfwd_dng(c->fa, w.sticks2, w.items_pp, mp, dng, ld_out, c->perm.as<int>(), c->sqvc.as<double>());
   if (unconv_host) WB_CU(cudaMemcpyAsync(unconv_host, w.unconv, sizeof(int) * mb, cudaMemcpyDeviceToHost, s));

@@ -55,6 +55,10 @@ struct wb_ctx {
   int npw = 0, nr = 0, nnr = 0, nocc = 0, nkb = 0, nproj = 0, npv = 0;
   int maxiter = 0, kinetic_only = 0, precision = WB_PRECISION_FP64, batch_cap = 0;
   int nfull = 0;             // fully occupied bands (nbnd_occ_full); nocc - nfull fractional ones
+  int nz = 0;                // stick length (box edge along z)
+  int rt = 0;                // 1: runtime-size FFT path (no compiled kernels for this box)
+  wb::RtGeo geo{};           // its geometry (radix plans, active columns, twiddle tables)
+  DBuf rt_colx, twx, twy, twz, twx32, twy32, twz32;
   double omega = 0, wk = 0, alpha = 0;
   wb::StickTab st{};
   wb::FftArgs fa{};

@@ -43,6 +43,9 @@ constexpr double kC51 = 0.30901699437494742410;  // cos(2 pi / 5)
 constexpr double kC52 = -0.80901699437494742410; // cos(4 pi / 5)
 constexpr double kS51 = 0.95105651629515357212;  // sin(2 pi / 5)
 constexpr double kS52 = 0.58778525229247312917;  // sin(4 pi / 5)
+// cos and sin of 2 pi k / 7, k = 1, 2, 3 (the radix-7 butterfly of the runtime-size path)
+constexpr double kC71 = 0.62348980185873353053, kC72 = -0.22252093395631440429, kC73 = -0.90096886790241912624;
+constexpr double kS71 = 0.78183148246802980871, kS72 = 0.97492791218182360702, kS73 = 0.43388373911755812048;
 
 template <int R> struct Factor2;  // composite radices R = A * B
 template <> struct Factor2<6> { static constexpr int A = 3, B = 2; };
@@ -107,6 +110,23 @@ WB_DEV void rdft(C* v, const C* twN) {
     v[4] = csub(a1, b1);
     v[2] = cadd(a2, b2);
     v[3] = csub(a2, b2);
+  } else if constexpr (R == 7) {
+    // X_k = x0 + sum_{n=1..3} cos(2 pi n k / 7) t_n + i DIR sin(2 pi n k / 7) d_n,
+    // t_n = x_n + x_{7-n}, d_n = x_n - x_{7-n}; X_{7-k} takes the opposite sine term
+    const T c1 = T(kC71), c2 = T(kC72), c3 = T(kC73), s1 = T(kS71), s2 = T(kS72), s3 = T(kS73);
+    const C x0 = v[0];
+    const C t1 = cadd(v[1], v[6]), t2 = cadd(v[2], v[5]), t3 = cadd(v[3], v[4]);
+    const C d1 = csub(v[1], v[6]), d2 = csub(v[2], v[5]), d3 = csub(v[3], v[4]);
+    auto lin = [](C a, C b, C c, T ka, T kb, T kc) {
+      return mkc<C>(ka * a.x + kb * b.x + kc * c.x, ka * a.y + kb * b.y + kc * c.y);
+    };
+    const C a1 = cadd(x0, lin(t1, t2, t3, c1, c2, c3)), b1 = cmul_i<DIR>(lin(d1, d2, d3, s1, s2, s3));
+    const C a2 = cadd(x0, lin(t1, t2, t3, c2, c3, c1)), b2 = cmul_i<DIR>(lin(d1, d2, d3, s2, -s3, -s1));
+    const C a3 = cadd(x0, lin(t1, t2, t3, c3, c1, c2)), b3 = cmul_i<DIR>(lin(d1, d2, d3, s3, -s1, s2));
+    v[0] = cadd(x0, cadd(t1, cadd(t2, t3)));
+    v[1] = cadd(a1, b1); v[6] = csub(a1, b1);
+    v[2] = cadd(a2, b2); v[5] = csub(a2, b2);
+    v[3] = cadd(a3, b3); v[4] = csub(a3, b3);
   } else {
     constexpr int A = Factor2<R>::A, B = Factor2<R>::B;
     C z[B][A];

@@ -1019,60 +1019,71 @@ void fft_setup(int n) {
   }
 
 void fft_zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks) {
+  if (f.rt) return rt_zinv(f, src, ld, items, nitems, sticks);
 #define X(n) case n: FftN<n>::zinv(f, src, ld, items, nitems, sticks); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_zfwd_store(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dst, long ld) {
+  if (f.rt) return rt_zfwd_store(f, sticks, items, nitems, dst, ld);
 #define X(n) case n: FftN<n>::zfwd(f, sticks, items, nitems, EpiStore{dst, ld}); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_zfwd_hpsi(const FftArgs& f, const double2* sticks, const int2* items, int nitems, const double2* P,
                    double2* T, long ld, const double* g2kin, const double* ecol) {
+  if (f.rt) return rt_zfwd_hpsi(f, sticks, items, nitems, P, T, ld, g2kin, ecol);
 #define X(n) case n: FftN<n>::zfwd(f, sticks, items, nitems, EpiHpsi{P, T, ld, g2kin, ecol}); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_zfwd_dng(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dng, long ld,
                   const int* perm, const double* sqvc) {
+  if (f.rt) return rt_zfwd_dng(f, sticks, items, nitems, dng, ld, perm, sqvc);
 #define X(n) case n: FftN<n>::zfwd(f, sticks, items, nitems, EpiDng{dng, ld, perm, sqvc}); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks) {
+  if (f.rt) return rt_zinv32(f, src, ld, items, nitems, sticks);
 #define X(n) case n: FftN<n>::zinv32(f, src, ld, items, nitems, sticks); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_plane_vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs) {
+  if (f.rt) return rt_plane_vloc32(f, sticks, nitems, vs);
 #define X(n) case n: FftN<n>::vloc32(f, sticks, nitems, vs); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, const float2* P,
                      float2* T, long ld, const float* g2kin, const float* ecol) {
+  if (f.rt) return rt_zfwd_hpsi32(f, sticks, items, nitems, P, T, ld, g2kin, ecol);
 #define X(n) case n: FftN<n>::zfwd_hpsi32(f, sticks, items, nitems, EpiHpsi32{P, T, ld, g2kin, ecol}); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_plane_vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs) {
+  if (f.rt) return rt_plane_vloc(f, sticks, nitems, vs);
 #define X(n) case n: FftN<n>::vloc(f, sticks, nitems, vs); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_plane_inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box) {
+  if (f.rt) return rt_plane_inv_box(f, sticks, nitems, box);
 #define X(n) case n: FftN<n>::inv_box(f, sticks, nitems, box); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_plane_rhs(const FftArgs& f, const double2* evcr, const double2* dvbox, int npv, int mb, double2* sticks) {
+  if (f.rt) return rt_plane_rhs(f, evcr, dvbox, npv, mb, sticks);
 #define X(n) case n: FftN<n>::rhs(f, evcr, dvbox, npv, mb, sticks); break;
   WB_DISPATCH(f.n, )
 #undef X
 }
 void fft_plane_drho(const FftArgs& f, const double2* dsticks, const double2* evcr, const double* occ, int nocc,
                     int mb, double2* acc, double scale, double2* osticks) {
+  if (f.rt) return rt_plane_drho(f, dsticks, evcr, occ, nocc, mb, acc, scale, osticks);
 #define X(n) case n: FftN<n>::drho(f, dsticks, evcr, occ, nocc, mb, acc, scale, osticks); break;
   WB_DISPATCH(f.n, )
 #undef X

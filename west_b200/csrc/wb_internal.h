@@ -18,16 +18,47 @@ struct StickTab {
   int prune;             // 1 if every |Miller index| < N/4 (sphere inside the outer quarters)
 };
 
+// Runtime-size transforms (boxes without a compiled edge: non-cubic boxes and
+// the other 2, 3, 5, 7-smooth edges).  A line of length n is transformed in
+// place by radix stages r[0..ns) (each 2, 3, 4, 5, 7 or 8): the inverse as
+// decimation in frequency (natural input, output at digit-reversed positions),
+// the forward as decimation in time over the same stages in reverse order
+// (digit-reversed input, natural output).  Real-space data therefore sit at
+// digit-reversed positions in every direction; they are only ever multiplied
+// point by point, with V(r) stored in the same permuted layout.
+constexpr int kRtMaxStages = 16;
+struct RtPlan {
+  int n, ns;
+  int r[kRtMaxStages];
+};
+struct RtGeo {
+  int nx, ny, nz;            // box edges, x fastest
+  RtPlan px, py, pz;
+  int ncols;                 // active x columns of a plane (the sticks' x values)
+  int cs;                    // column stride of the shared-memory half plane (>= ny, odd)
+  const int* colx;           // [ncols] box x index of active column c
+  const int* spos;           // [nst] half-plane offset c * cs + (y mod ny) of each stick, -1 = dummy
+  const double2 *twx, *twy, *twz;  // exp(+2 pi i j / n) per direction
+  const float2 *twx32, *twy32, *twz32;
+};
+// radix stages of n (empty if n has a prime factor above 7)
+RtPlan rt_plan(int n);
+// box index in a direction of the value stored at position p by the inverse
+int rt_digit_reverse(const RtPlan& pl, int p);
+// shared memory of the runtime plane kernels for the given geometry and element size
+size_t rt_plane_smem(const RtGeo& g, int elem_bytes, int* rows_per_chunk);
+
 // Launches that take a device count (dcount != nullptr, CUDA-graph replays)
 // size their grid for the host count as a maximum and read the number of
 // systems from *dcount; items are pairs of systems.
 struct FftArgs {
-  int n;                 // box edge
+  int n;                 // box edge (0 when the runtime-size path runs)
   StickTab st;
   const double2* tw;     // [n] exp(+2 pi i j / n)
   cudaStream_t stream;
   const int* dcount = nullptr;
   int unfused = 0;       // 1: the two-pass plane kernel even where the fused one applies
+  const RtGeo* rt = nullptr;  // runtime-size path when set
 };
 
 // FP32 twin of FftArgs for the mixed-precision inner solves.
@@ -38,7 +69,26 @@ struct FftArgs32 {
   cudaStream_t stream;
   const int* dcount = nullptr;
   int unfused = 0;
+  const RtGeo* rt = nullptr;
 };
+
+// runtime-size counterparts of the fft_* entry points below (f.rt set)
+void rt_zinv(const FftArgs& f, const double2* src, long ld, const int2* items, int nitems, double2* sticks);
+void rt_zinv32(const FftArgs32& f, const float2* src, long ld, const int2* items, int nitems, float2* sticks);
+void rt_zfwd_store(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dst, long ld);
+void rt_zfwd_hpsi(const FftArgs& f, const double2* sticks, const int2* items, int nitems, const double2* P,
+                  double2* T, long ld, const double* g2kin, const double* ecol);
+void rt_zfwd_hpsi32(const FftArgs32& f, const float2* sticks, const int2* items, int nitems, const float2* P,
+                    float2* T, long ld, const float* g2kin, const float* ecol);
+void rt_zfwd_dng(const FftArgs& f, const double2* sticks, const int2* items, int nitems, double2* dng, long ld,
+                 const int* perm, const double* sqvc);
+void rt_plane_vloc(const FftArgs& f, double2* sticks, int nitems, const double* vs);
+void rt_plane_vloc32(const FftArgs32& f, float2* sticks, int nitems, const float* vs);
+void rt_plane_inv_box(const FftArgs& f, const double2* sticks, int nitems, double2* box);
+void rt_plane_rhs(const FftArgs& f, const double2* evcr, const double2* dvbox, int npv, int mb, double2* sticks);
+void rt_plane_drho(const FftArgs& f, const double2* dsticks, const double2* evcr, const double* occ, int nocc,
+                   int mb, double2* acc, double scale, double2* osticks);
+void rt_setup(const RtGeo& g);
 
 bool fft_supported(int n);
 // the fused one-pass plane kernel applies to this box and stick table

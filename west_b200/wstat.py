@@ -52,7 +52,7 @@ class ResponseOperator:
         )
         ws = _lib.WbSystem()
         ws.npw = ws.npwx = s.npw
-        ws.nr1 = ws.nr2 = ws.nr3 = s.nr
+        ws.nr1, ws.nr2, ws.nr3 = s.nrs
         ws.nbnd_occ = s.nbnd_occ
         ws.nkb = s.nkb
         ws.n_dfpt_maxiter = n_dfpt_maxiter
