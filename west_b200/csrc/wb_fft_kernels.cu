@@ -315,16 +315,32 @@ WB_DEV void plane_gather(const C* pl, C* __restrict__ sz, const int* __restrict_
   }
 }
 // inverse transforms prune inputs, forward transforms prune outputs
-template <int N, int DIR, bool PR, class C>
+template <int N, int DIR, bool PR, class C, int NT = PNT>
 WB_DEV void plane_fft_cols(C* pl, const StickTab& st, const C* tw) {
   constexpr int P = !PR ? PRUNE_NONE : (DIR > 0 ? PRUNE_IN : PRUNE_OUT);
-  fft_lines<N, DIR, PNT, true, false, P>(pl, OffCols<N>{st.xhi + 1, st.ncols}, Plane<N>::RS, st.ncols, tw);
+  fft_lines<N, DIR, NT, true, false, P>(pl, OffCols<N>{st.xhi + 1, st.ncols}, Plane<N>::RS, st.ncols, tw);
 }
-template <int N, int DIR, bool PR, class C>
+template <int N, int DIR, bool PR, class C, int NT = PNT>
 WB_DEV void plane_fft_rows(C* pl, const C* tw) {
   constexpr int P = !PR ? PRUNE_NONE : (DIR > 0 ? PRUNE_IN : PRUNE_OUT);
-  fft_lines<N, DIR, PNT, false, true, P>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
+  fft_lines<N, DIR, NT, false, true, P>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
 }
+
+// RHS and density kernels.  Up to 72^3 a thread keeps its share of the plane
+// (N^2 / 256 doubles: dv(r) for the RHS, the band sum for the density) in
+// registers across the band loop; from 80^3 on that share does not fit beside
+// the 12- and 10-point transforms, so the RHS re-reads dv(r) and the density
+// accumulates in the CTA's own slice of the global acc buffer, one element per
+// thread throughout (148 such slices, 14 MB at 108^3, stay in L2).  The CTA
+// may use up to 255 registers per thread (for the large boxes one CTA per SM,
+// which their FP64 plane allows no more than anyway); two CTAs of 128
+// registers spilled up to 976 B per thread.
+template <int N>
+constexpr bool rd_regs() { return N < 80; }
+template <int N>
+constexpr int rd_threads() { return 256; }
+template <int N>
+constexpr int rd_min_blocks() { return 1; }
 
 // psi -> V(r) psi(r) / N^3 -> back, in place on the sticks (QE vloc_psi_gamma);
 // one unit = plane z of item `item`
@@ -388,42 +404,53 @@ __global__ void __launch_bounds__(PNT) k_plane_inv_box(const double2* __restrict
 // instead of once per band pair, and the psi planes come from L2 (the grid of
 // one CTA per band pair read 8.6 GB of boxes per c2 call; 1.7 against 2.1 ms).
 template <int N, bool PR>
-__global__ void __launch_bounds__(PNT, 2) k_plane_rhs(const double2* __restrict__ evcr,
+__global__ void __launch_bounds__(rd_threads<N>(), rd_min_blocks<N>()) k_plane_rhs(const double2* __restrict__ evcr,
                                                    const double2* __restrict__ dvbox, int npv,
                                                    StickTab st, double2* __restrict__ sticks,
                                                    const double2* __restrict__ twg) {
+  constexpr int NT = rd_threads<N>();
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* tw = reinterpret_cast<double2*>(smraw);
   double2* pl = tw + 2 * N;
   const int z = blockIdx.x, p = blockIdx.y;
   load_tw<N>(tw, twg);
-  constexpr int PER = (N * N + PNT - 1) / PNT;
+  constexpr bool REG = rd_regs<N>();
+  constexpr int PER = REG ? (N * N + NT - 1) / NT : 1;
   constexpr double inv = 1.0 / ((double)N * N * N);
   const double2* dv = dvbox + ((long)(p >> 1) * N + z) * N * N;
   const bool hi = p & 1;
   double w[PER];
+  if constexpr (REG) {
 #pragma unroll
-  for (int q = 0; q < PER; ++q) {
-    const int e = threadIdx.x + q * PNT;
-    w[q] = 0.0;
-    if (e < N * N) {
-      const double2 d = dv[e];
-      w[q] = (hi ? d.y : d.x) * inv;
+    for (int q = 0; q < PER; ++q) {
+      const int e = threadIdx.x + q * NT;
+      w[q] = 0.0;
+      if (e < N * N) {
+        const double2 d = dv[e];
+        w[q] = (hi ? d.y : d.x) * inv;
+      }
     }
   }
   for (int k = 0; k < npv; ++k) {
     const double2* ps = evcr + ((long)k * N + z) * N * N;
     __syncthreads();  // the previous band pair's gather is done with the plane
+    if constexpr (REG) {
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      const int e = threadIdx.x + q * PNT;
-      if (e < N * N) pl[Plane<N>::at_lin(e)] = cscale(ps[e], w[q]);
+      for (int q = 0; q < PER; ++q) {
+        const int e = threadIdx.x + q * NT;
+        if (e < N * N) pl[Plane<N>::at_lin(e)] = cscale(ps[e], w[q]);
+      }
+    } else {
+      for (int e = threadIdx.x; e < N * N; e += NT) {
+        const double2 d = dv[e];
+        pl[Plane<N>::at_lin(e)] = cscale(ps[e], (hi ? d.y : d.x) * inv);
+      }
     }
     __syncthreads();
-    plane_fft_rows<N, -1, PR>(pl, tw);
-    plane_fft_cols<N, -1, PR>(pl, st, tw);
+    plane_fft_rows<N, -1, PR, double2, NT>(pl, tw);
+    plane_fft_cols<N, -1, PR, double2, NT>(pl, st, tw);
     const long item = (long)p * npv + k;
-    plane_gather<N>(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+    plane_gather<N, double2, Plane<N>, NT>(pl, sticks + (item * N + z) * st.nst, st.st_pos, st.nst);
   }
 }
 
@@ -436,7 +463,7 @@ __global__ void __launch_bounds__(PNT, 2) k_plane_rhs(const double2* __restrict_
 // per band pair made the kernel DRAM-bound: 12.6 GB per c2 call); two CTAs per
 // SM (a few hundred bytes of spills) beat one (2.5 against 2.9 ms per c2 call).
 template <int N, bool PR>
-__global__ void __launch_bounds__(PNT, 2) k_plane_drho(const double2* __restrict__ dsticks,
+__global__ void __launch_bounds__(rd_threads<N>(), rd_min_blocks<N>()) k_plane_drho(const double2* __restrict__ dsticks,
                                                     const double2* __restrict__ evcr,
                                                     const double* __restrict__ occ, int nocc,
                                                     int mb, StickTab st, double2* __restrict__ acc,
@@ -447,55 +474,79 @@ __global__ void __launch_bounds__(PNT, 2) k_plane_drho(const double2* __restrict
   double2* pl = tw + 2 * N;
   const int z = blockIdx.x, pp = blockIdx.y;
   const int npv = (nocc + 1) / 2;
+  constexpr int NT = rd_threads<N>();
   load_tw<N>(tw, twg);
   // a perturbation's density of this plane is accumulated in registers (thread t
   // owns plane elements t + PNT q); the first of the two is parked in acc once
   double2* ac = acc + ((long)pp * N + z) * N * N;
-  constexpr int PER = (N * N + PNT - 1) / PNT;
+  constexpr bool REG = rd_regs<N>();
+  constexpr int PER = REG ? (N * N + NT - 1) / NT : 1;
   double a[PER];
   for (int pi = 0; pi < 2; ++pi) {
     const int p = 2 * pp + pi;
 #pragma unroll
     for (int q = 0; q < PER; ++q) a[q] = 0.0;
+    if constexpr (!REG) {  // the band sum of this perturbation in ac[].x (pi = 0) or ac[].y (pi = 1)
+      for (int e = threadIdx.x; e < N * N; e += NT) {
+        if (pi == 0) ac[e].x = 0.0;
+        else ac[e].y = 0.0;
+      }
+    }
     for (int k = 0; p < mb && k < npv; ++k) {
       const long item = (long)p * npv + k;
       __syncthreads();
-      plane_zero<N, PR>(pl, st);
+      plane_zero<N, PR, double2, Plane<N>, NT>(pl, st);
       __syncthreads();
-      plane_scatter<N>(pl, dsticks + (item * N + z) * st.nst, st.st_pos, st.nst);
+      plane_scatter<N, double2, Plane<N>, NT>(pl, dsticks + (item * N + z) * st.nst, st.st_pos, st.nst);
       __syncthreads();
-      plane_fft_cols<N, +1, PR>(pl, st, tw);
-      plane_fft_rows<N, +1, PR>(pl, tw);
+      plane_fft_cols<N, +1, PR, double2, NT>(pl, st, tw);
+      plane_fft_rows<N, +1, PR, double2, NT>(pl, tw);
       const double o1 = occ[2 * k];
       const double o2 = (2 * k + 1 < nocc) ? occ[2 * k + 1] : 0.0;
       const double2* ps = evcr + ((long)k * N + z) * N * N;
+      if constexpr (REG) {
 #pragma unroll
-      for (int q = 0; q < PER; ++q) {
-        const int e = threadIdx.x + q * PNT;
-        if (e < N * N) {
+        for (int q = 0; q < PER; ++q) {
+          const int e = threadIdx.x + q * NT;
+          if (e < N * N) {
+            const double2 d = pl[Plane<N>::at_lin(e)], s = ps[e];
+            a[q] += fma(o1 * s.x, d.x, o2 * s.y * d.y);
+          }
+        }
+      } else {
+        for (int e = threadIdx.x; e < N * N; e += NT) {
           const double2 d = pl[Plane<N>::at_lin(e)], s = ps[e];
-          a[q] += fma(o1 * s.x, d.x, o2 * s.y * d.y);
+          const double v = fma(o1 * s.x, d.x, o2 * s.y * d.y);
+          if (pi == 0) ac[e].x += v;
+          else ac[e].y += v;
         }
       }
     }
-    if (pi == 0) {
+    if (REG && pi == 0) {
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
-        const int e = threadIdx.x + q * PNT;
+        const int e = threadIdx.x + q * NT;
         if (e < N * N) ac[e].x = a[q];
       }
     }
   }
   __syncthreads();
+  if constexpr (REG) {
 #pragma unroll
-  for (int q = 0; q < PER; ++q) {
-    const int e = threadIdx.x + q * PNT;
-    if (e < N * N) pl[Plane<N>::at_lin(e)] = make_double2(ac[e].x * scale, a[q] * scale);
+    for (int q = 0; q < PER; ++q) {
+      const int e = threadIdx.x + q * NT;
+      if (e < N * N) pl[Plane<N>::at_lin(e)] = make_double2(ac[e].x * scale, a[q] * scale);
+    }
+  } else {
+    for (int e = threadIdx.x; e < N * N; e += NT) {
+      const double2 v = ac[e];
+      pl[Plane<N>::at_lin(e)] = make_double2(v.x * scale, v.y * scale);
+    }
   }
   __syncthreads();
-  plane_fft_rows<N, -1, PR>(pl, tw);
-  plane_fft_cols<N, -1, PR>(pl, st, tw);
-  plane_gather<N>(pl, osticks + ((long)pp * N + z) * st.nst, st.st_pos, st.nst);
+  plane_fft_rows<N, -1, PR, double2, NT>(pl, tw);
+  plane_fft_cols<N, -1, PR, double2, NT>(pl, st, tw);
+  plane_gather<N, double2, Plane<N>, NT>(pl, osticks + ((long)pp * N + z) * st.nst, st.st_pos, st.nst);
 }
 
 // Local potential for N1 == N2 boxes (64^3): the inverse-row second step, the
@@ -791,7 +842,7 @@ constexpr int gen_threads() {
 }
 
 template <int N, bool PR, class C>
-__global__ void __launch_bounds__(gen_threads<N, C>()) k_plane_vloc_gen(C* __restrict__ sticks, StickTab st,
+__global__ void __launch_bounds__(gen_threads<N, C>(), sizeof(C) == 8 ? 2 : 1) k_plane_vloc_gen(C* __restrict__ sticks, StickTab st,
                                                                          const real_t<C>* __restrict__ vs,
                                                                          const C* __restrict__ twg, const int* dn) {
   constexpr int NT = gen_threads<N, C>();
@@ -954,20 +1005,20 @@ struct FftN {
     if (mb <= 0) return;
     const dim3 g(N, mb);
     if (f.st.prune)
-      k_plane_rhs<N, true><<<g, PNT, psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
+      k_plane_rhs<N, true><<<g, rd_threads<N>(), psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
     else
-      k_plane_rhs<N, false><<<g, PNT, psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
+      k_plane_rhs<N, false><<<g, rd_threads<N>(), psmem<N>(), f.stream>>>(evcr, dvbox, npv, f.st, sticks, f.tw);
   }
   static void drho(const FftArgs& f, const double2* dsticks, const double2* evcr, const double* occ, int nocc,
                    int mb, double2* acc, double scale, double2* osticks) {
     if (mb <= 0) return;
     const dim3 g(N, (mb + 1) / 2);
     if (f.st.prune)
-      k_plane_drho<N, true><<<g, PNT, psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st, acc, scale,
-                                                              osticks, f.tw);
+      k_plane_drho<N, true><<<g, rd_threads<N>(), psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st, acc,
+                                                                          scale, osticks, f.tw);
     else
-      k_plane_drho<N, false><<<g, PNT, psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st, acc, scale,
-                                                               osticks, f.tw);
+      k_plane_drho<N, false><<<g, rd_threads<N>(), psmem<N>(), f.stream>>>(dsticks, evcr, occ, nocc, mb, f.st, acc,
+                                                                           scale, osticks, f.tw);
   }
 };
 

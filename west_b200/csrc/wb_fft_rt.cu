@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kRtPnt) k_plane_rhs_rt(const double2* __restri
 // psi_v(r) dpsi_v(r) for the two perturbations of pair pp, accumulated in the
 // CTA's own slice of acc (one element per thread throughout), then
 // (drho_p1 + i drho_p2) scale -> forward -> sticks
-__global__ void __launch_bounds__(kRtPnt) k_plane_drho_rt(const double2* __restrict__ dsticks,
+__global__ void __launch_bounds__(kRtPnt, 1) k_plane_drho_rt(const double2* __restrict__ dsticks,
                                                           const double2* __restrict__ evcr,
                                                           const double* __restrict__ occ, int nocc, int mb,
                                                           StickTab st, RtGeo g, double2* __restrict__ acc,
