@@ -1,5 +1,7 @@
 """Perturbation sharding over ranks: the cyclic distribution of WEST's images
-and a two-rank gloo run on CPU whose gathered result equals one rank's."""
+and a two-rank gloo run on CPU whose gathered result equals one rank's (the
+operator here is the oracle, as CPU-only ranks have no GPU kernels; the same
+sharding through the library's CUDA kernels is tests/test_gpu_multirank.py)."""
 import os
 import socket
 

@@ -1,0 +1,97 @@
+"""Two ranks through the library itself: two processes on the one GPU of this
+box (a gloo process group; no kernel of one rank waits on the other, the only
+exchange is the gloo collective on host memory between library calls), each
+applying its cyclic share of the perturbations (WEST's pert%l2g) with the CUDA
+kernels, the shares gathered, against one rank doing all the columns; and the
+perturbation-sharded PDEP Davidson (wb_davidson_set_apply +
+distribute.ShardedDavidsonApply) against the built-in one.  The all-gather is
+the same code as on several GPUs (there over NCCL)."""
+import datetime
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(n_pdep_times=4, n_pdep_maxiter=100, tr2_dfpt=1e-12, trev_pdep=1e-6, trev_pdep_rel=1e-1)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    from west_b200.distribute import PertDistribution, ShardedDavidsonApply
+    from west_b200.system import build_system, perturbations, randomized_basis
+    from west_b200.wstat import ResponseOperator
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        s = build_system("small")
+        # 1. sharded apply_operator: this rank's columns, then an all-gather of the shares
+        m = 7
+        dvg = perturbations(s, m)
+        d = PertDistribution(m, world, rank)
+        cols = d.local_columns()
+        op = ResponseOperator(s, verbose=False)
+        op.set_autotune(False)
+        loc = np.zeros((s.npw, d.nlocx), dtype=np.complex128, order="F")
+        ierr = op.apply_operator(len(cols), np.asfortranarray(dvg[:, cols]), loc, 1e-14)
+        parts = [torch.zeros(2 * s.npw * d.nlocx, dtype=torch.float64) for _ in range(world)]
+        dist.all_gather(parts, torch.from_numpy(np.ascontiguousarray(loc.T).view(np.float64).ravel().copy()))
+        full = np.zeros((s.npw, m), dtype=np.complex128)
+        for r in range(world):
+            blk = parts[r].numpy().view(np.complex128).reshape(d.nlocx, s.npw).T
+            c = d.local_columns(r)
+            full[:, c] = blk[:, :len(c)]
+        # 2. the sharded Davidson: same starting basis on every rank
+        dvg0 = randomized_basis(s, 4)
+        op2 = ResponseOperator(s, verbose=False)
+        hook = ShardedDavidsonApply(op2).install()
+        ev, conv, vec, info = op2.davidson(dvg0, 4, **KW)
+        hook.remove()
+        out.put((rank, full, [int(x) for x in ierr], ev, int(info["dav_iter"]), hook.calls))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_through_the_library():
+    from west_b200.system import build_system, perturbations, randomized_basis
+    from west_b200.wstat import ResponseOperator
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = {}
+    for _ in range(2):
+        r = q.get(timeout=600)
+        res[r[0]] = r
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    s = build_system("small")
+    dvg = perturbations(s, 7)
+    op = ResponseOperator(s, verbose=False)
+    op.set_autotune(False)
+    ref = np.zeros_like(dvg, order="F")
+    op.apply_operator(7, dvg, ref, 1e-14)
+    a = ResponseOperator(s, verbose=False)
+    a.set_autotune(False)
+    ev_ref, _, _, info_ref = a.davidson(randomized_basis(s, 4), 4, **KW)
+    for rank in (0, 1):
+        _, full, ierr, ev, dav_iter, calls = res[rank]
+        assert np.linalg.norm(full - ref) / np.linalg.norm(ref) < 1e-12
+        assert dav_iter == info_ref["dav_iter"] and calls == info_ref["apply_calls"]
+        assert np.abs((ev - ev_ref) / ev_ref).max() < 1e-10
+    assert np.array_equal(res[0][3], res[1][3])   # the ranks' Davidsons run in lock step

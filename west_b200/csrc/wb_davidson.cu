@@ -256,6 +256,7 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ hr, 
 // excluded from the selection.
 constexpr int kBJ = 16;
 constexpr int kMaxBasis = 4096;
+constexpr int kBJNormCtas = 1184;  // grid of the norm reduction (8 CTAs per SM)
 constexpr int kBJ2 = 2 * kBJ;
 constexpr int kBJThreads = 256;
 
@@ -280,8 +281,10 @@ __global__ void k_bj_init(const double* __restrict__ hr, long ldh, int n, int np
   }
 }
 
-// red[0] = sum of squared off-diagonal entries, red[1] = of all entries
-__global__ void k_bj_norms(const double* __restrict__ A, int npad, double* __restrict__ red) {
+// per-CTA partial sums of the squared off-diagonal entries and of all entries
+// (part[2 b], part[2 b + 1]); k_bj_norms_final adds them in a fixed order, so
+// every run (and every rank of a sharded Davidson) takes the same decisions
+__global__ void k_bj_norms(const double* __restrict__ A, int npad, double* __restrict__ part) {
   __shared__ double sh[2][32];
   double off = 0.0, tot = 0.0;
   const long nn = (long)npad * npad;
@@ -299,8 +302,16 @@ __global__ void k_bj_norms(const double* __restrict__ A, int npad, double* __res
   if (threadIdx.x == 0) {
     double so = 0.0, st = 0.0;
     for (int i = 0; i < (int)blockDim.x / 32; ++i) { so += sh[0][i]; st += sh[1][i]; }
-    atomicAdd(red, so);
-    atomicAdd(red + 1, st);
+    part[2 * blockIdx.x] = so;
+    part[2 * blockIdx.x + 1] = st;
+  }
+}
+__global__ void k_bj_norms_final(const double* __restrict__ part, int nparts, double* __restrict__ red) {
+  if (threadIdx.x == 0) {
+    double so = 0.0, st = 0.0;
+    for (int i = 0; i < nparts; ++i) { so += part[2 * i]; st += part[2 * i + 1]; }
+    red[0] = so;
+    red[1] = st;
   }
 }
 
@@ -533,7 +544,7 @@ size_t bj_doubles(int nmax) {
   int nb = (nmax + kBJ - 1) / kBJ;
   nb += nb & 1;
   const size_t npad = (size_t)nb * kBJ;
-  return 2 * npad * npad + (size_t)(nb / 2) * kBJ2 * kBJ2 + 2 + nmax + nb;
+  return 2 * npad * npad + (size_t)(nb / 2) * kBJ2 * kBJ2 + 2 + nmax + nb + 2 * kBJNormCtas;
 }
 
 // Lowest nsel eigenpairs of the symmetric hr[:n, :n] (upper triangle, column
@@ -548,16 +559,17 @@ int block_jacobi(const double* hr, long ldh, int n, int nsel, double* w, double*
   double* V = A + (size_t)npad * npad;
   double* U = V + (size_t)npad * npad;
   double* red = U + (size_t)npair * kBJ2 * kBJ2;
-  int* iw = reinterpret_cast<int*>(red + 2);  // skip flags, then the selection indices
+  double* npart = red + 2;                     // per-CTA partial norms
+  int* iw = reinterpret_cast<int*>(npart + 2 * kBJNormCtas);  // skip flags, then the selection indices
   int* skip = iw;
   int* idx = iw + nb;
-  const int g = std::min(1184, (int)(((long)npad * npad + 255) / 256));
+  const int g = std::min(kBJNormCtas, (int)(((long)npad * npad + 255) / 256));
   const double skip_frac = 1e-30 / (0.5 * nb * (nb - 1));
   k_bj_init<<<g, 256, 0, s>>>(hr, ldh, n, npad, A, V);
   int sweep = 0;
   for (;; ++sweep) {
-    WB_CU(cudaMemsetAsync(red, 0, 2 * sizeof(double), s));
-    k_bj_norms<<<g, 256, 0, s>>>(A, npad, red);
+    k_bj_norms<<<g, 256, 0, s>>>(A, npad, npart);
+    k_bj_norms_final<<<1, 32, 0, s>>>(npart, g, red);
     WB_CU(cudaMemcpyAsync(red_host, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     WB_CU(cudaStreamSynchronize(s));
     if (red_host[0] <= 1e-28 * red_host[1] || sweep == 40) break;

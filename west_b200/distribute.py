@@ -64,13 +64,14 @@ def gather_batch(local, col0: int, m: int, nranks: int, rank: int, group=None):
     send[: local.shape[0]] = local
     if cplx:  # exchanged as real pairs
         send = torch.view_as_real(send)
-    if local.is_cuda:
+    if local.is_cuda and dist.get_backend(group) == "nccl":
         recv = torch.empty((nranks * maxloc,) + tuple(send.shape[1:]), dtype=send.dtype, device=send.device)
         dist.all_gather_into_tensor(recv, send, group=group)
-    else:
-        parts = [torch.empty_like(send) for _ in range(nranks)]
-        dist.all_gather(parts, send, group=group)
-        recv = torch.cat(parts, 0)
+    else:  # gloo: through host memory
+        host = send.cpu()
+        parts = [torch.empty_like(host) for _ in range(nranks)]
+        dist.all_gather(parts, host, group=group)
+        recv = torch.cat(parts, 0).to(send.device)
     if cplx:
         recv = torch.view_as_complex(recv)
     out = torch.empty((m, n), dtype=local.dtype, device=local.device)
@@ -124,7 +125,8 @@ class ShardedDavidsonApply:
         import torch.distributed as dist
         x = torch.as_tensor(_CudaBuffer(dvg_ptr, m, ld), device="cuda")
         y = torch.as_tensor(_CudaBuffer(dng_ptr, m, ld), device="cuda")
-        chk = torch.tensor([col0, m, -col0, -m], dtype=torch.int64, device="cuda")
+        dev = "cuda" if dist.get_backend(self.group) == "nccl" else "cpu"
+        chk = torch.tensor([col0, m, -col0, -m], dtype=torch.int64, device=dev)
         dist.all_reduce(chk, op=dist.ReduceOp.MAX, group=self.group)
         if int(chk[0]) != col0 or int(chk[1]) != m or -int(chk[2]) != col0 or -int(chk[3]) != m:
             raise RuntimeError(f"ranks diverged: batch ({col0}, {m}) on rank {self.rank}")
