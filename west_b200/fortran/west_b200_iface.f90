@@ -76,7 +76,7 @@ CONTAINS
     USE ions_base,          ONLY : nat, ityp
     USE uspp_init,          ONLY : init_us_2
     USE cell_base,          ONLY : omega
-    USE klist,              ONLY : xk, igk_k
+    USE klist,              ONLY : igk_k
     USE westcom,            ONLY : nbnd_occ, occupation, alphapv_dfpt, n_dfpt_maxiter, l_kinetic_only
     USE types_bz_grid,      ONLY : k_grid
     USE types_coulomb,      ONLY : pot3D
@@ -86,9 +86,9 @@ CONTAINS
     INTEGER(C_INT) :: ierr
     !
     nb = nbnd_occ(1)
-    npw = ngk(1)
-    CALL g2_kin(1)
-    IF (nkb > 0) CALL init_us_2(npw, igk_k(1,1), xk(1,1), vkb)
+    npw = ngk(1)                               ! as dfpt_module.f90:34,175 (pwcom's npw)
+    CALL g2_kin(1)                             ! dfpt_module.f90:153
+    IF (nkb > 0) CALL init_us_2(npw, igk_k(1,1), k_grid%p_cart(1,1), vkb, .FALSE.)   ! :158-160, host vkb
     ALLOCATE(nl_c(npw), nlm_c(npw), g2kin_c(npw), vrs_c(dffts%nnr), et_c(nb), occ_c(nb))
     ALLOCATE(deeq_c(MAX(nkb,1), MAX(nkb,1)), sqvc_c(npw), evc_c(npwx, nb), vkb_c(npwx, MAX(nkb,1)))
     nl_c = dffts%nl(1:npw); nlm_c = dffts%nlm(1:npw)
