@@ -162,6 +162,7 @@ typedef struct wb_tuning {
   int tc_update_systems;     /* systems per CTA of the tcgen05 update (64, 128; 0 default) */
   int plane_fused_fp64;      /* 1: one-pass fused plane kernel in the FP64 operator   */
   int plane_fused_mixed;     /* 1: the same in the FP32 inner operator                */
+  int dmma_prefetch;         /* FP64 bra-ket: k steps between operand load and MMA (1, 2) */
   float tuning_ms;           /* host time spent tuning                                */
 } wb_tuning;
 int wb_get_tuning(const wb_ctx* ctx, wb_tuning* out);

@@ -381,7 +381,8 @@ int autotune64(wb_ctx* c, int nsys) {
   for (int ctas : {1, 2, 4}) {
     const int ns = gemm_tn_splits(M, nsys, K, ctas);
     const float ms = time_ms(c, [&] {
-      gemm_tn(W, K, M, (const double*)c->X.p, 2 * ld, c->act.as<int>(), nsys, K, ns, c->part.as<double>(), s);
+      gemm_tn(W, K, M, (const double*)c->X.p, 2 * ld, c->act.as<int>(), nsys, K, ns, c->part.as<double>(), s,
+              nullptr, ctas, c->tune.dmma_pf);
     });
     if (ms < best) { best = ms; c->tune.dmma_ctas = ctas; }
   }
@@ -486,7 +487,7 @@ void apply_A(wb_ctx* c, const double2* Xv, double2* Tv, const int* cols, const i
   {
     Stage g(c, WB_STAGE_GEMM_TN, 1, n);
     gemm_tn(Wsub, K, M, (const double*)Xv, 2 * ld, cols, n, K, nsplit, c->part.as<double>(), s, dn,
-            c->tune.dmma_ctas);
+            c->tune.dmma_ctas, c->tune.dmma_pf);
   }
   {
     Stage g(c, WB_STAGE_GEMM_REDUCE, 1, n);
@@ -1128,6 +1129,10 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
   c->omega = s->omega;
   c->wk = s->wk;
   c->alpha = s->alpha_pv;
+  // FP64 bra-ket operand prefetch: two k steps ahead for few projectors (64 at
+  // the c2 cell: 4.3 -> 3.3 ms per m = 16 call), one for many (208 at the 108^3
+  // cell, where the extra registers cost more: 222 -> 242 ms)
+  c->tune.dmma_pf = c->nproj <= 96 ? 2 : 1;
   // fractional occupations (Tools/set_nbndocc.f90:58-69): nbnd_occ_full is the
   // highest band occupied above 1 - docc_thr; the correction of dfpt_module.f90:
   // 363-398 needs non-degenerate energies wherever the occupations differ (:387)
@@ -1312,6 +1317,7 @@ int wb_get_tuning(const wb_ctx* c, wb_tuning* out) {
   out->tuned_fp64 = c->tune.done64;
   out->tuned_mixed = c->tune.done32;
   out->dmma_ctas_per_sm = c->tune.dmma_ctas;
+  out->dmma_prefetch = c->tune.dmma_pf;
   out->tc_braket_ctas_per_sm = c->tune.umma_ctas;
   out->tc_update_systems = c->tune.update_nj;
   out->plane_fused_fp64 = fft_fusable(c->nr, c->st) && !c->tune.unfused64;

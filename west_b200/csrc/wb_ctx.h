@@ -114,7 +114,7 @@ struct wb_ctx {
   // autotuned launch shapes (set on the first batch of each form, then fixed)
   struct Tune {
     int on = 1, done64 = 0, done32 = 0;
-    int dmma_ctas = 2, umma_ctas = 2, update_nj = 0, unfused64 = 0, unfused32 = 0;
+    int dmma_ctas = 2, dmma_pf = 1, umma_ctas = 2, update_nj = 0, unfused64 = 0, unfused32 = 0;
     float ms = 0.f;
   } tune;
   cudaEvent_t tev0 = nullptr, tev1 = nullptr;

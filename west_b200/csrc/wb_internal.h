@@ -147,9 +147,10 @@ __host__ __device__ inline int gemm_tn_splits(int M, int ncol, int K, int ctas_p
 }
 // part doubles for any column count up to nsys and any target up to ctas_max
 size_t gemm_tn_part_doubles(int M, int nsys, int K, int ctas_max);
-// with dn, ctas selects the device plan (nsplit is then ignored)
+// with dn, ctas selects the device plan (nsplit is then ignored); prefetch: k
+// steps between an operand load and its MMAs (1 or 2)
 void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
-             int nsplit, double* part, cudaStream_t s, const int* dn = nullptr, int ctas = 2);
+             int nsplit, double* part, cudaStream_t s, const int* dn = nullptr, int ctas = 2, int prefetch = 1);
 // S = 2 sum_s part - W0 X0 (Gamma bra-ket, glbrak.f90:39-40), then
 // C[j][r] = sum_{r'<nkb} D[r][r'] S[j][r'] for r < nkb, alpha S[j][r] otherwise
 void gamma_reduce(const double* part, int nsplit, int M, int ncol, const double* W, long ldw, const double* X,

@@ -26,6 +26,9 @@ WB_DEV void dmma(double& d0, double& d1, double a, double b) {
 constexpr int TN_T = 32;
 constexpr int TN_W = 4;
 
+// PF: k steps between an operand load and the MMAs that use it (1 or 2: two
+// pay at 64 projectors, cost at 208; same sums in the same order either way)
+template <int PF>
 __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict__ W, long ldw, int M,
                                                        const double* __restrict__ X, long ldx,
                                                        const int* __restrict__ cols, int ncol_host, const int* dn,
@@ -61,8 +64,6 @@ __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict_
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-  // operands of the next k step are loaded while this step's MMAs run
-  double av[4], bv[4];
   auto load = [&](int k, double* a, double* b) {
     const int kk = k + lk;
     const bool kok = kk < ke;
@@ -72,16 +73,35 @@ __global__ void __launch_bounds__(32 * TN_W) k_gemm_tn(const double* __restrict_
       b[i] = (bok[i] && kok) ? __ldg(bcol[i] + kk) : 0.0;
     }
   };
-  load(kb + warp * 4, av, bv);
-  for (int k = kb + warp * 4; k < ke; k += 4 * TN_W) {
-    double an[4], bn[4];
-    load(k + 4 * TN_W, an, bn);
+  auto mma_step = [&](const double* a, const double* b) {
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], av[a], bv[b]);
+      for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+  };
+  constexpr int KS = 4 * TN_W;  // k advanced per step (the CTA's warps interleave k)
+  const int k0 = kb + warp * 4;
+  if constexpr (PF == 1) {      // the next step's operands load while this step's MMAs run
+    double av[4], bv[4];
+    load(k0, av, bv);
+    for (int k = k0; k < ke; k += KS) {
+      double an[4], bn[4];
+      load(k + KS, an, bn);
+      mma_step(av, bv);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) { av[i] = an[i]; bv[i] = bn[i]; }
+      for (int i = 0; i < 4; ++i) { av[i] = an[i]; bv[i] = bn[i]; }
+    }
+  } else {                      // two steps ahead; two steps per trip, the buffers swap roles
+    double a0[4], b0[4], a1[4], b1[4];
+    load(k0, a0, b0);
+    load(k0 + KS, a1, b1);
+    for (int k = k0; k < ke; k += 2 * KS) {
+      mma_step(a0, b0);         // step k, loaded two steps ago
+      load(k + 2 * KS, a0, b0);
+      if (k + KS >= ke) break;
+      mma_step(a1, b1);         // step k + KS
+      load(k + 3 * KS, a1, b1);
+    }
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a)
@@ -109,13 +129,16 @@ size_t gemm_tn_part_doubles(int M, int nsys, int K, int ctas_max) {
 }
 
 void gemm_tn(const double* W, long ldw, int M, const double* X, long ldx, const int* cols, int ncol, int K,
-             int nsplit, double* part, cudaStream_t s, const int* dn, int ctas) {
+             int nsplit, double* part, cudaStream_t s, const int* dn, int ctas, int prefetch) {
   if (ncol <= 0 || M <= 0) return;
   if (dn) nsplit = gemm_tn_splits(M, 1, K, ctas);  // grid for the largest plan
   int kchunk = (K + nsplit - 1) / nsplit;
   kchunk = (kchunk + 15) / 16 * 16;
   dim3 grid((M + TN_T - 1) / TN_T, (ncol + TN_T - 1) / TN_T, nsplit);
-  k_gemm_tn<<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, dn, K, kchunk, ctas, part);
+  if (prefetch == 2)
+    k_gemm_tn<2><<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, dn, K, kchunk, ctas, part);
+  else
+    k_gemm_tn<1><<<grid, 32 * TN_W, 0, s>>>(W, ldw, M, X, ldx, cols, ncol, dn, K, kchunk, ctas, part);
 }
 
 __global__ void __launch_bounds__(256) k_gamma_reduce(const double* __restrict__ part, int nsplit, int M,

@@ -74,7 +74,7 @@ class WbDavidsonInfo(ctypes.Structure):
 class WbTuning(ctypes.Structure):
     _fields_ = [("autotune", _i), ("tuned_fp64", _i), ("tuned_mixed", _i), ("dmma_ctas_per_sm", _i),
                 ("tc_braket_ctas_per_sm", _i), ("tc_update_systems", _i), ("plane_fused_fp64", _i),
-                ("plane_fused_mixed", _i), ("tuning_ms", ctypes.c_float)]
+                ("plane_fused_mixed", _i), ("dmma_prefetch", _i), ("tuning_ms", ctypes.c_float)]
 
 
 class WestB200Error(RuntimeError):
