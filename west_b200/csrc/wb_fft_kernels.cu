@@ -810,16 +810,48 @@ WB_DEV void rows_vloc_middle(C* pl, const C* tw, const real_t<C>* __restrict__ v
   }
 }
 
+// Threads per row in the row phases 1 and 3 (B of them work): A when A > B, so
+// that a row's lanes never share a quarter-warp (FP64) or half-warp (FP32) with
+// the next row's in a way that lands two on one bank (9-lane rows at 108^3 gave
+// 2-way conflicts; 12-lane slots with the row stride 108 give none)
+template <int N>
+constexpr int row_slot() { return FftSplit<N>::N1 > FftSplit<N>::N2 ? FftSplit<N>::N1 : FftSplit<N>::N2; }
+
+// Rows, phase 1: the inverse step 1 of the split (A, B): thread n2 < B of a row
+// takes x = B n1 + n2 (pruned inputs in the outer quarters of A), A-point DFT,
+// twiddles, back to the same positions.
+template <int N, int NT, bool PIN, class C>
+WB_DEV void rows_inverse_step1(C* pl, const C* tw) {
+  constexpr int A = FftSplit<N>::N1, B = FftSplit<N>::N2, S = row_slot<N>();
+  static_assert(!PIN || A % 4 == 0, "input pruning needs A % 4 == 0");
+  using LP = LinePad<N>;
+  for (int it = threadIdx.x; it < N * S; it += NT) {
+    const int y = it / S, n2 = it % S;
+    if (n2 >= B) continue;
+    C* p = pl + Plane<N>::row(y);
+    C v[A];
+#pragma unroll
+    for (int n1 = 0; n1 < A; ++n1)
+      v[n1] = (PIN && !outer_quarter<A>(n1)) ? mkc<C>(0, 0) : p[LP::off_blk(n1, n2)];
+    rdft<A, +1, N>(v, tw);
+#pragma unroll
+    for (int k1 = 1; k1 < A; ++k1) v[k1] = ctw<+1>(v[k1], tw_step1<N, A, B>(tw, k1, n2));
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) p[LP::off_blk(k1, n2)] = v[k1];
+  }
+}
+
 // Rows, phase 3: the forward step 2 of the split (B, A): thread k1' < B takes
 // Y[k1', n2'] from off_blk(n2', k1') and writes output k1' + B k2' to
 // off_blk(k2', k1'), the positions it read.
 template <int N, int NT, bool POUT, class C>
 WB_DEV void rows_forward_step2(C* pl, const C* tw) {
-  constexpr int A = FftSplit<N>::N1, B = FftSplit<N>::N2;
+  constexpr int A = FftSplit<N>::N1, B = FftSplit<N>::N2, S = row_slot<N>();
   static_assert(!POUT || A % 4 == 0, "output pruning of the transposed split needs A % 4 == 0");
   using LP = LinePad<N>;
-  for (int it = threadIdx.x; it < N * B; it += NT) {
-    const int y = it / B, k1 = it % B;
+  for (int it = threadIdx.x; it < N * S; it += NT) {
+    const int y = it / S, k1 = it % S;
+    if (k1 >= B) continue;
     C* p = pl + Plane<N>::row(y);
     C v[A];
 #pragma unroll
@@ -860,7 +892,7 @@ __global__ void __launch_bounds__(gen_threads<N, C>(), sizeof(C) == 8 ? 2 : 1) k
   __syncthreads();
   const OffCols<N> cols{st.xhi + 1, st.ncols};
   fft_lines_split<N, N1, N2, +1, NT, RP, false>(pl, cols, Plane<N>::RS, st.ncols, tw);
-  fft_step1<N, +1, NT, false, true, RP ? PRUNE_IN : PRUNE_NONE>(pl, OffLinear{Plane<N>::RS}, 1, N, tw);
+  rows_inverse_step1<N, NT, RP>(pl, tw);
   __syncthreads();
   rows_vloc_middle<N, NT>(pl, tw, vs + (long)z * N * N);
   __syncthreads();
