@@ -332,6 +332,15 @@ def run_b200(args, rank, world, local_rank):
         steps_ms = ms / args.steps
         stage_share = {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in share_stats.values())), 4)
                        for k, v in share_stats.items()}
+        # in-place rates of the FP64 projector GEMMs (stage timers of the profiled step):
+        # 2 M K flops per active system, M = nkb + nbnd_occ, K = 2 npw real rows
+        gemm_rates = {}
+        for k in ("gemm_tn", "gemm_nn"):
+            v = share_stats.get(k)
+            if v and v["ms"] > 0:
+                tf = 2.0 * (s.nkb + s.nbnd_occ) * 2 * npw * v["items"] / (v["ms"] * 1e-3) / 1e12
+                gemm_rates[k] = {"tflops": tf, "frac_of_dgemm": tf / fp64_peak, "systems": int(v["items"]),
+                                 "ms": v["ms"]}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": steps_ms, "higher_is_better": True, "scaling": "weak",
@@ -352,6 +361,8 @@ def run_b200(args, rank, world, local_rank):
                          "fp64": {"achieved_tflops_nominal": fp64_ach, "dgemm_peak_tflops": fp64_peak,
                                   "frac": fp64_ach / fp64_peak}},
             "stage_share": stage_share,
+            "gemm_fp64": dict(gemm_rates, note="bra-ket (k_gemm_tn, DMMA, split K) and update (k_gemm_nn) "
+                                                "in the PCG operator, against the measured cuBLAS DGEMM"),
             "work": {"cg_active_sum": act_sum, "fft_boxes": boxes},
             "eager_profiled": {"value": world * m * args.steps / (ms_eager * 1e-3), "unit": UNIT,
                                "ms_per_step": ms_eager / args.steps,

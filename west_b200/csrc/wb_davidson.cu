@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ hr, 
           }
         }
       }
-      for (int e = tid; e < npairs * n; e += nt) {      // V <- V J
-        const int k = e / n, i = e % n;
+      for (int e = tid; e < npairs * n; e += nt) {      // V <- V J; lanes run over the planes of a
+        const int i = e / npairs, k = e % npairs;       // row (rows are n doubles apart: one bank)
         const int p = pp[k], q = qq[k];
         if (q >= n || sn[k] == 0.0) continue;
         const double c = cs[k], s = sn[k];
@@ -407,8 +407,8 @@ __global__ void __launch_bounds__(kBJThreads) k_bj_solve(const double* __restric
           S[q1 * n + p2] = cb * rc - sb * rd;
         }
       }
-      for (int e = tid; e < npairs * n; e += kBJThreads) {         // Q <- Q J
-        const int kq = e / n, i = e % n;
+      for (int e = tid; e < npairs * n; e += kBJThreads) {         // Q <- Q J, lanes over the planes
+        const int i = e / npairs, kq = e % npairs;
         const int p = pp[kq], q = qq[kq];
         const double c = cs[kq], s = sn[kq];
         const double vp = Q[i * n + p], vq = Q[i * n + q];
