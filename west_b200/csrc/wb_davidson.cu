@@ -234,6 +234,138 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double* __restrict__ hr, 
   for (int k = tid; k < nsel; k += nt) w[k] = A[idx[k] * n + idx[k]];
 }
 
+// Rotation of plane (p, q) that zeroes A[p][q]: t = tan(theta) from
+// cot(2 theta) = (a_qq - a_pp) / (2 a_pq), written as h sgn(d) / (|d| + sqrt(d^2 + h^2))
+// with d = a_qq - a_pp and h = 2 a_pq (one square root and one division).
+__device__ __forceinline__ void jacobi_rotation(const double* __restrict__ A, int ld, int p, int q, double& c,
+                                                double& s) {
+  const double apq = A[p * ld + q];
+  c = 1.0;
+  s = 0.0;
+  if (fabs(apq) > 1e-300) {
+    const double d = A[q * ld + q] - A[p * ld + p], h = 2.0 * apq;
+    const double t = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
+    c = rsqrt(fma(t, t, 1.0));
+    s = t * c;
+  }
+}
+
+// The same cyclic Jacobi for n <= kJacobiFastN with one barrier per round.  The
+// matrix is padded to ne = n + (n & 1) (the zero row and column of odd n never
+// rotate).  Thread (k1, k2) of the npairs^2 threads owns the 2 x 2 block of
+// planes k1, k2 and rows k2, k2 + npairs of plane k1's two columns of V
+// (column-major, so a warp's lanes touch consecutive rows).  Each thread derives
+// the rotations of its two planes from the previous round's matrix itself (the
+// lanes of a warp share k1) and writes the next matrix to the other buffer, so no
+// barrier separates the rotation parameters from the update; the planes of a
+// thread advance through the round-robin ordering by increments.
+constexpr int kJacobiFastN = 64;
+
+__host__ __device__ inline size_t jacobi_fast_bytes(int n) {
+  const int ne = n + (n & 1);
+  return 3 * sizeof(double) * ne * ne + sizeof(int) * n;
+}
+
+__global__ void __launch_bounds__(1024) k_jacobi_fast(const double* __restrict__ hr, long ldh, int n, int nsel,
+                                                      double* __restrict__ w, double* __restrict__ vr, long ldv,
+                                                      int* __restrict__ sweeps_out) {
+  extern __shared__ __align__(16) unsigned char shm[];
+  const int ne = n + (n & 1), np = ne / 2, m = ne - 1;
+  double* Ac = reinterpret_cast<double*>(shm);
+  double* An = Ac + ne * ne;
+  double* V = An + ne * ne;                          // V[col * ne + row]
+  int* idx = reinterpret_cast<int*>(V + ne * ne);    // [n]
+  __shared__ double red[2][32];
+  __shared__ int done;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < ne * ne; e += nt) {
+    const int i = e / ne, j = e % ne;
+    double a = 0.0;
+    if (i < n && j < n) a = (i <= j) ? hr[(long)j * ldh + i] : hr[(long)i * ldh + j];
+    Ac[e] = a;
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+  const bool act = tid < np * np;
+  const int k1 = act ? tid / np : 0, k2 = act ? tid % np : 0;
+  __syncthreads();
+  int sweep = 0;
+  for (; sweep < 60; ++sweep) {
+    double off = 0.0, dia = 0.0;
+    for (int e = tid; e < ne * ne; e += nt) {
+      const double v = Ac[e];
+      if (e / ne == e % ne) dia = fma(v, v, dia); else off = fma(v, v, off);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      dia += __shfl_xor_sync(0xffffffffu, dia, o);
+    }
+    if ((tid & 31) == 0) { red[0][tid >> 5] = off; red[1][tid >> 5] = dia; }
+    __syncthreads();
+    if (tid == 0) {
+      double to = 0.0, td = 0.0;
+      for (int i = 0; i < (nt + 31) / 32; ++i) { to += red[0][i]; td += red[1][i]; }
+      done = (to <= 1e-30 * (td + to)) ? 1 : 0;   // off-diagonal Frobenius norm below 1e-15 of the total
+    }
+    __syncthreads();
+    if (done) break;
+    // plane k of round r: (1 + (k - 1 + r) mod m, or 0 for k = 0) and 1 + (m - 1 - k + r) mod m
+    int xa1 = k1 > 0 ? k1 - 1 : 0, xb1 = m - 1 - k1;
+    int xa2 = k2 > 0 ? k2 - 1 : 0, xb2 = m - 1 - k2;
+    for (int r = 0; r < m; ++r) {
+      if (act) {
+        const int a1 = k1 > 0 ? 1 + xa1 : 0, b1 = 1 + xb1, a2 = k2 > 0 ? 1 + xa2 : 0, b2 = 1 + xb2;
+        const int p1 = min(a1, b1), q1 = max(a1, b1), p2 = min(a2, b2), q2 = max(a2, b2);
+        double ca, sa, cb, sb;
+        jacobi_rotation(Ac, ne, p1, q1, ca, sa);
+        jacobi_rotation(Ac, ne, p2, q2, cb, sb);
+        const double a = Ac[p1 * ne + p2], b = Ac[p1 * ne + q2], cc = Ac[q1 * ne + p2], d = Ac[q1 * ne + q2];
+        const double ra = ca * a - sa * cc, rc = sa * a + ca * cc;
+        const double rb = ca * b - sa * d, rd = sa * b + ca * d;
+        An[p1 * ne + p2] = cb * ra - sb * rb;
+        An[q1 * ne + q2] = sb * rc + cb * rd;
+        if (k1 == k2) {               // the plane's own pivot: zero by construction
+          An[p1 * ne + q2] = 0.0;
+          An[q1 * ne + p2] = 0.0;
+        } else {
+          An[p1 * ne + q2] = sb * ra + cb * rb;
+          An[q1 * ne + p2] = cb * rc - sb * rd;
+        }
+        double* vp = V + p1 * ne;
+        double* vq = V + q1 * ne;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = k2 + h * np;
+          const double x = vp[i], y = vq[i];
+          vp[i] = ca * x - sa * y;
+          vq[i] = sa * x + ca * y;
+        }
+      }
+      xa1 = xa1 + 1 == m ? 0 : xa1 + 1;
+      xb1 = xb1 + 1 == m ? 0 : xb1 + 1;
+      xa2 = xa2 + 1 == m ? 0 : xa2 + 1;
+      xb2 = xb2 + 1 == m ? 0 : xb2 + 1;
+      __syncthreads();
+      double* t = Ac; Ac = An; An = t;
+    }
+  }
+  for (int i = tid; i < n; i += nt) {   // rank of eigenvalue i (ascending, ties by index)
+    const double li = Ac[i * ne + i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double lj = Ac[j * ne + j];
+      rank += (lj < li || (lj == li && j < i)) ? 1 : 0;
+    }
+    if (rank < nsel) idx[rank] = i;
+  }
+  if (tid == 0) *sweeps_out = sweep;
+  __syncthreads();
+  for (int e = tid; e < nsel * n; e += nt) {
+    const int k = e / n, r = e % n;
+    vr[(long)k * ldv + r] = V[idx[k] * ne + r];
+  }
+  for (int k = tid; k < nsel; k += nt) w[k] = Ac[idx[k] * ne + idx[k]];
+}
+
 // ---------------------------------------------------------------------------
 // Parallel two-sided block Jacobi for bases above kJacobiSmemN (up to 1024)
 // ---------------------------------------------------------------------------
@@ -587,8 +719,8 @@ int block_jacobi(const double* hr, long ldh, int n, int nsel, double* w, double*
   return WB_OK;
 }
 
-// diagox_dsy (Wstat/wstat_tools.f90:48): the one-CTA shared-memory Jacobi up
-// to kJacobiSmemN, the block Jacobi above.  A and V: n^2 doubles each of
+// diagox_dsy (Wstat/wstat_tools.f90:48): the one-CTA shared-memory Jacobis up
+// to kJacobiFastN and kJacobiSmemN, the block Jacobi above.  A and V: n^2 doubles each of
 // global scratch (unused by the shared-memory path); bj: bj_doubles(n).
 int eigen_lowest(const double* hr, long ldh, int n, int nsel, double* w, double* vr, long ldv, double* A, double* V,
                  double* bj, int* sweeps, cudaStream_t s) {
@@ -597,6 +729,13 @@ int eigen_lowest(const double* hr, long ldh, int n, int nsel, double* w, double*
     double red[2];
     return block_jacobi(hr, ldh, n, nsel, w, vr, ldv, bj, red, &sw, s);
   }
+  if (n <= kJacobiFastN) {
+    const int np = (n + 1) / 2;
+    const int nt = std::max(32, (np * np + 31) / 32 * 32);
+    k_jacobi_fast<<<1, nt, jacobi_fast_bytes(n), s>>>(hr, ldh, n, nsel, w, vr, ldv, sweeps);
+    WB_CU(cudaGetLastError());
+    return WB_OK;
+  }
   const size_t shm = jacobi_pairs_bytes(n) + 2 * sizeof(double) * n * n;
   k_jacobi<<<1, 1024, shm, s>>>(hr, ldh, n, A, V, nsel, w, vr, ldv, sweeps, 1);
   WB_CU(cudaGetLastError());
@@ -604,6 +743,7 @@ int eigen_lowest(const double* hr, long ldh, int n, int nsel, double* w, double*
 }
 
 void jacobi_setup() {
+  cudaFuncSetAttribute(k_jacobi_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jacobi_fast_bytes(kJacobiFastN));
   cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(jacobi_pairs_bytes(kJacobiSmemN) + 2 * sizeof(double) * kJacobiSmemN * kJacobiSmemN));
 }
