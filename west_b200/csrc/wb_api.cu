@@ -1236,12 +1236,14 @@ int wb_ctx_destroy(wb_ctx* c) {
                   &c->X, &c->G, &c->T, &c->sticks, &c->sticks2, &c->acc, &c->part, &c->C, &c->rho, &c->conv,
                   &c->act, &c->items, &c->nact, &c->ecol, &c->epcol, &c->unconv, &c->items_pp, &c->items_pk,
                   &c->iota_items, &c->fcoef, &c->rt_colx, &c->twx, &c->twy, &c->twz, &c->twx32, &c->twy32, &c->twz32, &c->dav_dvg, &c->dav_dng, &c->dav_tmp, &c->dav_hr, &c->dav_vr, &c->dav_A,
-                  &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots, &c->dav_bj, &c->W32, &c->D32, &c->g2kin32,
+                  &c->dav_V, &c->dav_w, &c->dav_part, &c->dav_coef, &c->dav_dots, &c->dav_bj, &c->dav_st, &c->W32, &c->D32, &c->g2kin32,
                   &c->vs32, &c->tw32, &c->g32, &c->P32, &c->T32, &c->d32, &c->sticks32, &c->part32, &c->C32,
                   &c->ecol32, &c->rho0, &c->rho_in, &c->conv_in, &c->act_in, &c->items_in, &c->nact_in,
                   &c->umma_braket_w, &c->umma_update_w, &c->umma_err};
   c->loop64.release();
   c->loop32.release();
+  c->dav_graphs_release();
+  if (c->dav_host) cudaFreeHost(c->dav_host);
   for (DBuf* b : bufs) b->release();
   c->loopst.release();
   if (c->nact_host) cudaFreeHost(c->nact_host);

@@ -128,6 +128,23 @@ struct wb_ctx {
   DBuf dav_dvg, dav_dng, dav_tmp, dav_hr, dav_vr, dav_A, dav_V, dav_w, dav_part, dav_coef, dav_dots, dav_bj;
   wb_apply_fn dav_apply = nullptr;  // operator hook of the Davidson (wb_davidson_set_apply)
   void* dav_apply_user = nullptr;
+  // the Davidson's dense steps as CUDA graphs, one executable per phase, basis
+  // size, batch size and buffer set, most recently used first; dav_st holds the
+  // iteration's device state (unconverged count, conv flags, eigenvalues) and
+  // dav_host its pinned copy
+  struct DavGraph {
+    std::vector<long long> key;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<DavGraph> dav_graphs;
+  DBuf dav_st;
+  void* dav_host = nullptr;
+  size_t dav_host_bytes = 0;
+  void dav_graphs_release() {
+    for (DavGraph& g : dav_graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    dav_graphs.clear();
+  }
   // device address of the allocation-free entry point's scratch array, looked
   // up on this context's first such call (null until then)
   void* noalloc_base = nullptr;

@@ -748,6 +748,111 @@ void jacobi_setup() {
                        (int)(jacobi_pairs_bytes(kJacobiSmemN) + 2 * sizeof(double) * kJacobiSmemN * kJacobiSmemN));
 }
 
+// ---------------------------------------------------------------------------
+// Iteration state on the device: st[0] = number of unconverged eigenpairs,
+// st[1 + i] = conv(i), and ev(i) at dav_ev_offset(nvec) bytes.
+// ---------------------------------------------------------------------------
+inline size_t dav_ev_offset(int nvec) { return ((size_t)(1 + nvec) * sizeof(int) + 7) / 8 * 8; }
+inline size_t dav_state_bytes(int nvec) { return dav_ev_offset(nvec) + sizeof(double) * nvec; }
+
+// Reordering of davidson_diago.f90:273-296 (redistribute_vr_distr): the j-th
+// unconverged index n (conv(n) = 0, ascending) moves vr(:, n) to vr(:, nbase + j)
+// and ev(n) to w(nbase + j).  One CTA per new column; its first warp finds n by
+// ballots over conv.  Sources (n < nvec <= nbase) and targets never overlap.
+__global__ void __launch_bounds__(256) k_dav_shift(const int* __restrict__ st, const double* __restrict__ ev, int nvec,
+                                                   int nbase, double* __restrict__ vr, long ldv, int nrow,
+                                                   double* __restrict__ w) {
+  const int* conv = st + 1;
+  const int j = blockIdx.x;
+  __shared__ int src;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int base = 0, found = -1;
+    for (int n0 = 0; n0 < nvec && found < 0; n0 += 32) {
+      const int n = n0 + lane;
+      const unsigned b = __ballot_sync(0xffffffffu, n < nvec && conv[n] == 0);
+      const int cnt = __popc(b);
+      if (j < base + cnt) {
+        unsigned bb = b;
+        for (int t = 0; t < j - base; ++t) bb &= bb - 1;
+        found = n0 + __ffs(bb) - 1;
+      }
+      base += cnt;
+    }
+    if (lane == 0) src = found;
+  }
+  __syncthreads();
+  const int n = src;
+  if (n < 0) return;
+  if (threadIdx.x == 0) w[nbase + j] = ev[n];
+  for (int r = threadIdx.x; r < nrow; r += blockDim.x) vr[(long)(nbase + j) * ldv + r] = vr[(long)n * ldv + r];
+}
+
+// Convergence test of davidson_diago.f90:346-347 on the new Ritz values w
+// against ev (test = 1; the extra starting step only copies), then ev <- w and
+// st[0] = number not converged.  One CTA.
+__global__ void __launch_bounds__(256) k_dav_conv(const double* __restrict__ w, double* __restrict__ ev,
+                                                  int* __restrict__ st, int nvec, double trev, double trev_rel,
+                                                  int test) {
+  int* conv = st + 1;
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+    const double e = w[i], o = ev[i];
+    if (test) conv[i] = (fabs((e - o) / o) < trev_rel) && (fabs(e - o) < trev) ? 1 : 0;
+    mine += conv[i] ? 0 : 1;
+    ev[i] = e;
+  }
+  atomicAdd(&cnt, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) st[0] = cnt;
+}
+
+constexpr size_t kMaxDavGraphs = 64;
+
+// Runs body (stream work only) on s: eagerly without graphs, else from the
+// cached executable of key, capturing and instantiating it on a miss.
+template <class F>
+int dav_graph(wb_ctx* c, cudaStream_t s, const std::vector<long long>& key, F body) {
+  if (!c->use_graphs) return body();
+  auto& gs = c->dav_graphs;
+  for (size_t i = 0; i < gs.size(); ++i)
+    if (gs[i].key == key) {
+      std::rotate(gs.begin(), gs.begin() + i, gs.begin() + i + 1);
+      WB_CU(cudaGraphLaunch(gs[0].exec, s));
+      return WB_OK;
+    }
+  WB_CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const int rc = body();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(WB_ERR_CUDA, std::string("Davidson graph capture: ") + cudaGetErrorString(e));
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return fail(WB_ERR_CUDA, std::string("Davidson graph instantiation: ") + cudaGetErrorString(ei));
+  if (gs.size() >= kMaxDavGraphs) {
+    cudaGraphExecDestroy(gs.back().exec);
+    gs.pop_back();
+  }
+  gs.insert(gs.begin(), wb_ctx::DavGraph{key, ex});
+  WB_CU(cudaGraphLaunch(ex, s));
+  return WB_OK;
+}
+
+inline long long key_bits(double x) {
+  long long b;
+  std::memcpy(&b, &x, sizeof(b));
+  return b;
+}
+inline long long key_ptr(const void* p) { return (long long)(intptr_t)p; }
+
 struct Dav {
   wb_ctx* c;
   int npw, nvec, nvecx;
@@ -817,10 +922,64 @@ struct Dav {
     return WB_OK;
   }
   double* bj = nullptr;  // block Jacobi scratch (bases above kJacobiSmemN)
-  int diagox(int nbase, std::vector<double>& ew_host) {  // lowest nvec eigenpairs of hr[:nbase, :nbase]
-    int rc = eigen_lowest(hr, nvecx, nbase, nvec, w, vr, nvecx, A, V, bj, sweeps, s);
+  int* st = nullptr;     // device state (dav_ev_offset layout)
+  double* ev = nullptr;
+  unsigned char* host = nullptr;  // its pinned copy
+  double trev = 0.0, trev_rel = 0.0;
+  // Steps before the operator (davidson_diago.f90:273-306): move the
+  // unconverged Ritz pairs behind the basis, update_with_vr_distr, do_mgs.
+  int pre(int nbase, int notcnv) {
+    const std::vector<long long> key = {0, nbase, notcnv, nvec, nvecx, ld, nsplit, key_ptr(dvg), key_ptr(dng),
+                                        key_ptr(vr), key_ptr(w), key_ptr(coef), key_ptr(part), key_ptr(dots),
+                                        key_ptr(st)};
+    return dav_graph(c, s, key, [&]() -> int {
+      k_dav_shift<<<notcnv, 256, 0, s>>>(st, ev, nvec, nbase, vr, nvecx, nvecx, w);
+      const int K = 2 * npw;
+      double* c1 = coef;
+      double* c2 = coef + (size_t)nvecx * nvecx;
+      k_vr_coef<<<notcnv, 256, 0, s>>>(vr, nvecx, nbase, nbase, notcnv, w, c1, c2);
+      double* y = reinterpret_cast<double*>(dvg + (long)nbase * ld);
+      gemm_nn(reinterpret_cast<const double*>(dvg), 2 * ld, nbase, c1, y, 2 * ld, nullptr, notcnv, K, 0.0, s);
+      gemm_nn(reinterpret_cast<const double*>(dng), 2 * ld, nbase, c2, y, 2 * ld, nullptr, notcnv, K, 1.0, s);
+      WB_CU(cudaGetLastError());
+      return mgs(nbase, nbase + notcnv);
+    });
+  }
+  // Steps after the operator (:331-347): build_hr of the new columns, diagox of
+  // hr[:nbase + notcnv, :nbase + notcnv], the convergence test (test = 0: the
+  // extra starting step, ev <- ew only) and the copy of the state to the host;
+  // waits for it.  The block Jacobi above kJacobiSmemN reads its convergence
+  // norms on the host, so those bases run these steps eagerly.
+  int post(int nbase, int notcnv, int test) {
+    const int n = nbase + notcnv;
+    const std::vector<long long> key = {1, nbase, notcnv, test, nvec, nvecx, ld, nsplit, key_ptr(dvg), key_ptr(dng),
+                                        key_ptr(hr), key_ptr(vr), key_ptr(A), key_ptr(V), key_ptr(w), key_ptr(part),
+                                        key_ptr(st), key_ptr(host), key_bits(trev), key_bits(trev_rel)};
+    auto body = [&]() -> int {
+      int rc = build_hr(nbase, n, n);
+      if (rc) return rc;
+      if ((rc = eigen_lowest(hr, nvecx, n, nvec, w, vr, nvecx, A, V, bj, sweeps, s))) return rc;
+      k_dav_conv<<<1, 256, 0, s>>>(w, ev, st, nvec, trev, trev_rel, test);
+      WB_CU(cudaMemcpyAsync(host, st, dav_state_bytes(nvec), cudaMemcpyDeviceToHost, s));
+      WB_CU(cudaGetLastError());
+      return WB_OK;
+    };
+    const int rc = n > kJacobiSmemN ? body() : dav_graph(c, s, key, body);
     if (rc) return rc;
-    WB_CU(cudaMemcpyAsync(ew_host.data(), w, sizeof(double) * nvec, cudaMemcpyDeviceToHost, s));
+    WB_CU(cudaStreamSynchronize(s));
+    return WB_OK;
+  }
+  int unconverged() const { return reinterpret_cast<const int*>(host)[0]; }
+  int conv_at(int i) const { return reinterpret_cast<const int*>(host)[1 + i]; }
+  double ev_at(int i) const { return reinterpret_cast<const double*>(host + dav_ev_offset(nvec))[i]; }
+  // host conv/ev -> device state (start and resumption)
+  int upload(const std::vector<int>& conv_h, const std::vector<double>& ev_h) {
+    int* hi = reinterpret_cast<int*>(host);
+    int cnt = 0;
+    for (int i = 0; i < nvec; ++i) { hi[1 + i] = conv_h[i]; cnt += conv_h[i] ? 0 : 1; }
+    hi[0] = cnt;
+    std::memcpy(host + dav_ev_offset(nvec), ev_h.data(), sizeof(double) * nvec);
+    WB_CU(cudaMemcpyAsync(st, host, dav_state_bytes(nvec), cudaMemcpyHostToDevice, s));
     WB_CU(cudaStreamSynchronize(s));
     return WB_OK;
   }
@@ -893,12 +1052,29 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
   d.part = c->dav_part.as<double>();
   d.coef = c->dav_coef.as<double>();
   d.dots = c->dav_dots.as<double>();
+  const size_t stb = dav_state_bytes(nvec);
+  if (c->dav_st.ensure(stb)) return fail(WB_ERR_NOMEM, "device allocation of the Davidson state failed");
+  if (c->dav_host_bytes < stb) {
+    if (c->dav_host) cudaFreeHost(c->dav_host);
+    c->dav_host = nullptr;
+    c->dav_host_bytes = 0;
+    if (cudaMallocHost(&c->dav_host, stb) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(WB_ERR_NOMEM, "pinned host allocation of the Davidson state failed");
+    }
+    c->dav_host_bytes = stb;
+  }
+  d.st = c->dav_st.as<int>();
+  d.ev = reinterpret_cast<double*>(c->dav_st.as<unsigned char>() + dav_ev_offset(nvec));
+  d.host = static_cast<unsigned char*>(c->dav_host);
+  d.trev = p->trev_pdep;
+  d.trev_rel = p->trev_pdep_rel;
   cudaStream_t s = d.s;
   WB_CU(cudaMemsetAsync(d.dvg, 0, colb * nvecx, s));
   WB_CU(cudaMemsetAsync(d.dng, 0, colb * nvecx, s));
   WB_CU(cudaMemsetAsync(d.hr, 0, sizeof(double) * nvecx * nvecx, s));
   WB_CU(cudaMemsetAsync(d.vr, 0, sizeof(double) * nvecx * nvecx, s));
-  std::vector<double> ew(nvecx, 0.0), ev(nvec, 0.0), wtmp(nvec);
+  std::vector<double> ew(nvecx, 0.0), ev(nvec, 0.0);
   std::vector<int> conv(nvec, 0);
   int nbase = nvec, notcnv = nvec, rc;
   int dav_iter = -2;
@@ -945,49 +1121,30 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
     dav_iter = -1;
     if (nsw == 1 && (rc = checkpoint())) return rc;
   }
+  if ((rc = d.upload(conv, ev))) return rc;
   if (dav_iter == -1) {                                                    // extra starting step (:204-247)
     WB_CU(cudaMemcpyAsync(d.dvg, d.dng, colb * nvecx, cudaMemcpyDeviceToDevice, s));   // dvg = dng
     if ((rc = d.mgs(0, nvec))) return rc;
     if ((rc = d.apply(0, nvec, std::min(1e-4, 1e8 * p->tr2_dfpt)))) return rc;
-    if ((rc = d.build_hr(0, nvec, nvec))) return rc;
-    if ((rc = d.diagox(nbase, wtmp))) return rc;
-    for (int i = 0; i < nvec; ++i) ew[i] = ev[i] = wtmp[i];
+    if ((rc = d.post(0, nvec, 0))) return rc;                              // build_hr, diagox, ev = ew
+    for (int i = 0; i < nvec; ++i) ew[i] = ev[i] = d.ev_at(i);
     dav_iter = 0;
     if (nsw == 1 && (rc = checkpoint())) return rc;
   }
   bool refreshed = false;
   for (int kter = 1; kter <= p->n_pdep_maxiter; ++kter) {                 // :259
     ++dav_iter;
-    std::vector<int> ishift(nvecx, 0);
-    int np_ = 0;
-    for (int n = 0; n < nvec; ++n)                                        // :273-296
-      if (!conv[n]) { ishift[nbase + np_] = n; ew[nbase + np_] = ev[n]; ++np_; }
-    for (int j = nbase; j < nbase + notcnv; ++j)                          // redistribute_vr_distr
-      WB_CU(cudaMemcpyAsync(d.vr + (long)j * nvecx, d.vr + (long)ishift[j] * nvecx, sizeof(double) * nvecx,
-                            cudaMemcpyDeviceToDevice, s));
-    WB_CU(cudaMemcpyAsync(d.w, ew.data(), sizeof(double) * nvecx, cudaMemcpyHostToDevice, s));
-    {                                                                      // update_with_vr_distr
-      const int K = 2 * d.npw;
-      double* c1 = d.coef;
-      double* c2 = d.coef + (size_t)nvecx * nvecx;
-      k_vr_coef<<<notcnv, 256, 0, s>>>(d.vr, nvecx, nbase, nbase, notcnv, d.w, c1, c2);
-      double* y = reinterpret_cast<double*>(d.dvg + (long)nbase * d.ld);
-      gemm_nn(reinterpret_cast<const double*>(d.dvg), 2 * d.ld, nbase, c1, y, 2 * d.ld, nullptr, notcnv, K, 0.0, s);
-      gemm_nn(reinterpret_cast<const double*>(d.dng), 2 * d.ld, nbase, c2, y, 2 * d.ld, nullptr, notcnv, K, 1.0, s);
-      WB_CU(cudaGetLastError());
-    }
-    if ((rc = d.mgs(nbase, nbase + notcnv))) return rc;                   // :306
+    for (int n = 0, np_ = 0; n < nvec; ++n)                               // :273-296, host copy of ew
+      if (!conv[n]) ew[nbase + np_++] = ev[n];
+    if ((rc = d.pre(nbase, notcnv))) return rc;                           // :273-306 on the device
     if ((rc = d.apply(nbase, notcnv, p->tr2_dfpt))) return rc;             // :324
-    if ((rc = d.build_hr(nbase, nbase + notcnv, nbase + notcnv))) return rc;   // :331
+    if ((rc = d.post(nbase, notcnv, 1))) return rc;                        // :331-347
     nbase += notcnv;
-    if ((rc = d.diagox(nbase, wtmp))) return rc;                          // :340
-    for (int i = 0; i < nvec; ++i) ew[i] = wtmp[i];
-    notcnv = 0;
-    for (int i = 0; i < nvec; ++i) {                                      // :346-347
-      conv[i] = (std::fabs((ew[i] - ev[i]) / ev[i]) < p->trev_pdep_rel) && (std::fabs(ew[i] - ev[i]) < p->trev_pdep);
-      notcnv += conv[i] ? 0 : 1;
+    notcnv = d.unconverged();
+    for (int i = 0; i < nvec; ++i) {
+      conv[i] = d.conv_at(i);
+      ev[i] = ew[i] = d.ev_at(i);
     }
-    for (int i = 0; i < nvec; ++i) ev[i] = ew[i];
     if (notcnv == 0 || nbase + notcnv > nvecx || kter == p->n_pdep_maxiter) {
       if (notcnv == 0 || kter == p->n_pdep_maxiter) {
         if ((rc = d.refresh(d.dvg, nbase, nvec))) return rc;              // eigenvectors for the caller
