@@ -22,7 +22,9 @@ def _solve(op, dvg0, nvec, times, maxiter=100):
                        trev_pdep_rel=1e-1)
 
 
-@pytest.mark.parametrize("nvec,times", [(4, 4), (2, 2)])  # (2, 2): the basis refresh of :390-414
+# (2, 2): the basis refresh of :390-414; (32, 4): a basis of 128, whose diagox is
+# the block Jacobi with its sweep loop in a conditional WHILE node of the graph
+@pytest.mark.parametrize("nvec,times", [(4, 4), (2, 2), (32, 4)])
 def test_davidson_graphs_replay_and_eager(small, nvec, times):
     from west_b200.wstat import ResponseOperator
     s = small

@@ -1244,6 +1244,7 @@ int wb_ctx_destroy(wb_ctx* c) {
   c->loop32.release();
   c->dav_graphs_release();
   if (c->dav_host) cudaFreeHost(c->dav_host);
+  if (c->dav_aux) cudaStreamDestroy(c->dav_aux);
   for (DBuf* b : bufs) b->release();
   c->loopst.release();
   if (c->nact_host) cudaFreeHost(c->nact_host);

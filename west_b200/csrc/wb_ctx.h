@@ -138,6 +138,7 @@ struct wb_ctx {
   };
   std::vector<DavGraph> dav_graphs;
   DBuf dav_st;
+  cudaStream_t dav_aux = nullptr;  // second stream for captures that add conditional nodes
   void* dav_host = nullptr;
   size_t dav_host_bytes = 0;
   void dav_graphs_release() {

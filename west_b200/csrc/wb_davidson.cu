@@ -447,6 +447,24 @@ __global__ void k_bj_norms_final(const double* __restrict__ part, int nparts, do
   }
 }
 
+// k_bj_norms_final for the sweep loop of a CUDA graph: also counts the sweeps
+// (first: the check before any) and sets the loop's WHILE condition to the
+// host loop's test (continue while the off-diagonal norm exceeds 1e-14 of the
+// whole and fewer than 40 sweeps ran).
+__global__ void k_bj_norms_cond(const double* __restrict__ part, int nparts, double* __restrict__ red,
+                                cudaGraphConditionalHandle h, int first) {
+  if (threadIdx.x == 0) {
+    double so = 0.0, st = 0.0;
+    for (int i = 0; i < nparts; ++i) { so += part[2 * i]; st += part[2 * i + 1]; }
+    red[0] = so;
+    red[1] = st;
+    int* sweep = reinterpret_cast<int*>(red + 2);
+    const int sw = first ? 0 : *sweep + 1;
+    *sweep = sw;
+    cudaGraphSetConditional(h, (!(so <= 1e-28 * st) && sw < 40) ? 1u : 0u);
+  }
+}
+
 // One CTA per block pair of round r: U_P (row-major, U[l][m]) of the pair's
 // 2 kBJ x 2 kBJ submatrix, or the identity with skip[k] = 1.
 __global__ void __launch_bounds__(kBJThreads) k_bj_solve(const double* __restrict__ A, int npad, int nb, int r,
@@ -676,41 +694,93 @@ size_t bj_doubles(int nmax) {
   int nb = (nmax + kBJ - 1) / kBJ;
   nb += nb & 1;
   const size_t npad = (size_t)nb * kBJ;
-  return 2 * npad * npad + (size_t)(nb / 2) * kBJ2 * kBJ2 + 2 + nmax + nb + 2 * kBJNormCtas;
+  return 2 * npad * npad + (size_t)(nb / 2) * kBJ2 * kBJ2 + 4 + nmax + nb + 2 * kBJNormCtas;
+}
+
+// One sweep: nb - 1 rounds of block-pair solves and tile rotations.
+void bj_sweep(double* A, double* V, double* U, const double* red, int* skip, int npad, int nb, double skip_frac,
+              cudaStream_t s) {
+  const int npair = nb / 2;
+  for (int r = 0; r < nb - 1; ++r) {
+    k_bj_solve<<<npair, kBJThreads, 0, s>>>(A, npad, nb, r, red, U, skip, skip_frac);
+    k_bj_apply_a<<<dim3(npair, npair), kBJThreads, 0, s>>>(A, npad, nb, r, U, skip);
+    k_bj_apply_v<<<dim3(npad / kBJ2, npair), kBJThreads, 0, s>>>(V, npad, nb, r, U, skip);
+  }
 }
 
 // Lowest nsel eigenpairs of the symmetric hr[:n, :n] (upper triangle, column
 // major, ld ldh): w (device, ascending) and vr(:, 0:nsel) (device, ld ldv).
-// scratch holds bj_doubles(n); red2 is pinned host memory for two doubles.
+// scratch holds bj_doubles(n).  Run eagerly, the sweeps stop on norms read by
+// the host (red_host: two doubles); while s is being captured into a CUDA graph
+// they run inside a conditional WHILE node whose condition k_bj_norms_cond sets
+// from the same test, the sweeps' kernels captured on the idle stream aux into
+// the node's body (nodes added to the capture graph as cudaStreamGetCaptureInfo /
+// cudaStreamUpdateCaptureDependencies provide).  Both forms launch the same
+// kernels in the same order.
 int block_jacobi(const double* hr, long ldh, int n, int nsel, double* w, double* vr, long ldv, double* scratch,
-                 double* red_host, int* sweeps_out, cudaStream_t s) {
+                 double* red_host, int* sweeps_out, cudaStream_t s, cudaStream_t aux) {
   int nb = (n + kBJ - 1) / kBJ;
   nb += nb & 1;
   const int npad = nb * kBJ, npair = nb / 2;
   double* A = scratch;
   double* V = A + (size_t)npad * npad;
   double* U = V + (size_t)npad * npad;
-  double* red = U + (size_t)npair * kBJ2 * kBJ2;
-  double* npart = red + 2;                     // per-CTA partial norms
+  double* red = U + (size_t)npair * kBJ2 * kBJ2;  // red[0..1] norms, red[2] the sweep count of the graph form
+  double* npart = red + 4;                     // per-CTA partial norms
   int* iw = reinterpret_cast<int*>(npart + 2 * kBJNormCtas);  // skip flags, then the selection indices
   int* skip = iw;
   int* idx = iw + nb;
   const int g = std::min(kBJNormCtas, (int)(((long)npad * npad + 255) / 256));
   const double skip_frac = 1e-30 / (0.5 * nb * (nb - 1));
-  k_bj_init<<<g, 256, 0, s>>>(hr, ldh, n, npad, A, V);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  WB_CU(cudaStreamIsCapturing(s, &cs));
   int sweep = 0;
-  for (;; ++sweep) {
+  if (cs == cudaStreamCaptureStatusActive) {
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    WB_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, nullptr, nullptr));
+    cudaGraphConditionalHandle h;
+    WB_CU(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
+    k_bj_init<<<g, 256, 0, s>>>(hr, ldh, n, npad, A, V);
     k_bj_norms<<<g, 256, 0, s>>>(A, npad, npart);
-    k_bj_norms_final<<<1, 32, 0, s>>>(npart, g, red);
-    WB_CU(cudaMemcpyAsync(red_host, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    WB_CU(cudaStreamSynchronize(s));
-    if (red_host[0] <= 1e-28 * red_host[1] || sweep == 40) break;
-    for (int r = 0; r < nb - 1; ++r) {
-      k_bj_solve<<<npair, kBJThreads, 0, s>>>(A, npad, nb, r, red, U, skip, skip_frac);
-      k_bj_apply_a<<<dim3(npair, npair), kBJThreads, 0, s>>>(A, npad, nb, r, U, skip);
-      k_bj_apply_v<<<dim3(npad / kBJ2, npair), kBJThreads, 0, s>>>(V, npad, nb, r, U, skip);
-    }
+    k_bj_norms_cond<<<1, 32, 0, s>>>(npart, g, red, h, 1);
     WB_CU(cudaGetLastError());
+    WB_CU(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = h;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    WB_CU(cudaGraphAddNode(&wnode, cg, deps, nd, &wp));
+    WB_CU(cudaStreamUpdateCaptureDependencies(s, &wnode, 1, cudaStreamSetCaptureDependencies));
+    if (!aux) return fail(WB_ERR_ARG, "block Jacobi capture needs a second stream");
+    cudaStream_t s2 = aux;
+    cudaError_t e = cudaStreamBeginCaptureToGraph(s2, wp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      bj_sweep(A, V, U, red, skip, npad, nb, skip_frac, s2);
+      k_bj_norms<<<g, 256, 0, s2>>>(A, npad, npart);
+      k_bj_norms_cond<<<1, 32, 0, s2>>>(npart, g, red, h, 0);
+      e = cudaGetLastError();
+      cudaGraph_t bg = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(s2, &bg);
+      if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) return fail(WB_ERR_CUDA, std::string("block Jacobi sweep capture: ") + cudaGetErrorString(e));
+    sweep = -1;  // counted on the device
+  } else {
+    k_bj_init<<<g, 256, 0, s>>>(hr, ldh, n, npad, A, V);
+    for (;; ++sweep) {
+      k_bj_norms<<<g, 256, 0, s>>>(A, npad, npart);
+      k_bj_norms_final<<<1, 32, 0, s>>>(npart, g, red);
+      WB_CU(cudaMemcpyAsync(red_host, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      WB_CU(cudaStreamSynchronize(s));
+      if (red_host[0] <= 1e-28 * red_host[1] || sweep == 40) break;
+      bj_sweep(A, V, U, red, skip, npad, nb, skip_frac, s);
+      WB_CU(cudaGetLastError());
+    }
   }
   k_bj_select<<<1, 1024, 0, s>>>(A, V, n, npad, nsel, w, vr, ldv, idx);
   k_bj_rayleigh<<<nsel, 256, 0, s>>>(hr, ldh, n, vr, ldv, w);
@@ -721,13 +791,14 @@ int block_jacobi(const double* hr, long ldh, int n, int nsel, double* w, double*
 
 // diagox_dsy (Wstat/wstat_tools.f90:48): the one-CTA shared-memory Jacobis up
 // to kJacobiFastN and kJacobiSmemN, the block Jacobi above.  A and V: n^2 doubles each of
-// global scratch (unused by the shared-memory path); bj: bj_doubles(n).
+// global scratch (unused by the shared-memory path); bj: bj_doubles(n); aux: a
+// second stream, needed when s is being captured and n > kJacobiSmemN.
 int eigen_lowest(const double* hr, long ldh, int n, int nsel, double* w, double* vr, long ldv, double* A, double* V,
-                 double* bj, int* sweeps, cudaStream_t s) {
+                 double* bj, int* sweeps, cudaStream_t s, cudaStream_t aux = nullptr) {
   if (n > kJacobiSmemN) {
     int sw = 0;
     double red[2];
-    return block_jacobi(hr, ldh, n, nsel, w, vr, ldv, bj, red, &sw, s);
+    return block_jacobi(hr, ldh, n, nsel, w, vr, ldv, bj, red, &sw, s, aux);
   }
   if (n <= kJacobiFastN) {
     const int np = (n + 1) / 2;
@@ -862,6 +933,7 @@ struct Dav {
   int* sweeps;
   int nsplit;
   cudaStream_t s;
+  cudaStream_t aux = nullptr;  // second stream of the block Jacobi's graph form
   int apply_calls = 0;
   long long applied = 0;
   std::vector<int> unconv;
@@ -948,8 +1020,7 @@ struct Dav {
   // Steps after the operator (:331-347): build_hr of the new columns, diagox of
   // hr[:nbase + notcnv, :nbase + notcnv], the convergence test (test = 0: the
   // extra starting step, ev <- ew only) and the copy of the state to the host;
-  // waits for it.  The block Jacobi above kJacobiSmemN reads its convergence
-  // norms on the host, so those bases run these steps eagerly.
+  // waits for it.
   int post(int nbase, int notcnv, int test) {
     const int n = nbase + notcnv;
     const std::vector<long long> key = {1, nbase, notcnv, test, nvec, nvecx, ld, nsplit, key_ptr(dvg), key_ptr(dng),
@@ -958,13 +1029,13 @@ struct Dav {
     auto body = [&]() -> int {
       int rc = build_hr(nbase, n, n);
       if (rc) return rc;
-      if ((rc = eigen_lowest(hr, nvecx, n, nvec, w, vr, nvecx, A, V, bj, sweeps, s))) return rc;
+      if ((rc = eigen_lowest(hr, nvecx, n, nvec, w, vr, nvecx, A, V, bj, sweeps, s, aux))) return rc;
       k_dav_conv<<<1, 256, 0, s>>>(w, ev, st, nvec, trev, trev_rel, test);
       WB_CU(cudaMemcpyAsync(host, st, dav_state_bytes(nvec), cudaMemcpyDeviceToHost, s));
       WB_CU(cudaGetLastError());
       return WB_OK;
     };
-    const int rc = n > kJacobiSmemN ? body() : dav_graph(c, s, key, body);
+    const int rc = dav_graph(c, s, key, body);
     if (rc) return rc;
     WB_CU(cudaStreamSynchronize(s));
     return WB_OK;
@@ -1029,6 +1100,9 @@ extern "C" int wb_davidson(wb_ctx* c, const wb_davidson_params* p, const double*
   d.nvec = nvec;
   d.nvecx = nvecx;
   d.s = c->stream;
+  if (nvecx > kJacobiSmemN && c->use_graphs && !c->dav_aux)
+    WB_CU(cudaStreamCreateWithFlags(&c->dav_aux, cudaStreamNonBlocking));
+  d.aux = c->dav_aux;
   d.nsplit = gemm_tn_splits(nvecx, nvecx, 2 * c->npw);
   const size_t colb = sizeof(double2) * d.ld;
   if (c->dav_dvg.ensure(colb * nvecx) || c->dav_dng.ensure(colb * nvecx) || c->dav_tmp.ensure(colb * nvecx) ||
