@@ -168,11 +168,13 @@ typedef struct wb_tuning {
 int wb_get_tuning(const wb_ctx* ctx, wb_tuning* out);
 int wb_set_autotune(wb_ctx* ctx, int enable);
 
-/* CUDA graphs for the PCG loops: 1 (default) runs each batch's masked PCG
- * loop from one graph launch whose conditional WHILE node tests convergence on
- * the device; 0 runs it eagerly, reading the active count back to the host
- * every iteration.  Stage profiling always runs eagerly.  Same results either
- * way. */
+/* CUDA graphs: 1 (default) runs each batch's masked PCG loop from one graph
+ * launch whose conditional WHILE node tests convergence on the device, and each
+ * wb_davidson iteration's dense steps as two cached graph launches around the
+ * operator call; 0 runs both eagerly, reading the PCG's active count back to the
+ * host every iteration.  Stage profiling always runs the PCG loop eagerly.  The
+ * same results either way, to rounding (the eager PCG may split its GEMMs
+ * differently). */
 int wb_set_graphs(wb_ctx* ctx, int enable);
 
 /*

@@ -100,7 +100,8 @@ class ResponseOperator:
         _lib.check(self._lib.wb_set_profiling(self._ctx, mask))
 
     def set_graphs(self, enable: bool = True):
-        """Run each batch's PCG loop from one CUDA graph launch (default) or eagerly."""
+        """Run each batch's PCG loop from one CUDA graph launch and each Davidson
+        iteration's dense steps from two cached graphs (default), or both eagerly."""
         _lib.check(self._lib.wb_set_graphs(self._ctx, int(bool(enable))))
 
     def set_autotune(self, enable: bool = True):
