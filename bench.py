@@ -304,10 +304,14 @@ def run_b200(args, rank, world, local_rank):
     op.apply_operator(m, dvg_np, dng_np, TR2)   # untimed: sizes the host staging buffers
     barrier(); torch.cuda.synchronize()
     t_e2e0 = time.perf_counter()
+    e2e_marks, e2e_lib = [], []
     for _ in range(args.steps):
         op.apply_operator(m, dvg_np, dng_np, TR2)
+        e2e_marks.append(time.perf_counter())
+        e2e_lib.append(round(op.stats()["ms_total"], 2))
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t_e2e0)
+    e2e_steps = [round(1e3 * (b - a), 2) for a, b in zip([t_e2e0] + e2e_marks[:-1], e2e_marks)]
     barrier()
     e2e_val = world * m * args.steps / e2e_s
     e2e_ok = bool(np.allclose(dng_np, dng_val, rtol=0, atol=1e-12 * np.abs(dng_val).max()))
@@ -350,7 +354,8 @@ def run_b200(args, rank, world, local_rank):
                                      "step_ms": step_ms, "settle_steps": int(settle)}),
             "clocks": clk.summary(),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(m * npw * 16),
-                    "d2h_bytes_per_step": int(m * npw * 16), "matches_device_path": e2e_ok},
+                    "d2h_bytes_per_step": int(m * npw * 16), "matches_device_path": e2e_ok,
+                    "step_ms": e2e_steps, "library_ms": e2e_lib},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "kernel": "vloc FFT stage (k_zinv + k_plane_vloc + k_zfwd), per launch",
                          "timed_over": f"{args.steps} steps of the same workload right after the timed region, "
