@@ -120,6 +120,7 @@ struct wb_ctx {
   cudaEvent_t tev0 = nullptr, tev1 = nullptr;
   DBuf loopst;               // int[8] loop state (wb_la.cu loop_init / loop_ctl)
   int* loop_host = nullptr;  // pinned copy of it
+  int loop_pending = 0;      // launches per pass of a graph run whose counters await the batch's wait
   // tensor-core GEMMs of the mixed form: W split into bf16 hi/lo tiles, and the
   // error word their bounded waits write
   int umma = 0, umma_M = 0;
