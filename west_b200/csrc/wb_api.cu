@@ -800,7 +800,7 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
       cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
     }
     if (graph) WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    WB_CU(cudaStreamSynchronize(s));
+    WB_CU(wb_wait(c));
     nact = *c->nact_host;
     if (graph) inner_total = c->loop_host[3];
     if (nact == 0 || outer == kMaxRefinements - 1) break;
@@ -847,15 +847,16 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
   }
   if (graph) {
     WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    WB_CU(cudaStreamSynchronize(s));
+    WB_CU(wb_wait(c));
     inner_total = c->loop_host[3];
     loop_stats(c, inner_total, c->kinetic_only ? 6 : 9);
   }
   *iters_out = inner_total;
   if (c->umma) {  // a bounded wait of a tensor-core GEMM that ran out leaves its code here
-    int e = 0;
-    WB_CU(cudaMemcpyAsync(&e, c->umma_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    WB_CU(cudaStreamSynchronize(s));
+    int* eh = c->nact_host + 1;  // a pinned slot (nact_host[0] is the active count)
+    WB_CU(cudaMemcpyAsync(eh, c->umma_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    WB_CU(wb_wait(c));
+    const int e = *eh;
     if (e) {
       cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), s);
       return fail(WB_ERR_CUDA, "tensor-core GEMM wait limit reached (code " + std::to_string(e) + ")");
@@ -864,8 +865,7 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
   return WB_OK;
 }
 
-int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, long ld_out, double tr2,
-              int* unconv_host) {
+int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, long ld_out, double tr2) {
   cudaStream_t s = c->stream;
   const int npw = c->npw, nocc = c->nocc, npv = c->npv;
   const int nsys = mb * nocc;
@@ -876,8 +876,16 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
   std::vector<int2> ipp, ipk;
   pair_items(ipp, 0, mb);
   for (int p = 0; p < mb; ++p) pair_items(ipk, p * nocc, nocc);
-  WB_CU(cudaMemcpyAsync(c->items_pp.p, ipp.data(), sizeof(int2) * ipp.size(), cudaMemcpyHostToDevice, s));
-  WB_CU(cudaMemcpyAsync(c->items_pk.p, ipk.data(), sizeof(int2) * ipk.size(), cudaMemcpyHostToDevice, s));
+  {  // through the pinned staging area, after the unconverged counts' slots
+    const size_t off = ((size_t)mb * sizeof(int) + 15) / 16 * 16;
+    if (c->ensure_pin(off + sizeof(int2) * (ipp.size() + ipk.size())))
+      return fail(WB_ERR_NOMEM, "pinned host allocation failed");
+    int2* hp = reinterpret_cast<int2*>(c->pin + off);
+    std::memcpy(hp, ipp.data(), sizeof(int2) * ipp.size());
+    std::memcpy(hp + ipp.size(), ipk.data(), sizeof(int2) * ipk.size());
+    WB_CU(cudaMemcpyAsync(c->items_pp.p, hp, sizeof(int2) * ipp.size(), cudaMemcpyHostToDevice, s));
+    WB_CU(cudaMemcpyAsync(c->items_pk.p, hp + ipp.size(), sizeof(int2) * ipk.size(), cudaMemcpyHostToDevice, s));
+  }
   double2* aux = c->aux.as<double2>();
   double2* B = c->B.as<double2>();
   double2* X = c->X.as<double2>();
@@ -1006,7 +1014,8 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
                  c->sqvc.as<double>());
   }
   c->stats.fft_boxes += (long long)mb * npv + mp;
-  if (unconv_host) WB_CU(cudaMemcpyAsync(unconv_host, c->unconv.p, sizeof(int) * mb, cudaMemcpyDeviceToHost, s));
+  // to the pinned staging area; the caller reads it after its wait
+  WB_CU(cudaMemcpyAsync(c->pin, c->unconv.p, sizeof(int) * mb, cudaMemcpyDeviceToHost, s));
   return WB_OK;
 }
 
@@ -1032,7 +1041,6 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
   int rc = ensure_workspace(c, mb, on_device ? 1 : ld_dvg, on_device ? 1 : ld_dng);
   if (rc) return rc;
   std::vector<int> unc(m, 0);
-  std::vector<int> tmp(mb);
   for (int p0 = 0; p0 < m; p0 += mb) {
     const int nb = std::min(mb, m - p0);
     const double2* din;
@@ -1049,18 +1057,18 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
     // rows >= npw of dng are zero (apply_operator.f90:44, dng = 0)
     if (ld_dng > c->npw)
       WB_CU(cudaMemset2DAsync(dout + c->npw, sizeof(double2) * ld_dng, 0, sizeof(double2) * (ld_dng - c->npw), nb, s));
-    rc = run_batch(c, nb, din, ld_dvg, dout, ld_dng, tr2, tmp.data());
+    rc = run_batch(c, nb, din, ld_dvg, dout, ld_dng, tr2);
     if (rc) return rc;
     if (!on_device)
       WB_CU(cudaMemcpyAsync(dng + 2 * (size_t)p0 * ld_dng, c->dng_out.p, sizeof(double2) * (size_t)ld_dng * nb,
                             cudaMemcpyDeviceToHost, s));
-    WB_CU(cudaStreamSynchronize(s));
+    WB_CU(wb_wait(c));
     if (c->loop_pending) {  // the FP64 PCG graph's counters, copied by the batch
       c->stats.cg_iterations = std::max(c->stats.cg_iterations, c->loop_host[2]);
       loop_stats(c, c->loop_host[3], c->loop_pending);
       c->loop_pending = 0;
     }
-    for (int p = 0; p < nb; ++p) unc[p0 + p] = tmp[p];
+    std::memcpy(unc.data() + p0, c->pin, sizeof(int) * nb);
   }
   WB_CU(cudaEventRecord(c->ev1, s));
   WB_CU(cudaEventSynchronize(c->ev1));
@@ -1117,7 +1125,8 @@ int wb_ctx_create(wb_ctx** out, const wb_system* s, int device) {
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaMallocHost(&c->nact_host, sizeof(int) * 4) != cudaSuccess ||
       cudaMallocHost(&c->loop_host, sizeof(int) * 8) != cudaSuccess || c->loopst.ensure(sizeof(int) * 8) != 0 ||
-      cudaEventCreate(&c->tev0) != cudaSuccess || cudaEventCreate(&c->tev1) != cudaSuccess)
+      cudaEventCreate(&c->tev0) != cudaSuccess || cudaEventCreate(&c->tev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->wait_ev, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess)
     return bail(fail(WB_ERR_CUDA, "stream/event creation failed"));
   c->npw = s->npw;
   c->rt = compiled ? 0 : 1;
@@ -1265,6 +1274,8 @@ int wb_ctx_destroy(wb_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->tev0) cudaEventDestroy(c->tev0);
   if (c->tev1) cudaEventDestroy(c->tev1);
+  if (c->wait_ev) cudaEventDestroy(c->wait_ev);
+  if (c->pin) cudaFreeHost(c->pin);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;

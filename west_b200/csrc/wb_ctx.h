@@ -118,6 +118,24 @@ struct wb_ctx {
     float ms = 0.f;
   } tune;
   cudaEvent_t tev0 = nullptr, tev1 = nullptr;
+  cudaEvent_t wait_ev = nullptr;  // blocking-sync event of the calls' waits (wb_wait)
+  // pinned staging of a batch's small host transfers (unconverged counts, item
+  // tables): copies from or to pageable memory would wait for the stream by
+  // spinning, ahead of the blocking wait
+  unsigned char* pin = nullptr;
+  size_t pin_bytes = 0;
+  int ensure_pin(size_t b) {
+    if (b <= pin_bytes) return 0;
+    if (pin) cudaFreeHost(pin);
+    pin = nullptr;
+    pin_bytes = 0;
+    if (cudaMallocHost(&pin, b) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    pin_bytes = b;
+    return 0;
+  }
   DBuf loopst;               // int[8] loop state (wb_la.cu loop_init / loop_ctl)
   int* loop_host = nullptr;  // pinned copy of it
   int loop_pending = 0;      // launches per pass of a graph run whose counters await the batch's wait
@@ -160,3 +178,16 @@ struct wb_ctx {
   }
 };
 
+// Waits for the context's stream through a blocking-sync event: the calling
+// thread sleeps until the GPU signals instead of spinning on a core.  A thread
+// that spins through a wait on a host whose cores other processes keep busy
+// loses its time slices, and every slice it waits for leaves the GPU idle
+// before the next launch: c1 Davidson solves beside 32 busy processes took
+// 72-108 ms (medians of two runs) with spinning waits, 45-54 ms with sleeping
+// ones; on an idle host the wake-ups cost 1-5 ms of a 40 ms solve.  (Polling the
+// event for half a millisecond before sleeping did worse under load.)
+inline cudaError_t wb_wait(wb_ctx* c) {
+  if (!c->wait_ev) return cudaStreamSynchronize(c->stream);
+  const cudaError_t e = cudaEventRecord(c->wait_ev, c->stream);
+  return e == cudaSuccess ? cudaEventSynchronize(c->wait_ev) : e;
+}

@@ -1037,7 +1037,7 @@ struct Dav {
     };
     const int rc = dav_graph(c, s, key, body);
     if (rc) return rc;
-    WB_CU(cudaStreamSynchronize(s));
+    WB_CU(wb_wait(c));
     return WB_OK;
   }
   int unconverged() const { return reinterpret_cast<const int*>(host)[0]; }
