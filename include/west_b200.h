@@ -242,7 +242,11 @@ typedef struct wb_davidson_info {
  * ev, their convergence flags in conv and, when pdep != NULL, the eigenvectors
  * [ld_pdep, n_pdep_eigen] (host memory).  The subspace eigensolver is
  * wb_diagox's Jacobi method on the GPU (diagox uses LAPACK DSYEV / cuSOLVER in
- * WEST); n_pdep_basis up to 4096.
+ * WEST); n_pdep_basis up to 4096.  The basis, hr, vr, the eigenvalues and the
+ * convergence flags stay on the GPU: each iteration runs its dense steps as two
+ * CUDA graph launches around the operator call (cached per basis size; eager
+ * with wb_set_graphs(ctx, 0)) and the host reads back only the state it needs
+ * to choose the next batch.
  */
 /*
  * Operator hook of the Davidson: when set, wb_davidson calls fn instead of its
