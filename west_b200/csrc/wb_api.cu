@@ -1019,8 +1019,24 @@ int run_batch(wb_ctx* c, int mb, const double2* dvg, long ld_in, double2* dng, l
   return WB_OK;
 }
 
+}  // namespace
+
+// The FP64 PCG graph's counters of a finished batch (copied by the batch to
+// pinned memory) into the call's stats.
+void wb::apply_settle(wb_ctx* c) {
+  if (!c->loop_pending) return;
+  c->stats.cg_iterations = std::max(c->stats.cg_iterations, c->loop_host[2]);
+  loop_stats(c, c->loop_host[3], c->loop_pending);
+  c->loop_pending = 0;
+}
+
+namespace {
+
+// With defer (device buffers, one batch, no stage profiling) the call returns
+// right after enqueuing the batch: no wait, no unconverged counts, no ms_total;
+// the caller waits on the context's stream later and then calls apply_settle.
 int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng, double tr2, int iq,
-               int* unconverged, bool on_device) {
+               int* unconverged, bool on_device, bool* deferred = nullptr) {
   g_err.clear();
   if (!c) return fail(WB_ERR_ARG, "null context");
   if (m < 0) return fail(WB_ERR_ARG, "m < 0");
@@ -1038,6 +1054,8 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
   cudaStream_t s = c->stream;
   WB_CU(cudaEventRecord(c->ev0, s));
   const int mb = choose_batch(c, m);
+  const bool defer = deferred && on_device && mb >= m && !c->prof;
+  if (deferred) *deferred = defer;
   int rc = ensure_workspace(c, mb, on_device ? 1 : ld_dvg, on_device ? 1 : ld_dng);
   if (rc) return rc;
   std::vector<int> unc(m, 0);
@@ -1062,12 +1080,9 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
     if (!on_device)
       WB_CU(cudaMemcpyAsync(dng + 2 * (size_t)p0 * ld_dng, c->dng_out.p, sizeof(double2) * (size_t)ld_dng * nb,
                             cudaMemcpyDeviceToHost, s));
+    if (defer) return WB_OK;
     WB_CU(wb_wait(c));
-    if (c->loop_pending) {  // the FP64 PCG graph's counters, copied by the batch
-      c->stats.cg_iterations = std::max(c->stats.cg_iterations, c->loop_host[2]);
-      loop_stats(c, c->loop_host[3], c->loop_pending);
-      c->loop_pending = 0;
-    }
+    apply_settle(c);
     std::memcpy(unc.data() + p0, c->pin, sizeof(int) * nb);
   }
   WB_CU(cudaEventRecord(c->ev1, s));
@@ -1082,6 +1097,11 @@ int apply_impl(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int
 }
 
 }  // namespace
+
+int wb::apply_deferred(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng, double tr2,
+                       bool* deferred) {
+  return apply_impl(c, m, dvg, ld_dvg, dng, ld_dng, tr2, 1, nullptr, true, deferred);
+}
 
 extern "C" {
 
@@ -1266,6 +1286,8 @@ int wb_ctx_destroy(wb_ctx* c) {
   c->dav_graphs_release();
   if (c->dav_host) cudaFreeHost(c->dav_host);
   if (c->dav_aux) cudaStreamDestroy(c->dav_aux);
+  for (cudaEvent_t e : c->dav_ev)
+    if (e) cudaEventDestroy(e);
   for (DBuf* b : bufs) b->release();
   c->loopst.release();
   if (c->nact_host) cudaFreeHost(c->nact_host);

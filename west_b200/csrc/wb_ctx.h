@@ -158,6 +158,7 @@ struct wb_ctx {
   std::vector<DavGraph> dav_graphs;
   DBuf dav_st;
   cudaStream_t dav_aux = nullptr;  // second stream for captures that add conditional nodes
+  cudaEvent_t dav_ev[2] = {nullptr, nullptr};  // timing of a deferred operator call
   void* dav_host = nullptr;
   size_t dav_host_bytes = 0;
   void dav_graphs_release() {
@@ -191,3 +192,12 @@ inline cudaError_t wb_wait(wb_ctx* c) {
   const cudaError_t e = cudaEventRecord(c->wait_ev, c->stream);
   return e == cudaSuccess ? cudaEventSynchronize(c->wait_ev) : e;
 }
+
+namespace wb {
+// apply_operator on device buffers for the Davidson: when *deferred comes back
+// true the batch is only enqueued and the caller, after waiting on ctx's
+// stream, calls apply_settle; otherwise the call completed as usual.
+int apply_deferred(wb_ctx* c, int m, const double* dvg, int ld_dvg, double* dng, int ld_dng, double tr2,
+                   bool* deferred);
+void apply_settle(wb_ctx* c);
+}  // namespace wb

@@ -936,7 +936,6 @@ struct Dav {
   cudaStream_t aux = nullptr;  // second stream of the block Jacobi's graph form
   int apply_calls = 0;
   long long applied = 0;
-  std::vector<int> unconv;
 
   // do_mgs on columns [start, end) (davidson_diago.f90:909): the columns before
   // start are orthonormal, so the new block is first projected against all of
@@ -966,23 +965,45 @@ struct Dav {
     return WB_OK;
   }
   double apply_s = 0.0;
+  bool pending = false;  // an operator call whose batch is enqueued but not yet waited for
+  // Completes a pending operator call: waits for the stream unless the caller
+  // just did, folds in its counters and its time (events around the batch).
+  int settle(bool waited) {
+    if (!pending) return WB_OK;
+    if (!waited) WB_CU(wb_wait(c));
+    apply_settle(c);
+    float ms = 0.f;
+    WB_CU(cudaEventElapsedTime(&ms, c->dav_ev[0], c->dav_ev[1]));
+    apply_s += 1e-3 * ms;
+    pending = false;
+    return WB_OK;
+  }
+  // The operator on columns col0 .. col0 + n - 1.  The library's own call is
+  // only enqueued when it fits one batch: the steps after it follow on the same
+  // stream, and one wait (after them) covers both.
   int apply(int col0, int n, double tr2) {
-    unconv.assign(std::max(n, 1), 0);
-    const auto t0 = std::chrono::steady_clock::now();
     const double* x = reinterpret_cast<const double*>(dvg + (long)col0 * ld);
     double* y = reinterpret_cast<double*>(dng + (long)col0 * ld);
-    int rc;
+    int rc = settle(false);  // its pinned staging is reused by this call
+    if (rc) return rc;
     if (c->dav_apply) {
+      const auto t0 = std::chrono::steady_clock::now();
       WB_CU(cudaStreamSynchronize(s));  // the hook runs on its own streams
       rc = c->dav_apply(c->dav_apply_user, col0, n, x, y, (int)ld, tr2);
       if (rc) return fail(rc, "Davidson operator hook failed (code " + std::to_string(rc) + ")");
+      apply_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     } else {
-      rc = wb_apply_operator_device(c, n, x, (int)ld, y, (int)ld, tr2, 1, unconv.data());
+      for (cudaEvent_t& e : c->dav_ev)
+        if (!e) WB_CU(cudaEventCreate(&e));
+      WB_CU(cudaEventRecord(c->dav_ev[0], s));
+      bool deferred = false;
+      if ((rc = apply_deferred(c, n, x, (int)ld, y, (int)ld, tr2, &deferred))) return rc;
+      WB_CU(cudaEventRecord(c->dav_ev[1], s));
+      pending = true;
     }
-    apply_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     ++apply_calls;
     applied += n;
-    return rc;
+    return WB_OK;
   }
   int build_hr(int col0, int col1, int g_e) {  // hr(0:g_e, col0:col1) = <dvg|dng>
     const int ncol = col1 - col0, K = 2 * npw;
@@ -1038,7 +1059,7 @@ struct Dav {
     const int rc = dav_graph(c, s, key, body);
     if (rc) return rc;
     WB_CU(wb_wait(c));
-    return WB_OK;
+    return settle(true);
   }
   int unconverged() const { return reinterpret_cast<const int*>(host)[0]; }
   int conv_at(int i) const { return reinterpret_cast<const int*>(host)[1 + i]; }
