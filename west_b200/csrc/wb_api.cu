@@ -799,7 +799,11 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
                       c->g32.as<float2>(), c->d32.as<float2>(), npw, ld, s);
       cg_compact(conv, nsys, act, items, c->nact.as<int>(), c->nact_host, s);
     }
+    // the loop counters and the tensor-core GEMMs' error word ride along with the
+    // active count: the loop always leaves at this wait, with no launch after it,
+    // so the last copies are final
     if (graph) WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (c->umma) WB_CU(cudaMemcpyAsync(c->nact_host + 1, c->umma_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     WB_CU(wb_wait(c));
     nact = *c->nact_host;
     if (graph) inner_total = c->loop_host[3];
@@ -845,18 +849,10 @@ int cg_mixed(wb_ctx* c, int mb, double tr2, int nsplit, int* iters_out) {
     Stage g(c, WB_STAGE_CG, 1, mb);
     count_unconverged(conv, nocc, mb, c->unconv.as<int>(), s);
   }
-  if (graph) {
-    WB_CU(cudaMemcpyAsync(c->loop_host, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    WB_CU(wb_wait(c));
-    inner_total = c->loop_host[3];
-    loop_stats(c, inner_total, c->kinetic_only ? 6 : 9);
-  }
+  if (graph) loop_stats(c, inner_total, c->kinetic_only ? 6 : 9);
   *iters_out = inner_total;
   if (c->umma) {  // a bounded wait of a tensor-core GEMM that ran out leaves its code here
-    int* eh = c->nact_host + 1;  // a pinned slot (nact_host[0] is the active count)
-    WB_CU(cudaMemcpyAsync(eh, c->umma_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-    WB_CU(wb_wait(c));
-    const int e = *eh;
+    const int e = c->nact_host[1];
     if (e) {
       cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), s);
       return fail(WB_ERR_CUDA, "tensor-core GEMM wait limit reached (code " + std::to_string(e) + ")");
