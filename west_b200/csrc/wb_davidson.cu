@@ -11,6 +11,7 @@
 // and rank-1 updates, and Jacobi eigensolvers (diagox): cyclic in one CTA for
 // bases up to 112, parallel two-sided block Jacobi over many CTAs above.
 #include <algorithm>
+#include <iterator>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -1046,7 +1047,7 @@ struct Dav {
     const int n = nbase + notcnv;
     const std::vector<long long> key = {1, nbase, notcnv, test, nvec, nvecx, ld, nsplit, key_ptr(dvg), key_ptr(dng),
                                         key_ptr(hr), key_ptr(vr), key_ptr(A), key_ptr(V), key_ptr(w), key_ptr(part),
-                                        key_ptr(st), key_ptr(host), key_bits(trev), key_bits(trev_rel)};
+                                        key_ptr(bj), key_ptr(st), key_ptr(host), key_bits(trev), key_bits(trev_rel)};
     auto body = [&]() -> int {
       int rc = build_hr(nbase, n, n);
       if (rc) return rc;
@@ -1286,10 +1287,14 @@ extern "C" int wb_diagox(wb_ctx* c, int nbase, int nvec, const double* hr, int l
   jacobi_setup();
   WB_CU(cudaGetLastError());
   const size_t nn = (size_t)nbase * nbase;
+  const void* before[] = {c->dav_A.p, c->dav_V.p, c->dav_w.p, c->dav_bj.p};
   if (c->dav_A.ensure(sizeof(double) * nn) || c->dav_V.ensure(sizeof(double) * nn) ||
       c->dav_w.ensure(sizeof(double) * nbase + 64) ||
       (nbase > kJacobiSmemN && c->dav_bj.ensure(sizeof(double) * bj_doubles(nbase))))
     return fail(WB_ERR_NOMEM, "device allocation of the eigensolver scratch failed");
+  const void* after[] = {c->dav_A.p, c->dav_V.p, c->dav_w.p, c->dav_bj.p};
+  if (!std::equal(std::begin(before), std::end(before), std::begin(after)))
+    c->dav_graphs_release();  // the Davidson's cached graphs point into the old buffers
   double* w = c->dav_w.as<double>();
   int rc = eigen_lowest(hr, ldh, nbase, nvec, w, vr, ldv, c->dav_A.as<double>(), c->dav_V.as<double>(),
                         c->dav_bj.as<double>(), reinterpret_cast<int*>(w + nbase), c->stream);
