@@ -11,10 +11,10 @@
 // and rank-1 updates, and Jacobi eigensolvers (diagox): cyclic in one CTA for
 // bases up to 112, parallel two-sided block Jacobi over many CTAs above.
 #include <algorithm>
-#include <iterator>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <iterator>
 #include <vector>
 
 #include "wb_common.cuh"
