@@ -42,3 +42,23 @@ def test_davidson_graphs_replay_and_eager(small, nvec, times):
     assert np.abs((ev3 - ev1) / ev1).max() < 1e-10
     ov = O.glbrak_gamma(vec1, vec3)
     assert np.allclose(np.abs(np.diag(ov)), 1.0, atol=1e-8)
+
+
+def test_davidson_graphs_after_diagox_grows_the_scratch(small):
+    """wb_diagox on a larger matrix reallocates the eigensolver scratch the
+    Davidson's cached graphs point into; the next solve must capture anew and
+    reproduce the first one bit for bit."""
+    import torch
+    from west_b200.wstat import ResponseOperator, diagox
+    s = small
+    dvg0 = randomized_basis(s, 32)
+    op = ResponseOperator(s, verbose=False)
+    ev1, conv1, vec1, info1 = _solve(op, dvg0, 32, 4)             # basis 128: block Jacobi in the graph
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((200, 200))
+    hr = torch.from_numpy(np.ascontiguousarray((x + x.T) / 2)).cuda()
+    ew, _ = diagox(op, hr, 200, 8)
+    assert np.allclose(ew, np.linalg.eigvalsh((x + x.T) / 2)[:8], rtol=0, atol=1e-11 * np.abs(ew).max())
+    ev2, conv2, vec2, info2 = _solve(op, dvg0, 32, 4)
+    assert info1["dav_iter"] == info2["dav_iter"]
+    assert (ev1 == ev2).all() and (conv1 == conv2).all() and (vec1 == vec2).all()
